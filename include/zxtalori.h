@@ -1,0 +1,119 @@
+/* zxtalori B200 engine: the C ABI.
+ *
+ * Drop-in replacement for the reference engine's shared library (libzxtalori.so) as bound
+ * by python/zxtalori/api.py:18-55 through ctypes: every symbol that file binds is exported
+ * with the same signature, return convention and error-message prefixes. Each declaration
+ * cites the reference entry point it replaces (path:line in the reference project).
+ *
+ * Conventions (src/exports.zig, src/engine.zig:75,110-113):
+ *   - int results: 0 success, -1 failure; zo_error(h) then holds "<prefix>: <ErrorName>".
+ *   - Host arrays returned (quaternions, operations, point values) are owned by the engine
+ *     and valid until the next call that changes the sample; copy them.
+ *   - One engine per handle, called from one thread; zo_cancel may come from another.
+ *   - Quaternions are float32 [n][4], scalar first, symmetry acting on the right (q*g).
+ *   - Groups: 0 C2, 1 C3, 2 C4, 3 C6, 4 D2, 5 D3, 6 D4, 7 D6, 8 T, 9 O, 10 I.
+ */
+#ifndef ZXTALORI_H
+#define ZXTALORI_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* src/exports.zig:4 */
+const char* zo_version(void);
+
+/* src/native_api.zig:129. The wgpu directory argument is accepted and ignored; the engine
+ * runs on CUDA device ZXTALORI_DEVICE (default: the current device). NULL on failure. */
+void* zo_create(const char* wgpu_dir);
+/* src/native_api.zig:140 */
+const char* zo_create_error(void);
+/* src/native_api.zig:143 */
+void zo_destroy(void* h);
+
+/* src/exports.zig:9. Inverse Hopf product grids (kind 0/1); transports (kind 2). */
+int zo_generate(void* h, uint32_t group, uint32_t freq, uint32_t target, uint32_t seed, uint32_t kind);
+/* src/exports.zig:16. Exact-count insertion needs the covering triangulation: returns -1. */
+int zo_generate_exact(void* h, uint32_t group, uint32_t target, uint32_t flags);
+/* src/exports.zig:83. Seeded Haar-uniform sample folded into the zone (shaders/haar.wgsl). */
+int zo_random(void* h, uint32_t group, uint32_t count, uint32_t seed);
+/* src/exports.zig:23. Import n quaternions (folded into the zone). */
+int zo_set(void* h, uint32_t group, const float* q, uint32_t n);
+
+/* src/exports.zig:29-40 */
+uint32_t zo_count(void* h);
+uint32_t zo_order(void* h);
+const float* zo_quaternions(void* h);
+const float* zo_operations(void* h);
+
+/* src/exports.zig:41. Full measures below the ratio limit, else Quey energy + separation. */
+int zo_measure(void* h);
+/* src/exports.zig:60. Nearest orbit neighbour of every point (near field above 20,000). */
+int zo_spacing(void* h);
+/* src/exports.zig:49. Up to 1,000 Barzilai-Borwein steps of QVM repulsion. */
+int zo_relax(void* h, uint32_t steps);
+/* src/exports.zig:55. Forces within delta mean orientation radii; 0 for all pairs. */
+int zo_relax_neighbourhood(void* h, float delta);
+/* src/exports.zig:66. kind 0: nearest-neighbour SO(3) degrees; NULL before a pass. Kinds 1
+ * and 2 (covering) are always NULL here. */
+const float* zo_point_values(void* h, uint32_t kind);
+/* src/exports.zig:69. bit 0 add the identity, bit 1 hold it fixed. */
+int zo_identity(void* h, uint32_t flags);
+
+/* src/exports.zig:45,88-120. Covering radius, meshes and covering optimisation are not part
+ * of this engine: these return -1 (or NULL / 0) with an explanatory message. */
+int zo_cover(void* h);
+int zo_cover_optimize(void* h, uint32_t steps, uint32_t mode, uint32_t finish, float floor_deg);
+int zo_cover_kicks(void* h, uint32_t patience, float progress, float size, float trust);
+int zo_mesh(void* h);
+const float* zo_mesh_vertices(void* h);
+const uint32_t* zo_mesh_tets(void* h);
+uint32_t zo_mesh_vertex_count(void* h);
+uint32_t zo_mesh_tet_count(void* h);
+
+/* src/exports.zig:73-81 */
+const char* zo_stats(void* h);
+const char* zo_error(void* h);
+void zo_cancel(void* h);
+
+/* src/native_api.zig:161. Scales the all-pairs work split (smaller: more chunks). */
+void zo_pair_budget(void* h, float scale);
+/* src/native_api.zig:151-156. Per-dispatch profiling is not offered: false / 0. */
+bool zo_profile(void* h, bool enabled);
+size_t zo_profile_report(void* h, uint8_t* output, size_t capacity);
+
+/* Extension, no reference counterpart: arithmetic of this engine's pair path.
+ * 0 FP32 pair arithmetic with FP64 sums, BB products and renormalisation (default);
+ * 1 FP64 throughout (the plain method). Resets the BB history. */
+int zo_precision(void* h, uint32_t mode);
+uint32_t zo_get_precision(void* h);
+/* Extension: the nearest orbit neighbour's source index of every point (same pass as
+ * zo_point_values kind 0), or NULL before such a pass. */
+const int32_t* zo_point_neighbours(void* h);
+/* Development hook, in the spirit of the reference's dev symbols (src/native_api.zig:150-175):
+ * one pass's raw per-source rows into `out` (the caller's n * width doubles).
+ * what 0: the relaxation's force pass (all pairs, or the near field when a neighbourhood is
+ *   set): force x y z, curvature, Quey energy, nearest squared chord, neighbour position
+ *   (image index k*n+j for all pairs, sorted site for the near field), 0 (width 8).
+ * what 1: full measure rows: force x y z, curvature, Quey energy, nearest squared chord,
+ *   Riesz 1, 2, 3, Green, log sums (the self pair's antipode not yet added), degenerate
+ *   flag (width 12). */
+int zo_debug_rows(void* h, uint32_t what, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#endif /* ZXTALORI_H */

@@ -1,0 +1,836 @@
+// Engine: sample state and the reference's policies over the CUDA kernels.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+namespace zo {
+
+namespace {
+constexpr double kPiH = 3.14159265358979323846;
+constexpr uint32_t kMaxCount = 10000000;          // hopf.max_count (src/hopf.zig:23)
+constexpr double kFullMeasurePairs = 5e10;        // src/engine.zig:1123
+constexpr uint32_t kSpacingAllPairs = 20000;      // src/engine.zig:1126
+constexpr double kSpacingDelta = 4;               // src/engine.zig:1127
+constexpr const char* kVersion = "0.3.0";
+
+std::mutex g_tables_mutex;
+bool g_tables_uploaded[64] = {false};
+
+void ensure_tables(int device) {
+  std::lock_guard<std::mutex> lock(g_tables_mutex);
+  if (device < 0 || device >= 64) throw Failure("InvalidDevice");
+  if (g_tables_uploaded[device]) return;
+  ZO_CUDA(upload_tables(host_tables()));
+  g_tables_uploaded[device] = true;
+}
+
+double separation_of(double chord2) {
+  return 4.0 * std::asin(std::min(1.0, std::sqrt(std::max(chord2, 0.0)) / 2.0)) * 180.0 / kPiH;
+}
+}  // namespace
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  char msg[512];
+  std::snprintf(msg, sizeof msg, "CudaError %s (%s)", cudaGetErrorString(e), what);
+  throw Failure(msg);
+}
+
+double mean_radius(double count) {
+  // d_r: half the m with pi (m - sin m) = pi^2 / count, 60 bisections (src/pairs.zig:205-215).
+  const double target = kPiH * kPiH / count;
+  double lo = 0, hi = kPiH;
+  for (int k = 0; k < 60; ++k) {
+    const double middle = 0.5 * (lo + hi);
+    if (kPiH * (middle - std::sin(middle)) < target) lo = middle;
+    else hi = middle;
+  }
+  return 0.25 * (lo + hi);
+}
+
+// ------------------------------------------------------------------ buffers
+void* DeviceBuffer::ensure(size_t bytes) {
+  if (bytes <= bytes_ && ptr_) return ptr_;
+  release();
+  const size_t want = std::max<size_t>(bytes, 256);
+  ZO_CUDA(cudaMalloc(&ptr_, want));
+  bytes_ = want;
+  return ptr_;
+}
+void DeviceBuffer::release() {
+  if (ptr_) cudaFree(ptr_);
+  ptr_ = nullptr;
+  bytes_ = 0;
+}
+
+Rows RowBuffers::ensure(size_t n) {
+  force.ensure(n * sizeof(double4));
+  energy.ensure(n * sizeof(double));
+  nearest.ensure(n * sizeof(double));
+  nearest_at.ensure(n * sizeof(int));
+  return rows();
+}
+
+// ------------------------------------------------------------------ near field
+void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_r, int sms) {
+  ready_ = false;
+  n_ = n;
+  prec_ = prec;
+  radius_ = std::min(1.5, delta_ * mean_r);
+  s_margin_ = std::sin(radius_ + 1e-4);
+  chord_ = 2.0 * std::sin(radius_ / 2.0);
+  counts_.ensure((size_t)(n + 1) * 4);
+  offsets_.ensure((size_t)(n + 1) * 4);
+  scan_tmp_.ensure(4096 * 4);
+  ZO_CUDA(launch_shell_count(prec, q32, q64, n, gid_, s_margin_, counts_.as<uint32_t>(), offsets_.as<uint32_t>(),
+                             scan_tmp_.as<uint32_t>(), s));
+  uint32_t total = 0;
+  ZO_CUDA(cudaMemcpyAsync(&total, offsets_.as<uint32_t>() + n, 4, cudaMemcpyDeviceToHost, s));
+  ZO_CUDA(cudaStreamSynchronize(s));
+  // Room for the shell to change as the sources move (src/near.zig:115-123).
+  const uint64_t order = (uint64_t)host_group_order(gid_);
+  uint64_t cap = (uint64_t)total + total / 4 + 1024;
+  cap = std::min<uint64_t>(cap, 2 * order * (uint64_t)n);
+  cap = std::max<uint64_t>(cap, (uint64_t)total);
+  if (cap > (1ull << 31) - 1) throw Failure("NearShellTooLarge");
+  capacity_ = (int)cap;
+  sdim_max_ = (int)std::lround(std::cbrt((double)capacity_ / 8.0));
+  sdim_max_ = std::max(1, std::min(sdim_max_, kMaxCellDim));
+  const size_t cells = (size_t)sdim_max_ * sdim_max_ * sdim_max_ + 1;
+  const size_t qsize = prec == kFP64 ? sizeof(double4) : sizeof(float4);
+  site_q_.ensure(capacity_ * qsize);
+  site_code_.ensure(capacity_ * 4ull);
+  site_img_.ensure(capacity_ * 4ull);
+  site_cell_.ensure(capacity_ * 4ull);
+  site_rank_.ensure(capacity_ * 4ull);
+  site_pos_.ensure(capacity_ * sizeof(float4));
+  cell_count_.ensure(cells * 4);
+  cell_off_.ensure(cells * 4);
+  perm_.ensure(capacity_ * 4ull);
+  sq_.ensure(capacity_ * qsize);
+  scode_.ensure(capacity_ * 4ull);
+  simg_.ensure(capacity_ * 4ull);
+  const size_t mcells = (size_t)kMortonDim * kMortonDim * kMortonDim + 1;
+  src_key_.ensure((size_t)n * 4);
+  src_rank_.ensure((size_t)n * 4);
+  mcount_.ensure(mcells * 4);
+  moff_.ensure(mcells * 4);
+  src_perm_.ensure((size_t)n * 4);
+  grid_.ensure(sizeof(NearGrid));
+  cells_.ensure(sizeof(int));
+  NearGrid g{};
+  for (int a = 0; a < 3; ++a) {
+    g.box_bits[a] = 0xffffffffu;
+    g.box_bits[3 + a] = 0u;
+  }
+  ZO_CUDA(cudaMemcpyAsync(grid_.as<NearGrid>(), &g, sizeof g, cudaMemcpyHostToDevice, s));
+  // Warp tasks (32 sources x one slice of their cell rows): several waves of resident warps.
+  const int warps = (n + 31) / 32;
+  slices_ = std::max(1, std::min(64, (sms * 48 + warps - 1) / warps));
+  partial_.ensure((size_t)slices_ * n);
+  ZO_CUDA(cudaStreamSynchronize(s));
+  ready_ = true;
+}
+
+void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_r, bool track,
+                     Rows out, int sms) {
+  if (!ready_ || n != n_ || prec != prec_) setup(s, prec, q32, q64, n, mean_r, sms);
+  NearLaunch L{};
+  L.prec = prec;
+  L.gid = gid_;
+  L.n = n;
+  L.capacity = capacity_;
+  L.sdim_max = sdim_max_;
+  L.slices = slices_;
+  L.track = track;
+  L.s_margin = s_margin_;
+  L.cut2 = chord_ * chord_;
+  L.chord = chord_;
+  L.cut_z = taper_ * radius_;
+  L.cut_w = 1.0 / std::max(1e-9, (1.0 - taper_) * radius_);
+  L.q32 = q32;
+  L.q64 = q64;
+  L.counts = counts_.as<uint32_t>();
+  L.offsets = offsets_.as<uint32_t>();
+  L.scan_tmp = scan_tmp_.as<uint32_t>();
+  L.site_q32 = prec == kFP64 ? nullptr : site_q_.as<float4>();
+  L.site_q64 = prec == kFP64 ? site_q_.as<double4>() : nullptr;
+  L.site_code = site_code_.as<uint32_t>();
+  L.site_img = site_img_.as<uint32_t>();
+  L.site_cell = site_cell_.as<uint32_t>();
+  L.site_rank = site_rank_.as<uint32_t>();
+  L.site_pos = site_pos_.as<float4>();
+  L.cell_count = cell_count_.as<uint32_t>();
+  L.cell_off = cell_off_.as<uint32_t>();
+  L.perm = perm_.as<uint32_t>();
+  L.sq32 = prec == kFP64 ? nullptr : sq_.as<float4>();
+  L.sq64 = prec == kFP64 ? sq_.as<double4>() : nullptr;
+  L.scode = scode_.as<uint32_t>();
+  L.simg = simg_.as<uint32_t>();
+  L.src_key = src_key_.as<uint32_t>();
+  L.src_rank = src_rank_.as<uint32_t>();
+  L.mcount = mcount_.as<uint32_t>();
+  L.moff = moff_.as<uint32_t>();
+  L.src_perm = src_perm_.as<uint32_t>();
+  L.grid = grid_.as<NearGrid>();
+  L.cells = cells_.as<int>();
+  L.partial = partial_.rows();
+  L.out = out;
+  ZO_CUDA(launch_near(L, s));
+}
+
+bool NearField::overflowed(cudaStream_t s) {
+  if (!ready_) return false;
+  unsigned int flag = 0;
+  ZO_CUDA(cudaMemcpyAsync(&flag, &grid_.as<NearGrid>()->overflow, 4, cudaMemcpyDeviceToHost, s));
+  ZO_CUDA(cudaStreamSynchronize(s));
+  if (!flag) return false;
+  ready_ = false;
+  return true;
+}
+
+// ------------------------------------------------------------------ relaxation state
+void RelaxState::reset() {
+  n_ = 0;
+  prec_ = -1;
+  current = false;
+  // The near-field settings stay; its buffers are sized again on the next pass.
+  if (near_) near_ = std::make_unique<NearField>(near_->gid(), near_->delta());
+}
+
+void RelaxState::set_near(int gid, std::optional<double> delta) {
+  if (near_) {
+    if (delta && near_->gid() == gid && near_->delta() == *delta) return;
+    near_.reset();
+    current = false;
+  }
+  if (delta) {
+    near_ = std::make_unique<NearField>(gid, *delta);
+    current = false;
+  }
+}
+
+void RelaxState::prepare(int n, int prec) {
+  if (n_ == n && prec_ == prec) return;
+  n_ = n;
+  prec_ = prec;
+  current = false;
+  rows_.ensure(n);
+  prev_f_.ensure((size_t)n * sizeof(double4));
+  prev_d_.ensure((size_t)n * sizeof(double4));
+  ZO_CUDA(cudaMemset(prev_f_.as<void>(), 0, (size_t)n * sizeof(double4)));
+  ZO_CUDA(cudaMemset(prev_d_.as<void>(), 0, (size_t)n * sizeof(double4)));
+  state_.ensure(sizeof(RelaxDev));
+  ZO_CUDA(cudaMemset(state_.as<void>(), 0, sizeof(RelaxDev)));
+  const int blocks = reduce_blocks(n);
+  stats_partials_.ensure((size_t)blocks * 5 * sizeof(double));
+  hist_.ensure(512 * 4);
+  ZO_CUDA(cudaMemset(hist_.as<void>(), 0, 512 * 4));
+  summary_.ensure(sizeof(RowSummary));
+  ZO_CUDA(cudaMemset(summary_.as<void>(), 0, sizeof(RowSummary)));
+  summary_partials_.ensure((size_t)blocks * 2 * sizeof(double));
+  near_partials_.ensure((size_t)blocks * sizeof(double));
+  near_rows_.ensure((size_t)blocks * sizeof(int));
+  degrees_.ensure((size_t)n * sizeof(float));
+  neighbours_.ensure((size_t)n * sizeof(int));
+}
+
+void RelaxState::record_forces(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, int gid,
+                               bool track, double budget_scale, int sms) {
+  const int order = host_group_order(gid);
+  if (near_) {
+    near_->pass(s, prec, q32, q64, n, mean_radius((double)n * order), track, rows_.rows(), sms);
+    return;
+  }
+  const PairsPlan pl = plan_pairs(n, order, budget_scale, sms);
+  Rows partial{};
+  if (pl.chunks > 1) partial = partial_.ensure((size_t)pl.chunks * n);
+  ZO_CUDA(launch_pairs(prec, track, q32, q64, n, gid, pl, partial, rows_.rows(), s));
+}
+
+void RelaxState::step(cudaStream_t s, int prec, float4* q32, double4* q64, int n, int gid, int fixed,
+                      double budget_scale, int sms) {
+  prepare(n, prec);
+  if (!current) record_forces(s, prec, q32, q64, n, gid, false, budget_scale, sms);
+  current = false;
+  order_ = host_group_order(gid);
+  const double radius = mean_radius((double)n * order_);
+  const double alpha0 = (0.8 / 3.4) * radius * radius * radius;
+  RelaxDev* st = state_.as<RelaxDev>();
+  ZO_CUDA(launch_relax_stats(rows_.rows(), prev_f_.as<double4>(), prev_d_.as<double4>(), n, fixed,
+                             stats_partials_.as<double>(), st, s));
+  ZO_CUDA(launch_median(prec, rows_.rows(), n, st, hist_.as<unsigned int>(), alpha0, radius, sms, s));
+  ZO_CUDA(launch_move_fold(q32, q64, n, gid, prec, rows_.rows(), prev_f_.as<double4>(), prev_d_.as<double4>(), st,
+                           fixed, radius, 1.0, s));
+}
+
+StepResult RelaxState::step_result(const RelaxDev& st) const {
+  if (st.flags & 1u) throw Failure("NonFiniteForce");
+  if (st.flags & 2u) throw Failure("DuplicateOrientations");
+  const double n = n_;
+  double step_max;
+  std::memcpy(&step_max, &st.step_bits, 8);
+  StepResult r;
+  r.max_step_deg = step_max * 360.0 / kPiH;
+  r.force_rms = std::sqrt(st.sums[3] / n);
+  r.energy = st.sums[4] / (n * order_ * std::max(n - 1, 1.0));
+  return r;
+}
+
+StepResult RelaxState::finish(cudaStream_t s) {
+  RelaxDev st;
+  ZO_CUDA(cudaMemcpyAsync(&st, state_.as<RelaxDev>(), sizeof st, cudaMemcpyDeviceToHost, s));
+  ZO_CUDA(cudaStreamSynchronize(s));
+  return step_result(st);
+}
+
+Measures RelaxState::summarize(cudaStream_t s, int n, int order, float* degrees, int* neighbours, int prec,
+                               const float4* q32, int gid) {
+  const Rows r = rows_.rows();
+  const bool near_sites = near_ != nullptr;
+  const uint32_t* scode = near_sites ? near_->sorted_codes() : nullptr;
+  const uint32_t* simg = near_sites ? near_->sorted_images() : nullptr;
+  if (prec == kFP32) ZO_CUDA(launch_refine_nearest(q32, n, gid, r, near_sites, scode, simg, neighbours_.as<int>(), s));
+  else ZO_CUDA(launch_neighbour_index(r, n, near_sites, scode, neighbours_.as<int>(), s));
+  ZO_CUDA(launch_row_summary(r, n, summary_partials_.as<double>(), near_partials_.as<double>(), near_rows_.as<int>(),
+                             summary_.as<RowSummary>(), s));
+  ZO_CUDA(launch_nearest_degrees(r.nearest, n, degrees_.as<float>(), s));
+  RowSummary sum;
+  ZO_CUDA(cudaMemcpyAsync(&sum, summary_.as<RowSummary>(), sizeof sum, cudaMemcpyDeviceToHost, s));
+  if (degrees) ZO_CUDA(cudaMemcpyAsync(degrees, degrees_.as<float>(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+  if (neighbours) ZO_CUDA(cudaMemcpyAsync(neighbours, neighbours_.as<int>(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
+  ZO_CUDA(cudaStreamSynchronize(s));
+  order_ = order;
+  if (!(sum.nearest > 0)) throw Failure("DuplicateOrientations");
+  Measures m;
+  m.count_extended = 2.0 * order * n;
+  m.quey_energy = sum.energy / ((double)n * order * std::max<double>(n - 1, 1));
+  m.separation_deg = separation_of(sum.nearest);
+  m.force_rms = std::sqrt(sum.force2 / n);
+  return m;
+}
+
+// ------------------------------------------------------------------ engine
+Engine::Engine() {
+  const char* dev = std::getenv("ZXTALORI_DEVICE");
+  int count = 0;
+  ZO_CUDA(cudaGetDeviceCount(&count));
+  if (count <= 0) throw Failure("NoCudaDevice");
+  if (dev && *dev) device_ = std::atoi(dev);
+  else ZO_CUDA(cudaGetDevice(&device_));
+  if (device_ < 0 || device_ >= count) throw Failure("InvalidDevice");
+  ZO_CUDA(cudaSetDevice(device_));
+  cudaDeviceProp prop;
+  ZO_CUDA(cudaGetDeviceProperties(&prop, device_));
+  if (prop.major < 10) throw Failure("NeedsSm100");
+  sms_ = prop.multiProcessorCount;
+  ensure_tables(device_);
+  ZO_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+}
+
+Engine::~Engine() {
+  cudaSetDevice(device_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+uint32_t Engine::ratio_limit() const {
+  return (uint32_t)std::floor(std::sqrt(kFullMeasurePairs / (double)order()));
+}
+
+std::optional<uint32_t> Engine::identity_index() const {
+  for (uint32_t i = 0; i < n_; ++i) {
+    const float* a = &host_[(size_t)i * 4];
+    if (std::fabs(a[1]) + std::fabs(a[2]) + std::fabs(a[3]) < 1e-6f) return i;
+  }
+  return std::nullopt;
+}
+
+void Engine::fetch() {
+  host_.resize((size_t)n_ * 4);
+  ZO_CUDA(cudaMemcpyAsync(host_.data(), q32_.as<float4>(), (size_t)n_ * 16, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::reset_run() {
+  point_separation_iteration_.reset();
+  relax_state_.reset();
+  iteration_ = 0;
+  step_deg_ = 0;
+  force_rms_ = 0;
+  measures_.reset();
+  full_measures_ = false;
+  cancelled_.store(false);
+  err[0] = 0;
+}
+
+void Engine::adopt(uint32_t n) {
+  n_ = n;
+  fixed_index_.reset();
+  if (fix_identity_) fixed_index_ = identity_index();
+  reset_run();
+}
+
+void Engine::set(int gid, const float* values, size_t count) {
+  if (count == 0 || count > kMaxCount) throw Failure("InvalidCount");
+  for (size_t i = 0; i < count; ++i) {
+    double norm = 0;
+    for (int c = 0; c < 4; ++c) {
+      const float x = values[i * 4 + c];
+      if (!std::isfinite(x)) throw Failure("NonFiniteQuaternion");
+      norm += (double)x * x;
+    }
+    if (norm < 1e-20) throw Failure("ZeroQuaternion");
+  }
+  ZO_CUDA(cudaSetDevice(device_));
+  const uint32_t n = (uint32_t)count;
+  q32_.ensure((size_t)n * 16);
+  ZO_CUDA(cudaMemcpyAsync(q32_.as<float4>(), values, (size_t)n * 16, cudaMemcpyHostToDevice, stream_));
+  if (prec_ == kFP64) q64_.ensure((size_t)n * 32);
+  ZO_CUDA(launch_fold(q32_.as<float4>(), q64(), (int)n, gid, prec_, true, stream_));
+  group_ = gid;
+  n_ = n;
+  fetch();
+  adopt(n);
+  generator_ = "Imported quaternions";
+}
+
+void Engine::generate_random(int gid, uint32_t count, uint32_t seed) {
+  if (count < 1 || count > kMaxCount) throw Failure("InvalidCount");
+  ZO_CUDA(cudaSetDevice(device_));
+  q32_.ensure((size_t)count * 16);
+  if (prec_ == kFP64) q64_.ensure((size_t)count * 32);
+  ZO_CUDA(launch_haar(q32_.as<float4>(), (int)count, seed, stream_));
+  group_ = gid;
+  ZO_CUDA(launch_fold(q32_.as<float4>(), q64(), (int)count, gid, prec_, true, stream_));
+  n_ = count;
+  fetch();
+  adopt(count);
+  generator_ = "Haar random";
+  seed_ = seed;
+}
+
+void Engine::generate_grid(int gid, uint32_t freq, uint32_t target, uint32_t seed, uint32_t kind) {
+  (void)gid, (void)freq, (void)target, (void)seed, (void)kind;
+  throw Failure("HopfGridNotAvailable");
+}
+
+void Engine::set_precision(int prec) {
+  if (prec != kFP32 && prec != kFP64) throw Failure("UnknownPrecision");
+  if (prec == prec_) return;
+  ZO_CUDA(cudaSetDevice(device_));
+  if (prec == kFP64 && n_ > 0) {
+    std::vector<double> wide(host_.begin(), host_.end());
+    q64_.ensure((size_t)n_ * 32);
+    ZO_CUDA(cudaMemcpyAsync(q64_.as<double4>(), wide.data(), (size_t)n_ * 32, cudaMemcpyHostToDevice, stream_));
+    ZO_CUDA(cudaStreamSynchronize(stream_));
+  }
+  prec_ = prec;
+  relax_state_.reset();
+  spacing_state_.reset();
+}
+
+void Engine::set_neighbourhood(double delta) {
+  if (!(delta == 0 || (delta >= 2 && delta <= 1000))) throw Failure("NeighbourhoodOutside2To1000");
+  neighbourhood_ = delta;
+}
+
+void Engine::sync_neighbourhood() {
+  relax_state_.set_near(group_, neighbourhood_ > 0 ? std::optional<double>(neighbourhood_) : std::nullopt);
+  measure_neighbourhood_ = neighbourhood_;
+}
+
+Measures Engine::relax_state_measure() {
+  relax_state_.prepare((int)n_, prec_);
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    relax_state_.current = false;
+    relax_state_.record_forces(stream_, prec_, q32(), q64(), (int)n_, group_, true, budget_scale_, sms_);
+    ZO_CUDA(cudaStreamSynchronize(stream_));
+    if (relax_state_.near_overflowed(stream_)) continue;
+    point_separation_.resize(n_);
+    point_neighbours_.resize(n_);
+    point_separation_iteration_ = iteration_;
+    Measures m = relax_state_.summarize(stream_, (int)n_, (int)order(), point_separation_.data(),
+                                        point_neighbours_.data(), prec_, q32(), group_);
+    relax_state_.current = true;
+    return m;
+  }
+  throw Failure("NearShellTooLarge");
+}
+
+Measures Engine::full_measure() {
+  const int n = (int)n_, order = (int)this->order();
+  const PairsPlan pl = plan_pairs(n, order, budget_scale_, sms_);
+  const Rows out = full_rows_.ensure(n);
+  Rows partial{};
+  double* pextra = nullptr;
+  int* pdegen = nullptr;
+  if (pl.chunks > 1) {
+    partial = full_partial_.ensure((size_t)pl.chunks * n);
+    pextra = (double*)full_pextra_.ensure((size_t)pl.chunks * n * 5 * sizeof(double));
+    pdegen = (int*)full_pdegen_.ensure((size_t)pl.chunks * n * sizeof(int));
+  }
+  double* extra = (double*)full_extra_.ensure((size_t)n * 5 * sizeof(double));
+  int* degen = (int*)full_degen_.ensure((size_t)n * sizeof(int));
+  ZO_CUDA(launch_full(prec_, q32(), q64(), n, group_, pl, partial, pextra, pdegen, out, extra, degen, stream_));
+  if (prec_ == kFP32) {
+    DeviceBuffer scratch;
+    ZO_CUDA(launch_refine_nearest(q32(), n, group_, out, false, nullptr, nullptr, (int*)scratch.ensure((size_t)n * 4),
+                                  stream_));
+    ZO_CUDA(cudaStreamSynchronize(stream_));
+  }
+  std::vector<double> hx((size_t)n * 5), he(n), hn(n);
+  std::vector<double4> hf(n);
+  std::vector<int> hd(n);
+  ZO_CUDA(cudaMemcpyAsync(hx.data(), extra, hx.size() * 8, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaMemcpyAsync(he.data(), out.energy, he.size() * 8, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaMemcpyAsync(hn.data(), out.nearest, hn.size() * 8, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaMemcpyAsync(hf.data(), out.force, hf.size() * sizeof(double4), cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaMemcpyAsync(hd.data(), degen, hd.size() * 4, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  // Host FP64 sums and normalisations (src/pairs.zig:142-173); the self pair's antipode
+  // adds (1/2, 1/4, 1/8) to the Riesz rows, -3/(8 pi^2) to Green and 1/4 - ln 2 to log.
+  double sum[5] = {0, 0, 0, 0, 0}, energy = 0, force2 = 0, nearv = 4;
+  bool degenerate = false;
+  for (int i = 0; i < n; ++i) {
+    sum[0] += hx[(size_t)i * 5 + 0] + 0.5;
+    sum[1] += hx[(size_t)i * 5 + 1] + 0.25;
+    sum[2] += hx[(size_t)i * 5 + 2] + 0.125;
+    sum[3] += hx[(size_t)i * 5 + 4] + (0.25 - std::log(2.0));
+    sum[4] += hx[(size_t)i * 5 + 3] - 3.0 / (8.0 * kPiH * kPiH);
+    degenerate |= hd[i] != 0;
+    energy += he[i];
+    force2 += hf[i].x * hf[i].x + hf[i].y * hf[i].y + hf[i].z * hf[i].z;
+    nearv = std::min(nearv, hn[i]);
+  }
+  if (degenerate) sum[3] = 1e30 * n;
+  if (nearv <= 0) throw Failure("DuplicateOrientations");
+  const double ext = 2.0 * order, total = n * ext;
+  for (double& v : sum) v *= ext;
+  const double c_green = std::pow(3.0, 5.0 / 3.0) /
+                         (5.0 * std::pow(2.0 * kPiH * kPiH, 1.0 / 3.0) * std::pow(4.0 * kPiH, 2.0 / 3.0));
+  const double delta_log = (sum[3] + 0.25 * total + std::log(total) * total / 3.0) / total;
+  Measures m;
+  m.count_extended = total;
+  m.riesz_1 = sum[0] / (total * total * (8.0 / (3.0 * kPiH)));
+  m.riesz_2 = sum[1] / (total * total);
+  m.riesz_3 = sum[2] / ((2.0 / (3.0 * kPiH)) * total * total * std::log(total));
+  m.green_ratio = sum[4] / (-c_green * std::pow(total, 4.0 / 3.0));
+  m.log_ratio = delta_log / (-5.0 / 12.0);
+  m.quey_energy = energy / ((double)n * order * std::max(n - 1.0, 1.0));
+  m.separation_deg = separation_of(nearv);
+  m.force_rms = std::sqrt(force2 / n);
+  return m;
+}
+
+void Engine::measure() {
+  if (n_ == 0) throw Failure("NoOrientations");
+  ZO_CUDA(cudaSetDevice(device_));
+  if (n_ > ratio_limit()) {
+    sync_neighbourhood();
+    measures_ = relax_state_measure();
+    full_measures_ = false;
+  } else {
+    measures_ = full_measure();
+    full_measures_ = true;
+    measure_neighbourhood_ = 0;
+    sync_neighbourhood();
+    relax_state_measure();
+    measure_neighbourhood_ = 0;
+  }
+  measure_iteration_ = iteration_;
+}
+
+void Engine::spacing() {
+  if (n_ < 2) throw Failure("TooFewOrientations");
+  ZO_CUDA(cudaSetDevice(device_));
+  spacing_state_.set_near(group_, n_ > kSpacingAllPairs ? std::optional<double>(kSpacingDelta) : std::nullopt);
+  spacing_state_.prepare((int)n_, prec_);
+  point_separation_.resize(n_);
+  point_neighbours_.resize(n_);
+  point_separation_iteration_ = iteration_;
+  for (int attempt = 0;; ++attempt) {
+    if (attempt == 4) throw Failure("NearShellTooLarge");
+    spacing_state_.record_forces(stream_, prec_, q32(), q64(), (int)n_, group_, true, budget_scale_, sms_);
+    ZO_CUDA(cudaStreamSynchronize(stream_));
+    if (!spacing_state_.near_overflowed(stream_)) break;
+  }
+  try {
+    spacing_state_.summarize(stream_, (int)n_, (int)order(), point_separation_.data(), point_neighbours_.data(), prec_,
+                             q32(), group_);
+  } catch (const Failure&) {
+    // A duplicate shows as a zero separation below.
+  }
+  float least = 180.0f;
+  for (float d : point_separation_) least = std::min(least, d);
+  if (!(least > 0)) throw Failure("DuplicateOrientations");
+  if (measures_ && measure_iteration_ == iteration_) {
+    measures_->separation_deg = least;
+    return;
+  }
+  Measures m;
+  m.count_extended = 2.0 * order() * n_;
+  m.separation_deg = least;
+  measures_ = m;
+  measure_iteration_ = iteration_;
+  full_measures_ = false;
+}
+
+void Engine::relax(uint32_t steps) {
+  if (n_ < 2) throw Failure("TooFewOrientations");
+  ZO_CUDA(cudaSetDevice(device_));
+  cancelled_.store(false);
+  sync_neighbourhood();
+  const double n = n_, order = this->order();
+  // Wait every ~2e10 pair evaluations so a cancel is seen (src/engine.zig:899-907).
+  const double neighbours =
+      neighbourhood_ > 0 ? std::min(n * order, 0.94 * std::pow(neighbourhood_, 3) + 64) : n * order;
+  const uint64_t sync_every = (uint64_t)std::max(1.0, std::floor(2e10 / (n * neighbours)));
+  const uint32_t run = std::min<uint32_t>(steps, 1000);
+  bool recorded = false;
+  for (uint32_t index = 0; index < run; ++index) {
+    if (cancelled_.load()) break;
+    if (fix_identity_ && !fixed_index_) throw Failure("IdentityMissingEnableAddIdentity");
+    relax_state_.step(stream_, prec_, q32(), q64(), (int)n_, group_, fixed_arg(), budget_scale_, sms_);
+    ++iteration_;
+    recorded = true;
+    if ((index + 1) % sync_every == 0 && index + 1 < run) {
+      const StepResult r = relax_state_.finish(stream_);
+      step_deg_ = r.max_step_deg;
+      force_rms_ = r.force_rms;
+      recorded = false;
+    }
+  }
+  measures_.reset();
+  // One wait ends the batch: the last step, positions, energy and separation, whose forces
+  // start the next step (RelaxState.complete, src/pairs.zig:377-399).
+  std::optional<StepResult> last;
+  if (recorded) last = relax_state_.finish(stream_);
+  Measures m = relax_state_measure();
+  fetch();
+  if (last) {
+    step_deg_ = last->max_step_deg;
+    force_rms_ = last->force_rms;
+  }
+  measures_ = m;
+  full_measures_ = false;
+  measure_iteration_ = iteration_;
+}
+
+void Engine::identity(bool add, bool fixed) {
+  if (n_ == 0) throw Failure("NoOrientations");
+  std::optional<uint32_t> index = identity_index();
+  if (add && !index) {
+    std::vector<float> values(host_);
+    values.insert(values.end(), {1.f, 0.f, 0.f, 0.f});
+    const std::string generator = generator_;
+    set(group_, values.data(), values.size() / 4);
+    generator_ = generator;
+    index = n_ - 1;
+  }
+  if (fixed && !index) throw Failure("IdentityMissingEnableAddIdentity");
+  if (fix_identity_ != fixed) relax_state_.reset();
+  fix_identity_ = fixed;
+  fixed_index_ = fixed ? index : std::nullopt;
+  if (fixed) {
+    const uint32_t i = *index;
+    const float one[4] = {1.f, 0.f, 0.f, 0.f};
+    std::memcpy(&host_[(size_t)i * 4], one, 16);
+    ZO_CUDA(cudaMemcpyAsync(q32() + i, one, 16, cudaMemcpyHostToDevice, stream_));
+    if (prec_ == kFP64) {
+      const double one64[4] = {1, 0, 0, 0};
+      ZO_CUDA(cudaMemcpyAsync(q64() + i, one64, 32, cudaMemcpyHostToDevice, stream_));
+    }
+    ZO_CUDA(cudaStreamSynchronize(stream_));
+    relax_state_.current = false;
+  }
+}
+
+void Engine::debug_rows(uint32_t what, double* out) {
+  if (n_ == 0) throw Failure("NoOrientations");
+  if (what > 1) throw Failure("UnknownRows");
+  ZO_CUDA(cudaSetDevice(device_));
+  const int n = (int)n_;
+  Rows r;
+  std::vector<double> extra;
+  std::vector<int> degen;
+  if (what == 0) {
+    sync_neighbourhood();
+    relax_state_.prepare(n, prec_);
+    relax_state_.current = false;
+    relax_state_.record_forces(stream_, prec_, q32(), q64(), n, group_, true, budget_scale_, sms_);
+    r = relax_state_.rows();
+  } else {
+    const PairsPlan pl = plan_pairs(n, (int)order(), budget_scale_, sms_);
+    r = full_rows_.ensure(n);
+    Rows partial{};
+    double* pextra = nullptr;
+    int* pdegen = nullptr;
+    if (pl.chunks > 1) {
+      partial = full_partial_.ensure((size_t)pl.chunks * n);
+      pextra = (double*)full_pextra_.ensure((size_t)pl.chunks * n * 5 * sizeof(double));
+      pdegen = (int*)full_pdegen_.ensure((size_t)pl.chunks * n * sizeof(int));
+    }
+    double* dx = (double*)full_extra_.ensure((size_t)n * 5 * sizeof(double));
+    int* dd = (int*)full_degen_.ensure((size_t)n * sizeof(int));
+    ZO_CUDA(launch_full(prec_, q32(), q64(), n, group_, pl, partial, pextra, pdegen, r, dx, dd, stream_));
+    extra.resize((size_t)n * 5);
+    degen.resize(n);
+    ZO_CUDA(cudaMemcpyAsync(extra.data(), dx, extra.size() * 8, cudaMemcpyDeviceToHost, stream_));
+    ZO_CUDA(cudaMemcpyAsync(degen.data(), dd, degen.size() * 4, cudaMemcpyDeviceToHost, stream_));
+  }
+  std::vector<double4> f(n);
+  std::vector<double> e(n), nb(n);
+  std::vector<int> at(n);
+  ZO_CUDA(cudaMemcpyAsync(f.data(), r.force, (size_t)n * sizeof(double4), cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaMemcpyAsync(e.data(), r.energy, (size_t)n * 8, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaMemcpyAsync(nb.data(), r.nearest, (size_t)n * 8, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaMemcpyAsync(at.data(), r.nearest_at, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  const int width = what == 0 ? 8 : 12;
+  for (int i = 0; i < n; ++i) {
+    double* o = out + (size_t)i * width;
+    o[0] = f[i].x;
+    o[1] = f[i].y;
+    o[2] = f[i].z;
+    o[3] = f[i].w;
+    o[4] = e[i];
+    o[5] = nb[i];
+    if (what == 0) {
+      o[6] = at[i];
+      o[7] = 0;
+    } else {
+      for (int c = 0; c < 5; ++c) o[6 + c] = extra[(size_t)i * 5 + c];
+      o[11] = degen[i];
+    }
+  }
+}
+
+const float* Engine::point_values(uint32_t kind) const {
+  if (kind != 0 || !point_separation_iteration_ || point_separation_.size() != n_) return nullptr;
+  return point_separation_.data();
+}
+const int* Engine::point_neighbours() const {
+  if (!point_separation_iteration_ || point_neighbours_.size() != n_) return nullptr;
+  return point_neighbours_.data();
+}
+
+// ------------------------------------------------------------------ stats JSON
+namespace {
+struct Json {
+  std::string s = "{";
+  bool first = true;
+  void key(const char* k) {
+    if (!first) s += ",";
+    first = false;
+    s += "\"";
+    s += k;
+    s += "\":";
+  }
+  void num(const char* k, double v) {
+    key(k);
+    if (!std::isfinite(v)) {
+      s += "null";
+      return;
+    }
+    char b[64];
+    std::snprintf(b, sizeof b, "%.17g", v);
+    s += b;
+  }
+  void opt(const char* k, std::optional<double> v) {
+    if (v) num(k, *v);
+    else null(k);
+  }
+  void integer(const char* k, long long v) {
+    key(k);
+    s += std::to_string(v);
+  }
+  void str(const char* k, const std::string& v) {
+    key(k);
+    s += "\"";
+    for (char c : v) {
+      if (c == '"' || c == '\\') s += '\\';
+      s += c;
+    }
+    s += "\"";
+  }
+  void boolean(const char* k, bool v) {
+    key(k);
+    s += v ? "true" : "false";
+  }
+  void null(const char* k) {
+    key(k);
+    s += "null";
+  }
+};
+std::optional<double> finite(double v) { return std::isfinite(v) ? std::optional<double>(v) : std::nullopt; }
+}  // namespace
+
+const char* Engine::stats() {
+  const std::optional<Measures>& m = measures_;
+  const bool current = m && measure_iteration_ == iteration_;
+  Json j;
+  j.str("version", kVersion);
+  j.str("group", host_group_name(group_));
+  j.integer("order", order());
+  j.integer("count", n_);
+  j.integer("count_extended", 2ll * order() * n_);
+  j.str("generator", generator_);
+  j.null("grid");
+  j.integer("h", 0);
+  j.integer("seed", seed_);
+  j.integer("iteration", iteration_);
+  j.boolean("fixed_identity", fix_identity_);
+  if (auto idx = identity_index()) j.integer("identity_index", *idx);
+  else j.null("identity_index");
+  j.integer("base_count", n_);
+  j.integer("inserted_count", 0);
+  j.str("triangulation_backend", "none");
+  j.null("covering_radius_deg");
+  j.boolean("covering_current", false);
+  j.null("mesh_ratio");
+  j.null("covering_excess");
+  j.boolean("measured", m.has_value());
+  j.boolean("measures_current", current);
+  if (m) j.integer("measures_iteration", measure_iteration_);
+  else j.null("measures_iteration");
+  j.boolean("energy_ratios_current", full_measures_ && current);
+  if (neighbourhood_ > 0) j.num("relax_neighbourhood", neighbourhood_);
+  else j.null("relax_neighbourhood");
+  if (point_separation_iteration_) j.integer("point_separation_iteration", *point_separation_iteration_);
+  else j.null("point_separation_iteration");
+  j.null("point_covering_iteration");
+  if (m && measure_neighbourhood_ > 0) j.num("energy_neighbourhood", measure_neighbourhood_);
+  else j.null("energy_neighbourhood");
+  j.integer("ratio_limit", ratio_limit());
+  const char* precision = !m                          ? "Not measured"
+                          : !current                  ? "Energy and separation from an earlier iteration"
+                          : !std::isfinite(m->quey_energy) ? "Separation current; energy not measured"
+                          : full_measures_            ? "All measures current"
+                          : n_ > ratio_limit()        ? "Energy and separation current; this sample exceeds the ratio limit"
+                                                      : "Energy and separation current; refresh energy ratios";
+  j.str("precision", precision);
+  j.opt("energy", m ? finite(m->quey_energy) : std::nullopt);
+  j.opt("quey_energy", m ? finite(m->quey_energy) : std::nullopt);
+  j.opt("riesz_1", m ? finite(m->riesz_1) : std::nullopt);
+  j.opt("riesz_2", m ? finite(m->riesz_2) : std::nullopt);
+  j.opt("riesz_3", m ? finite(m->riesz_3) : std::nullopt);
+  j.opt("green_ratio", m ? finite(m->green_ratio) : std::nullopt);
+  j.opt("log_ratio", m ? finite(m->log_ratio) : std::nullopt);
+  j.opt("separation_deg", m ? finite(m->separation_deg) : std::nullopt);
+  j.num("step_deg", step_deg_);
+  j.opt("force_rms", m ? finite(m->force_rms) : finite(force_rms_));
+  j.str("arithmetic", prec_ == kFP64 ? "fp64" : "fp32-refined");
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device_) == cudaSuccess) j.str("adapter", prop.name);
+  j.s += "}";
+  text_ = j.s;
+  return text_.c_str();
+}
+
+}  // namespace zo

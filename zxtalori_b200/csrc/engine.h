@@ -1,0 +1,206 @@
+// The engine behind the zo_* C ABI: one orientation sample resident on one GPU, with the
+// reference's relaxation, measure and spacing policies (src/engine.zig:17-1021,
+// src/pairs.zig:217-413, src/near.zig:31-196).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <limits>
+#include <memory>
+#include <optional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+namespace zo {
+
+const char* host_group_name(int gid);
+const float* host_ops32(int gid);
+
+// An error carrying the reference's error name (src/exports.zig prefixes it).
+struct Failure : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void check_cuda(cudaError_t e, const char* what);
+#define ZO_CUDA(expr) ::zo::check_cuda((expr), #expr)
+
+// Device allocation that only grows; contents are not preserved across growth.
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { release(); }
+  void* ensure(size_t bytes);
+  void release();
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr_); }
+  size_t bytes() const { return bytes_; }
+
+ private:
+  void* ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+struct Measures {
+  double count_extended = 0;
+  double riesz_1 = NAN, riesz_2 = NAN, riesz_3 = NAN, green_ratio = NAN, log_ratio = NAN;
+  double quey_energy = NAN, separation_deg = NAN, force_rms = NAN;
+};
+
+struct StepResult {
+  double max_step_deg = 0, force_rms = 0, energy = 0;
+};
+
+// Rows of n sources in one set of device buffers.
+struct RowBuffers {
+  DeviceBuffer force, energy, nearest, nearest_at;
+  Rows ensure(size_t n);
+  Rows rows() const { return Rows{force.as<double4>(), energy.as<double>(), nearest.as<double>(), nearest_at.as<int>()}; }
+};
+
+// Near-field workspace (src/near.zig:31-196): sized by one shell pass, then reused.
+class NearField {
+ public:
+  NearField(int gid, double delta) : gid_(gid), delta_(delta) {}
+  int gid() const { return gid_; }
+  double delta() const { return delta_; }
+  double radius() const { return radius_; }
+  // Records a pass writing rows of q into `out`.
+  void pass(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_radius, bool track,
+            Rows out, int sms);
+  // Whether the last pass produced more sites than the workspace holds (after a sync);
+  // the next pass sizes it again.
+  bool overflowed(cudaStream_t s);
+  const uint32_t* sorted_codes() const { return scode_.as<uint32_t>(); }
+  const uint32_t* sorted_images() const { return simg_.as<uint32_t>(); }
+  int capacity() const { return capacity_; }
+  int slices() const { return slices_; }
+
+ private:
+  void setup(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_radius, int sms);
+  int gid_;
+  double delta_;
+  double taper_ = 0.5;
+  bool ready_ = false;
+  int n_ = 0, prec_ = -1, capacity_ = 0, sdim_max_ = 1, slices_ = 1;
+  double radius_ = 0, s_margin_ = 0, chord_ = 0;
+  DeviceBuffer counts_, offsets_, scan_tmp_, site_q_, site_code_, site_img_, site_cell_, site_rank_, site_pos_;
+  DeviceBuffer cell_count_, cell_off_, perm_, sq_, scode_, simg_, src_key_, src_rank_, mcount_, moff_, src_perm_;
+  DeviceBuffer grid_, cells_;
+  RowBuffers partial_;
+};
+
+// BB relaxation state (src/pairs.zig:220-413): rows of the current positions, the previous
+// force and move per source, and the device-resident step state.
+class RelaxState {
+ public:
+  void reset();
+  void set_near(int gid, std::optional<double> delta);
+  bool near() const { return near_ != nullptr; }
+  std::optional<double> near_delta() const {
+    return near_ ? std::optional<double>(near_->delta()) : std::nullopt;
+  }
+  Rows rows() const { return rows_.rows(); }
+  bool current = false;
+
+  void prepare(int n, int prec);
+  void record_forces(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, int gid, bool track,
+                     double budget_scale, int sms);
+  void step(cudaStream_t s, int prec, float4* q32, double4* q64, int n, int gid, int fixed, double budget_scale, int sms);
+  StepResult finish(cudaStream_t s);
+  // Quick measures of `rows()` (after a force pass), nearest degrees and neighbours to host.
+  Measures summarize(cudaStream_t s, int n, int order, float* degrees, int* neighbours, int prec, const float4* q32,
+                     int gid);
+  bool near_overflowed(cudaStream_t s) { return near_ && near_->overflowed(s); }
+  NearField* near_field() { return near_.get(); }
+
+ private:
+  StepResult step_result(const RelaxDev& st) const;
+  int n_ = 0, prec_ = -1, order_ = 0;
+  RowBuffers rows_, partial_;
+  DeviceBuffer prev_f_, prev_d_, state_, stats_partials_, hist_, summary_, summary_partials_, near_partials_,
+      near_rows_, degrees_, neighbours_;
+  std::unique_ptr<NearField> near_;
+};
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+  // Reference entry points (src/engine.zig). Each throws Failure on error.
+  void set(int gid, const float* values, size_t count);
+  void generate_random(int gid, uint32_t count, uint32_t seed);
+  void generate_grid(int gid, uint32_t freq, uint32_t target, uint32_t seed, uint32_t kind);
+  void measure();
+  void spacing();
+  void relax(uint32_t steps);
+  void set_neighbourhood(double delta);
+  void identity(bool add, bool fixed);
+  const char* stats();
+  const float* point_values(uint32_t kind) const;
+  const int* point_neighbours() const;
+  void cancel() { cancelled_.store(true); }
+  // Extensions.
+  void set_precision(int prec);
+  int precision() const { return prec_; }
+  void set_pair_budget(double scale) { budget_scale_ = scale; }
+  // Development: one pass's raw rows to host. what 0: force pass of the relaxation
+  // (8 doubles per source), 1: full measure rows (12 doubles per source).
+  void debug_rows(uint32_t what, double* out);
+
+  int group() const { return group_; }
+  uint32_t count() const { return n_; }
+  uint32_t order() const { return (uint32_t)host_group_order(group_); }
+  const float* quaternions() const { return host_.data(); }
+  uint32_t ratio_limit() const;
+  char err[2048] = {0};
+
+ private:
+  void adopt(uint32_t n);
+  void reset_run();
+  void sync_neighbourhood();
+  void fetch();
+  Measures full_measure();
+  Measures relax_state_measure();
+  int fixed_arg() const { return fixed_index_ ? (int)*fixed_index_ : -1; }
+  std::optional<uint32_t> identity_index() const;
+  float4* q32() { return q32_.as<float4>(); }
+  double4* q64() { return prec_ == kFP64 ? q64_.as<double4>() : nullptr; }
+
+  int device_ = 0, sms_ = 148;
+  cudaStream_t stream_ = nullptr;
+  int group_ = 9;
+  int prec_ = kFP32;
+  uint32_t n_ = 0;
+  DeviceBuffer q32_, q64_;
+  std::vector<float> host_;
+  uint32_t iteration_ = 0;
+  uint32_t seed_ = 0;
+  std::string generator_ = "none";
+  std::optional<Measures> measures_;
+  uint32_t measure_iteration_ = 0;
+  bool full_measures_ = false;
+  RelaxState relax_state_, spacing_state_;
+  double neighbourhood_ = 0, measure_neighbourhood_ = 0;
+  std::vector<float> point_separation_;
+  std::vector<int> point_neighbours_;
+  std::optional<uint32_t> point_separation_iteration_;
+  double step_deg_ = 0, force_rms_ = 0;
+  std::atomic<bool> cancelled_{false};
+  bool fix_identity_ = false;
+  std::optional<uint32_t> fixed_index_;
+  double budget_scale_ = 1.0;
+  // Full-measure scratch.
+  RowBuffers full_rows_, full_partial_;
+  DeviceBuffer full_extra_, full_pextra_, full_degen_, full_pdegen_;
+  std::string text_;
+};
+
+double mean_radius(double count);
+
+}  // namespace zo

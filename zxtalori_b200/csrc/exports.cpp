@@ -1,0 +1,155 @@
+// extern "C" entry points: the reference's zo_* ABI (src/exports.zig, src/native_api.zig),
+// bound by ctypes from Python (python/zxtalori/api.py:29-50). 0 is success, -1 failure with
+// the message in the engine's 2,048-byte error buffer, prefixed as the reference does.
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <new>
+
+#include "engine.h"
+#include "zxtalori.h"
+
+using zo::Engine;
+
+namespace {
+char g_create_error[1024] = {0};
+
+template <class F>
+int guarded(void* h, const char* prefix, F&& f) {
+  Engine* e = static_cast<Engine*>(h);
+  try {
+    f(*e);
+    return 0;
+  } catch (const std::exception& x) {
+    std::snprintf(e->err, sizeof e->err, "%s: %s", prefix, x.what());
+    return -1;
+  }
+}
+
+int fail(void* h, const char* message) {
+  Engine* e = static_cast<Engine*>(h);
+  std::snprintf(e->err, sizeof e->err, "%s", message);
+  return -1;
+}
+
+// Covering, meshes and exact-count generation are outside this engine.
+const char* kNoCovering = "covering radius, triangulation and covering optimisation are not part of this engine";
+}  // namespace
+
+extern "C" {
+
+const char* zo_version(void) { return "0.3.0"; }
+
+void* zo_create(const char* wgpu_dir) {
+  (void)wgpu_dir;
+  try {
+    return new Engine();
+  } catch (const std::exception& x) {
+    std::snprintf(g_create_error, sizeof g_create_error, "GPU init: %s", x.what());
+    return nullptr;
+  }
+}
+
+const char* zo_create_error(void) { return g_create_error; }
+
+void zo_destroy(void* h) { delete static_cast<Engine*>(h); }
+
+int zo_generate(void* h, uint32_t group, uint32_t freq, uint32_t target, uint32_t seed, uint32_t kind) {
+  if (group >= 11) return fail(h, "Unknown group");
+  if (kind > 2) return fail(h, "Unknown grid kind");
+  return guarded(h, "Generation failed", [&](Engine& e) { e.generate_grid((int)group, freq, target, seed, kind); });
+}
+
+int zo_generate_exact(void* h, uint32_t group, uint32_t target, uint32_t flags) {
+  (void)target;
+  (void)flags;
+  if (group >= 11) return fail(h, "Unknown group");
+  return fail(h, "Exact-count generation: InsertionNotAvailable");
+}
+
+int zo_random(void* h, uint32_t group, uint32_t count, uint32_t seed) {
+  if (group >= 11) return fail(h, "Unknown group");
+  return guarded(h, "Haar initialization", [&](Engine& e) { e.generate_random((int)group, count, seed); });
+}
+
+int zo_set(void* h, uint32_t group, const float* q, uint32_t n) {
+  if (group >= 11) return fail(h, "Unknown group");
+  return guarded(h, "Import failed", [&](Engine& e) {
+    if (n > 0 && !q) throw zo::Failure("InvalidCount");
+    e.set((int)group, q, n);
+  });
+}
+
+uint32_t zo_count(void* h) { return static_cast<Engine*>(h)->count(); }
+uint32_t zo_order(void* h) { return static_cast<Engine*>(h)->order(); }
+const float* zo_quaternions(void* h) { return static_cast<Engine*>(h)->quaternions(); }
+const float* zo_operations(void* h) { return zo::host_ops32(static_cast<Engine*>(h)->group()); }
+
+int zo_measure(void* h) { return guarded(h, "Measure failed", [](Engine& e) { e.measure(); }); }
+int zo_spacing(void* h) { return guarded(h, "Spacing failed", [](Engine& e) { e.spacing(); }); }
+int zo_relax(void* h, uint32_t steps) { return guarded(h, "Relaxation failed", [&](Engine& e) { e.relax(steps); }); }
+
+int zo_relax_neighbourhood(void* h, float delta) {
+  return guarded(h, "Relaxation neighbourhood", [&](Engine& e) { e.set_neighbourhood((double)delta); });
+}
+
+const float* zo_point_values(void* h, uint32_t kind) { return static_cast<Engine*>(h)->point_values(kind); }
+
+int zo_identity(void* h, uint32_t flags) {
+  return guarded(h, "Identity constraint", [&](Engine& e) { e.identity((flags & 1u) != 0, (flags & 2u) != 0); });
+}
+
+int zo_cover(void* h) { return fail(h, (std::string("Covering radius: ") + kNoCovering).c_str()); }
+int zo_cover_optimize(void* h, uint32_t steps, uint32_t mode, uint32_t finish, float floor_deg) {
+  (void)steps, (void)mode, (void)finish, (void)floor_deg;
+  return fail(h, (std::string("Covering optimization: ") + kNoCovering).c_str());
+}
+int zo_cover_kicks(void* h, uint32_t patience, float progress, float size, float trust) {
+  (void)patience, (void)progress, (void)size, (void)trust;
+  return fail(h, (std::string("Covering kicks: ") + kNoCovering).c_str());
+}
+int zo_mesh(void* h) { return fail(h, (std::string("DT display: ") + kNoCovering).c_str()); }
+const float* zo_mesh_vertices(void* h) {
+  (void)h;
+  return nullptr;
+}
+const uint32_t* zo_mesh_tets(void* h) {
+  (void)h;
+  return nullptr;
+}
+uint32_t zo_mesh_vertex_count(void* h) {
+  (void)h;
+  return 0;
+}
+uint32_t zo_mesh_tet_count(void* h) {
+  (void)h;
+  return 0;
+}
+
+const char* zo_stats(void* h) { return static_cast<Engine*>(h)->stats(); }
+const char* zo_error(void* h) { return static_cast<Engine*>(h)->err; }
+void zo_cancel(void* h) { static_cast<Engine*>(h)->cancel(); }
+
+void zo_pair_budget(void* h, float scale) { static_cast<Engine*>(h)->set_pair_budget((double)scale); }
+bool zo_profile(void* h, bool enabled) {
+  (void)h;
+  (void)enabled;
+  return false;
+}
+size_t zo_profile_report(void* h, uint8_t* output, size_t capacity) {
+  (void)h;
+  if (output && capacity) output[0] = 0;
+  return 0;
+}
+
+int zo_precision(void* h, uint32_t mode) {
+  return guarded(h, "Precision", [&](Engine& e) { e.set_precision((int)mode); });
+}
+uint32_t zo_get_precision(void* h) { return (uint32_t) static_cast<Engine*>(h)->precision(); }
+const int32_t* zo_point_neighbours(void* h) { return static_cast<Engine*>(h)->point_neighbours(); }
+
+int zo_debug_rows(void* h, uint32_t what, double* out) {
+  return guarded(h, "Rows", [&](Engine& e) { e.debug_rows(what, out); });
+}
+
+}  // extern "C"

@@ -1,0 +1,549 @@
+// Near-field force pass (src/near.zig, shaders/near.wgsl, shaders/shell.wgsl:18-130,
+// shaders/pairs.wgsl:328-427).
+//
+// A source in the zone only feels orbit points within S3 angle r of it, and those lie within
+// r of the zone. Per pass:
+//   1. shell: every source's identity image, and for sources near a zone plane ("rim") each
+//      image (operator, sign) inside every bisector half-space widened by sin(r + 1e-4);
+//      counted, scanned and written in (source, image) order - deterministic sites;
+//   2. the sites' stereographic chart box, a grid of sdim^3 cells, a counting sort of the
+//      sites into row-major cells with each cell ordered by site index;
+//   3. sources counting-sorted into a 32^3 Morton grid (then by index), so 32 consecutive
+//      sources are close together;
+//   4. one warp per 32 sources and slice: the warp's chart box, the cell rows within the
+//      chart reach of the cutoff chord, each row's x-run trimmed; runs stream through shared
+//      memory 32 sites at a time and every lane tests its source against each site;
+//   5. the slices' partial rows summed in slice order into each source's row.
+// Nothing is read back between passes: grid parameters live in device memory.
+#pragma once
+#include "k_common.cuh"
+#include "kernels.h"
+
+namespace zo {
+
+// ------------------------------------------------------------------ 1. shell
+// Whether image q (of the normalised source `orig`) lies inside every widened bisector
+// half-space (shell.wgsl:19-22; the rim test is done by the caller).
+__device__ __forceinline__ bool inside_planes(double4 q, int poff, int planes, bool fp64, double margin) {
+  for (int k = 0; k < planes; ++k) {
+    const double4 h = fp64 ? c_planes64[poff + k] : to_d4(c_planes32[poff + k]);
+    if (dot4(q, h) < -margin) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ bool on_rim(double4 orig, int poff, int planes, bool fp64, double margin) {
+  for (int k = 0; k < planes; ++k) {
+    const double4 h = fp64 ? c_planes64[poff + k] : to_d4(c_planes32[poff + k]);
+    if (dot4(orig, h) <= margin) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ double4 source_d(const float4* q32, const double4* q64, int j, bool fp64) {
+  return fp64 ? q64[j] : to_d4(q32[j]);
+}
+
+// Classification image of (source, operator k, sign): normalize(orig * normalize(g_k)), negated.
+__device__ __forceinline__ double4 shell_image(double4 orig, int op_row, bool neg, bool fp64) {
+  const double4 g = normalize4(fp64 ? c_ops64[op_row] : c_ops32[op_row]);
+  double4 c = normalize4(qmul(orig, g));
+  return neg ? neg4(c) : c;
+}
+
+__global__ void k_shell_count(const float4* __restrict__ q32, const double4* __restrict__ q64, int n, int gid, int fp64i,
+                              double s_margin, uint32_t* __restrict__ counts) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const bool fp64 = fp64i != 0;
+  const int off = c_group_offset[gid], order = c_group_order[gid];
+  const int poff = c_plane_offset[gid], planes = 2 * order - 1;
+  const double4 orig = normalize4(source_d(q32, q64, j, fp64));
+  uint32_t c = 1;  // the identity image (a core site)
+  if (on_rim(orig, poff, planes, fp64, s_margin + 2e-6)) {
+    for (int img = 1; img < 2 * order; ++img) {
+      const double4 y = shell_image(orig, off + img / 2, img & 1, fp64);
+      if (y.x > -0.9999999 && inside_planes(y, poff, planes, fp64, s_margin + 2e-6)) ++c;
+    }
+  }
+  counts[j] = c;
+}
+
+// Writes the sites of each source at its scanned offset: the rebuilt image quaternion
+// (pairs.wgsl:181 / near.wgsl:263-269), its code (source, high bit for the identity
+// image), its image number 2*operator+sign, and its chart position; plus the chart box.
+template <bool FP64>
+__global__ void __launch_bounds__(256) k_shell_write(const float4* __restrict__ q32, const double4* __restrict__ q64,
+                                                     int n, int gid, double s_margin,
+                                                     const uint32_t* __restrict__ offsets, int capacity,
+                                                     float4* __restrict__ site_q32, double4* __restrict__ site_q64,
+                                                     uint32_t* __restrict__ site_code, uint32_t* __restrict__ site_img,
+                                                     float4* __restrict__ site_pos, NearGrid* grid) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+  bool overflow = false;
+  if (j < n) {
+    const int off = c_group_offset[gid], order = c_group_order[gid];
+    const int poff = c_plane_offset[gid], planes = 2 * order - 1;
+    const double4 src = source_d(q32, q64, j, FP64);
+    const double4 orig = normalize4(src);
+    uint32_t at = offsets[j];
+    auto emit = [&](double4 cls, int img, bool identity) {
+      if ((int)at >= capacity) {
+        overflow = true;
+        return;
+      }
+      const float3 p = chart(cls);
+      if (FP64) {
+        double4 y = identity ? src : (img / 2 == 0 ? src : normalize4(qmul(src, c_ops64[off + img / 2])));
+        site_q64[at] = (img & 1) ? neg4(y) : y;
+      } else {
+        const float4 s = q32[j];
+        float4 y = (img / 2 == 0) ? s : to_f4(normalize4(qmul(to_d4(s), c_ops32[off + img / 2])));
+        if (img & 1) y = make_float4(-y.x, -y.y, -y.z, -y.w);
+        site_q32[at] = y;
+      }
+      site_code[at] = (uint32_t)j | (identity ? kIdentityBit : 0u);
+      site_img[at] = (uint32_t)img;
+      site_pos[at] = make_float4(p.x, p.y, p.z, 0.f);
+      lo[0] = fminf(lo[0], p.x);
+      lo[1] = fminf(lo[1], p.y);
+      lo[2] = fminf(lo[2], p.z);
+      hi[0] = fmaxf(hi[0], p.x);
+      hi[1] = fmaxf(hi[1], p.y);
+      hi[2] = fmaxf(hi[2], p.z);
+      ++at;
+    };
+    emit(orig, 0, true);
+    if (on_rim(orig, poff, planes, FP64, s_margin + 2e-6)) {
+      for (int img = 1; img < 2 * order; ++img) {
+        const double4 y = shell_image(orig, off + img / 2, img & 1, FP64);
+        if (y.x > -0.9999999 && inside_planes(y, poff, planes, FP64, s_margin + 2e-6)) emit(y, img, false);
+      }
+    }
+  }
+  // Block-reduce the box, then one atomic per block and axis.
+  __shared__ float red[6][8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int a = 0; a < 3; ++a) {
+    const float l = warp_min(lo[a]), h = warp_max(hi[a]);
+    if (lane == 0) {
+      red[a][w] = l;
+      red[3 + a][w] = h;
+    }
+  }
+  const int any_overflow = __syncthreads_or(overflow);
+  if (threadIdx.x < 3) {
+    float l = red[threadIdx.x][0], h = red[3 + threadIdx.x][0];
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+      l = fminf(l, red[threadIdx.x][k]);
+      h = fmaxf(h, red[3 + threadIdx.x][k]);
+    }
+    if (l <= h) {
+      atomicMin(&grid->box_bits[threadIdx.x], ordered_bits(l));
+      atomicMax(&grid->box_bits[3 + threadIdx.x], ordered_bits(h));
+    }
+  }
+  if (threadIdx.x == 0 && any_overflow) atomicOr(&grid->overflow, 1u);
+}
+
+// ------------------------------------------------------------------ 2. grid and site sort
+// Chart grid from the box (near.zig:124-137): a 5% margin, width 1.1x the largest extent,
+// sdim = clamp(round(cbrt(sites/8)), 1, sdim_max). The box is reset for the next pass.
+__global__ void k_grid_setup(NearGrid* g, const uint32_t* __restrict__ total, int capacity, int sdim_max,
+                             int* __restrict__ cells) {
+  const uint32_t s = *total;
+  g->sites = (int)min((uint32_t)capacity, s);
+  if (s > (uint32_t)capacity) g->overflow = 1u;
+  float lo[3], hi[3];
+  float width = 1e-6f;
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = unordered_bits(g->box_bits[a]);
+    hi[a] = unordered_bits(g->box_bits[3 + a]);
+    if (!(hi[a] >= lo[a])) lo[a] = hi[a] = 0.f;
+    width = fmaxf(width, hi[a] - lo[a]);
+  }
+  for (int a = 0; a < 3; ++a) g->lower[a] = lo[a] - 0.05f * width;
+  width *= 1.1f;
+  int sdim = (int)rint(cbrt((double)g->sites / 8.0));
+  sdim = max(1, min(sdim, sdim_max));
+  g->width = width;
+  g->sdim = sdim;
+  g->cells_per_unit = (float)sdim / width;
+  g->morton_per_unit = (float)kMortonDim / width;
+  *cells = sdim * sdim * sdim;
+  for (int a = 0; a < 3; ++a) {
+    g->box_bits[a] = 0xffffffffu;
+    g->box_bits[3 + a] = 0u;
+  }
+}
+
+__device__ __forceinline__ int cell_axis(float v, float lower, float per_unit, int dim) {
+  const float c = floorf((v - lower) * per_unit);
+  return (int)fminf(fmaxf(c, 0.f), (float)(dim - 1));
+}
+
+__global__ void k_cell_count(const float4* __restrict__ pos, const NearGrid* __restrict__ gp, uint32_t* __restrict__ cell,
+                             uint32_t* __restrict__ rank, uint32_t* __restrict__ counts) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= gp->sites) return;
+  const float4 p = pos[s];
+  const int d = gp->sdim;
+  const float u = gp->cells_per_unit;
+  const int c = cell_axis(p.x, gp->lower[0], u, d) + d * (cell_axis(p.y, gp->lower[1], u, d) + d * cell_axis(p.z, gp->lower[2], u, d));
+  cell[s] = (uint32_t)c;
+  rank[s] = atomicAdd(&counts[c], 1u);
+}
+
+__global__ void k_scatter(const uint32_t* __restrict__ key, const uint32_t* __restrict__ rank,
+                          const uint32_t* __restrict__ offsets, int max_items, const int* __restrict__ items,
+                          uint32_t* __restrict__ perm) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int count = items ? min(*items, max_items) : max_items;
+  if (s >= count) return;
+  perm[offsets[key[s]] + rank[s]] = (uint32_t)s;
+}
+
+// Each bucket's items in index order (near.wgsl:270-282), so every pass sums in the same
+// order. Insertion sort; buckets hold a handful of items on average.
+__global__ void k_bucket_sort(const uint32_t* __restrict__ offsets, int max_buckets, const int* __restrict__ buckets,
+                              uint32_t* __restrict__ perm) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int count = buckets ? min(*buckets, max_buckets) : max_buckets;
+  if (b >= count) return;
+  const uint32_t begin = offsets[b], end = offsets[b + 1];
+  for (uint32_t at = begin + 1; at < end; ++at) {
+    const uint32_t v = perm[at];
+    uint32_t k = at;
+    while (k > begin && perm[k - 1] > v) {
+      perm[k] = perm[k - 1];
+      --k;
+    }
+    perm[k] = v;
+  }
+}
+
+template <bool FP64>
+__global__ void k_site_gather(const uint32_t* __restrict__ perm, const NearGrid* __restrict__ gp,
+                              const float4* __restrict__ q32, const double4* __restrict__ q64,
+                              const uint32_t* __restrict__ code, const uint32_t* __restrict__ img,
+                              float4* __restrict__ sq32, double4* __restrict__ sq64, uint32_t* __restrict__ scode,
+                              uint32_t* __restrict__ simg) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= gp->sites) return;
+  const uint32_t s = perm[p];
+  if (FP64) sq64[p] = q64[s];
+  else sq32[p] = q32[s];
+  scode[p] = code[s];
+  simg[p] = img[s];
+}
+
+// ------------------------------------------------------------------ 3. sources in Morton order
+__device__ __forceinline__ uint32_t spread5(uint32_t v) {
+  uint32_t x = v & 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  return (x | (x << 2)) & 0x09249249u;
+}
+
+template <bool FP64>
+__global__ void k_source_count(const float4* __restrict__ q32, const double4* __restrict__ q64, int n,
+                               const NearGrid* __restrict__ gp, uint32_t* __restrict__ code,
+                               uint32_t* __restrict__ rank, uint32_t* __restrict__ counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float3 p = FP64 ? chart(q64[i]) : chart(q32[i]);
+  const float u = gp->morton_per_unit;
+  const uint32_t cx = cell_axis(p.x, gp->lower[0], u, kMortonDim), cy = cell_axis(p.y, gp->lower[1], u, kMortonDim),
+                 cz = cell_axis(p.z, gp->lower[2], u, kMortonDim);
+  const uint32_t m = spread5(cx) | (spread5(cy) << 1) | (spread5(cz) << 2);
+  code[i] = m;
+  rank[i] = atomicAdd(&counts[m], 1u);
+}
+
+// ------------------------------------------------------------------ 4. the gather
+struct NearCut {
+  double cut2, chord, cut_z, cut_w;
+};
+
+constexpr int kNearWarps = 4;
+
+struct WarpBox {
+  float lo[3], hi[3];
+  int clo[3], chi[3];
+  float d;
+};
+
+// The warp's chart box and the cells within chart reach d of it (pairs.wgsl:368-379):
+// chart distance = chord/2 sqrt((1+|p|^2)(1+|p'|^2)), bounded by fixed-point iteration.
+__device__ __forceinline__ bool warp_box(float3 pos, bool live, const NearGrid& g, float chord, WarpBox& b) {
+  float v[6] = {live ? pos.x : 3e38f, live ? pos.y : 3e38f, live ? pos.z : 3e38f,
+                live ? pos.x : -3e38f, live ? pos.y : -3e38f, live ? pos.z : -3e38f};
+  for (int a = 0; a < 3; ++a) {
+    b.lo[a] = warp_min(v[a]);
+    b.hi[a] = warp_max(v[3 + a]);
+  }
+  if (!(b.lo[0] <= b.hi[0])) return false;
+  float r2 = 0.f;
+  for (int a = 0; a < 3; ++a) {
+    const float m = fmaxf(fabsf(b.lo[a]), fabsf(b.hi[a]));
+    r2 += m * m;
+  }
+  const float reach = sqrtf(r2), lift = 1.0f + reach * reach;
+  float d = 0.5f * chord * lift;
+  for (int k = 0; k < 4; ++k) d = 0.5f * chord * sqrtf(lift * (1.0f + (reach + d) * (reach + d)));
+  d = d * 1.01f + 1e-6f;
+  b.d = d;
+  for (int a = 0; a < 3; ++a) {
+    b.clo[a] = cell_axis(b.lo[a] - d, g.lower[a], g.cells_per_unit, g.sdim);
+    b.chi[a] = cell_axis(b.hi[a] + d, g.lower[a], g.cells_per_unit, g.sdim);
+  }
+  return true;
+}
+
+// Row r of the warp's (y, z) cell rows: the run of sorted sites of its x cells within reach.
+__device__ __forceinline__ bool row_run(const WarpBox& b, const NearGrid& g, const uint32_t* cell_off, int r,
+                                        uint32_t& start, uint32_t& end) {
+  const int ny = b.chi[1] - b.clo[1] + 1;
+  const int y = b.clo[1] + r % ny, z = b.clo[2] + r / ny;
+  const float width = 1.0f / g.cells_per_unit;
+  const float cy = g.lower[1] + (float)y * width, cz = g.lower[2] + (float)z * width;
+  const float gy = fmaxf(0.f, fmaxf(cy - b.hi[1], b.lo[1] - (cy + width)));
+  const float gz = fmaxf(0.f, fmaxf(cz - b.hi[2], b.lo[2] - (cz + width)));
+  const float rest = b.d * b.d - gy * gy - gz * gz;
+  if (rest < 0.f) return false;
+  const float span = sqrtf(rest);
+  const int x0 = cell_axis(b.lo[0] - span, g.lower[0], g.cells_per_unit, g.sdim);
+  const int x1 = cell_axis(b.hi[0] + span, g.lower[0], g.cells_per_unit, g.sdim);
+  const int row = g.sdim * (y + g.sdim * z);
+  start = cell_off[row + x0];
+  end = cell_off[row + x1 + 1];
+  return start < end;
+}
+
+template <bool TRACK>
+__global__ void __launch_bounds__(kNearWarps * 32) k_near32(const float4* __restrict__ q, int n,
+                                                              const uint32_t* __restrict__ src_perm,
+                                                              const float4* __restrict__ sq,
+                                                              const uint32_t* __restrict__ scode,
+                                                              const uint32_t* __restrict__ cell_off,
+                                                              const NearGrid* __restrict__ gp, NearCut cut, int slices,
+                                                              Rows out, int stride) {
+  __shared__ float4 tq[kNearWarps][32];
+  __shared__ uint32_t tc[kNearWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int warp = blockIdx.x * kNearWarps + w;
+  const int slice = blockIdx.y;
+  if (warp * 32 >= n) return;
+  const int p = warp * 32 + lane;
+  const bool live = p < n;
+  const uint32_t i = live ? src_perm[p] : 0u;
+  const float4 x = q[i];
+  const NearGrid g = *gp;
+  WarpBox box;
+  if (!warp_box(chart(x), live, g, (float)cut.chord, box)) return;
+  const float cut2 = (float)cut.cut2, cz = (float)cut.cut_z, cw = (float)cut.cut_w;
+  double f1 = 0, f2 = 0, f3 = 0, fc = 0, fe = 0;
+  float best = 4.0f;
+  int best_at = -1;
+  const int ny = box.chi[1] - box.clo[1] + 1, nz = box.chi[2] - box.clo[2] + 1;
+  const int rows = ny * nz;
+  for (int r = slice; r < rows; r += slices) {
+    uint32_t start, end;
+    if (!row_run(box, g, cell_off, r, start, end)) continue;
+    for (uint32_t base = start; base < end; base += 32) {
+      const int count = (int)min(32u, end - base);
+      __syncwarp();
+      if (lane < count) {
+        tq[w][lane] = sq[base + lane];
+        tc[w][lane] = scode[base + lane];
+      }
+      __syncwarp();
+      if (!live) continue;
+      float s1 = 0.f, s2 = 0.f, s3 = 0.f, sc = 0.f, se = 0.f;
+      for (int t = 0; t < count; ++t) {
+        const float4 y = tq[w][t];
+        const float mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
+        const float dm2 = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
+        if (dm2 > cut2) continue;
+        const uint32_t code = tc[w][t];
+        if ((code & ~kIdentityBit) == i) {
+          if (code == i && dm2 < best) {
+            best = dm2;
+            if (TRACK) best_at = (int)(base + t);
+          }
+          continue;
+        }
+        if (dm2 < best) {
+          best = dm2;
+          if (TRACK) best_at = (int)(base + t);
+        }
+        const float pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
+        const float dp2 = fmaf(pw, pw, fmaf(px, px, fmaf(py, py, pz * pz)));
+        PairF pr = quey_pair32(dm2, dp2);
+        window32(pr, dm2, dp2, cz, cw);
+        float d1, d2, d3;
+        pair_direction(x, y, d1, d2, d3);
+        s1 = fmaf(pr.coef, d1, s1);
+        s2 = fmaf(pr.coef, d2, s2);
+        s3 = fmaf(pr.coef, d3, s3);
+        sc += pr.curv;
+        se += pr.energy;
+      }
+      f1 += s1;
+      f2 += s2;
+      f3 += s3;
+      fc += sc;
+      fe += se;
+    }
+  }
+  if (!live) return;
+  const size_t at = (size_t)slice * stride + p;
+  out.force[at] = make_double4(f1, f2, f3, fc);
+  out.energy[at] = fe;
+  out.nearest[at] = best;
+  if (TRACK) out.nearest_at[at] = best_at;
+}
+
+template <bool TRACK>
+__global__ void __launch_bounds__(kNearWarps * 32) k_near64(const double4* __restrict__ q, int n,
+                                                              const uint32_t* __restrict__ src_perm,
+                                                              const double4* __restrict__ sq,
+                                                              const uint32_t* __restrict__ scode,
+                                                              const uint32_t* __restrict__ cell_off,
+                                                              const NearGrid* __restrict__ gp, NearCut cut, int slices,
+                                                              Rows out, int stride) {
+  __shared__ double4 tq[kNearWarps][32];
+  __shared__ uint32_t tc[kNearWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int warp = blockIdx.x * kNearWarps + w;
+  const int slice = blockIdx.y;
+  if (warp * 32 >= n) return;
+  const int p = warp * 32 + lane;
+  const bool live = p < n;
+  const uint32_t i = live ? src_perm[p] : 0u;
+  const double4 x = q[i];
+  const NearGrid g = *gp;
+  WarpBox box;
+  if (!warp_box(chart(x), live, g, (float)cut.chord, box)) return;
+  double f1 = 0, f2 = 0, f3 = 0, fc = 0, fe = 0, best = 4.0;
+  int best_at = -1;
+  const int ny = box.chi[1] - box.clo[1] + 1, nz = box.chi[2] - box.clo[2] + 1;
+  const int rows = ny * nz;
+  for (int r = slice; r < rows; r += slices) {
+    uint32_t start, end;
+    if (!row_run(box, g, cell_off, r, start, end)) continue;
+    for (uint32_t base = start; base < end; base += 32) {
+      const int count = (int)min(32u, end - base);
+      __syncwarp();
+      if (lane < count) {
+        tq[w][lane] = sq[base + lane];
+        tc[w][lane] = scode[base + lane];
+      }
+      __syncwarp();
+      if (!live) continue;
+      for (int t = 0; t < count; ++t) {
+        const double4 y = tq[w][t];
+        const double mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
+        const double dm2 = mw * mw + mx * mx + my * my + mz * mz;
+        if (dm2 > cut.cut2) continue;
+        const uint32_t code = tc[w][t];
+        if ((code & ~kIdentityBit) == i) {
+          if (code == i && dm2 < best) {
+            best = dm2;
+            if (TRACK) best_at = (int)(base + t);
+          }
+          continue;
+        }
+        if (dm2 < best) {
+          best = dm2;
+          if (TRACK) best_at = (int)(base + t);
+        }
+        const double pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
+        const double dp2 = pw * pw + px * px + py * py + pz * pz;
+        PairD pr = quey_pair64(dm2, dp2);
+        window64(pr, dm2, dp2, cut.cut_z, cut.cut_w);
+        double d1, d2, d3;
+        pair_direction(x, y, d1, d2, d3);
+        f1 += pr.coef * d1;
+        f2 += pr.coef * d2;
+        f3 += pr.coef * d3;
+        fc += pr.curv;
+        fe += pr.energy;
+      }
+    }
+  }
+  if (!live) return;
+  const size_t at = (size_t)slice * stride + p;
+  out.force[at] = make_double4(f1, f2, f3, fc);
+  out.energy[at] = fe;
+  out.nearest[at] = best;
+  if (TRACK) out.nearest_at[at] = best_at;
+}
+
+// ------------------------------------------------------------------ the pass
+// Site count of a shell pass (offsets[n] after the scan), for sizing the workspace.
+cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, int n, int gid, double s_margin,
+                               uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, cudaStream_t s) {
+  k_shell_count<<<(n + 255) / 256, 256, 0, s>>>(q32, q64, n, gid, prec == kFP64, s_margin, counts);
+  return launch_scan(counts, offsets, n, nullptr, scan_tmp, s);
+}
+
+cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
+  const int n = L.n;
+  const bool fp64 = L.prec == kFP64;
+  const int tb = 256;
+  // 1. shell
+  k_shell_count<<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, fp64, L.s_margin, L.counts);
+  cudaError_t e = launch_scan(L.counts, L.offsets, n, nullptr, L.scan_tmp, s);
+  if (e) return e;
+  if (fp64)
+    k_shell_write<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.s_margin, L.offsets, L.capacity,
+                                                         L.site_q32, L.site_q64, L.site_code, L.site_img, L.site_pos,
+                                                         L.grid);
+  else
+    k_shell_write<false><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.s_margin, L.offsets, L.capacity,
+                                                          L.site_q32, L.site_q64, L.site_code, L.site_img, L.site_pos,
+                                                          L.grid);
+  // 2. grid and the site sort
+  k_grid_setup<<<1, 1, 0, s>>>(L.grid, L.offsets + n, L.capacity, L.sdim_max, L.cells);
+  const int max_cells = L.sdim_max * L.sdim_max * L.sdim_max;
+  cudaMemsetAsync(L.cell_count, 0, sizeof(uint32_t) * (max_cells + 1), s);
+  k_cell_count<<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.site_pos, L.grid, L.site_cell, L.site_rank, L.cell_count);
+  if ((e = launch_scan(L.cell_count, L.cell_off, max_cells, L.cells, L.scan_tmp, s))) return e;
+  k_scatter<<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.site_cell, L.site_rank, L.cell_off, L.capacity,
+                                                      &L.grid->sites, L.perm);
+  k_bucket_sort<<<(max_cells + tb - 1) / tb, tb, 0, s>>>(L.cell_off, max_cells, L.cells, L.perm);
+  if (fp64)
+    k_site_gather<true><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_code,
+                                                                  L.site_img, L.sq32, L.sq64, L.scode, L.simg);
+  else
+    k_site_gather<false><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_code,
+                                                                   L.site_img, L.sq32, L.sq64, L.scode, L.simg);
+  // 3. sources in Morton order
+  const int mcells = kMortonDim * kMortonDim * kMortonDim;
+  cudaMemsetAsync(L.mcount, 0, sizeof(uint32_t) * (mcells + 1), s);
+  if (fp64)
+    k_source_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.grid, L.src_key, L.src_rank, L.mcount);
+  else
+    k_source_count<false><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.grid, L.src_key, L.src_rank, L.mcount);
+  if ((e = launch_scan(L.mcount, L.moff, mcells, nullptr, L.scan_tmp, s))) return e;
+  k_scatter<<<(n + tb - 1) / tb, tb, 0, s>>>(L.src_key, L.src_rank, L.moff, n, nullptr, L.src_perm);
+  k_bucket_sort<<<(mcells + tb - 1) / tb, tb, 0, s>>>(L.moff, mcells, nullptr, L.src_perm);
+  // 4. gather, 5. slices summed into rows
+  const int warps = (n + 31) / 32;
+  const dim3 grid((warps + kNearWarps - 1) / kNearWarps, L.slices);
+  NearCut cut{L.cut2, L.chord, L.cut_z, L.cut_w};
+  const Rows dst = L.partial;
+  if (fp64) {
+    if (L.track) k_near64<true><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
+    else k_near64<false><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
+  } else {
+    if (L.track) k_near32<true><<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
+    else k_near32<false><<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
+  }
+  k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(L.partial, n, L.slices, n, (const int*)L.src_perm, L.out, L.track ? 1 : 0);
+  return cudaGetLastError();
+}
+
+}  // namespace zo

@@ -1,0 +1,413 @@
+// Tables, sampler, fold, scan and the all-pairs row kernels.
+//
+// All-pairs rows (shaders/pairs.wgsl:151-326, src/pairs.zig:52-128): one thread per source,
+// 128 sources per block; the images j*g_k of a block's chunk stream through shared memory
+// in tiles of 128 (each built once per block, in registers from the constant operator
+// table, never stored in HBM). Tiles are plain FP32 sums merged into FP64 row sums
+// once per tile. A chunk's partial rows are reduced in chunk order afterwards, so the sums
+// do not depend on scheduling.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "k_common.cuh"
+#include "kernels.h"
+
+namespace zo {
+
+cudaError_t upload_tables(const HostTables& t) {
+  cudaError_t e;
+  double4 ops64[kMaxOperatorRows], ops32[kMaxOperatorRows], planes64[kMaxPlaneRows];
+  float4 planes32[kMaxPlaneRows];
+  for (int r = 0; r < kMaxOperatorRows; ++r) {
+    ops64[r] = make_double4(t.ops64[r][0], t.ops64[r][1], t.ops64[r][2], t.ops64[r][3]);
+    ops32[r] = make_double4(t.ops32[r][0], t.ops32[r][1], t.ops32[r][2], t.ops32[r][3]);
+  }
+  for (int r = 0; r < kMaxPlaneRows; ++r) {
+    planes64[r] = make_double4(t.planes64[r][0], t.planes64[r][1], t.planes64[r][2], t.planes64[r][3]);
+    planes32[r] = make_float4(t.planes32[r][0], t.planes32[r][1], t.planes32[r][2], t.planes32[r][3]);
+  }
+  if ((e = cudaMemcpyToSymbol(c_ops64, ops64, sizeof(ops64)))) return e;
+  if ((e = cudaMemcpyToSymbol(c_ops32, ops32, sizeof(ops32)))) return e;
+  if ((e = cudaMemcpyToSymbol(c_planes64, planes64, sizeof(planes64)))) return e;
+  if ((e = cudaMemcpyToSymbol(c_planes32, planes32, sizeof(planes32)))) return e;
+  if ((e = cudaMemcpyToSymbol(c_group_offset, t.group_offset, sizeof(int) * 11))) return e;
+  if ((e = cudaMemcpyToSymbol(c_group_order, t.group_order, sizeof(int) * 11))) return e;
+  return cudaMemcpyToSymbol(c_plane_offset, t.plane_offset, sizeof(int) * 11);
+}
+
+// ------------------------------------------------------------------ Haar sampler
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  return x ^ (x >> 16);
+}
+__device__ __forceinline__ float unit_random(uint32_t v) {
+  return ((float)(hash32(v) >> 8) + 0.5f) / 16777216.0f;
+}
+
+// Shoemake uniform quaternions (shaders/haar.wgsl:5-10): u, a, b exactly as the shader
+// forms them in float32, the quaternion evaluated in FP64 and rounded once.
+__global__ void k_haar(float4* __restrict__ q, int n, uint32_t seed_hash) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t base = hash32((uint32_t)i ^ seed_hash);
+  const float two_pi = 6.28318530718f;
+  const float u = unit_random(base);
+  const float a = __fmul_rn(two_pi, unit_random(base + 1u));
+  const float b = __fmul_rn(two_pi, unit_random(base + 2u));
+  const double su = sqrt((double)u), sv = sqrt(1.0 - (double)u);
+  double sa, ca, sb, cb;
+  sincos((double)a, &sa, &ca);
+  sincos((double)b, &sb, &cb);
+  q[i] = make_float4((float)(su * cb), (float)(sv * sa), (float)(sv * ca), (float)(su * sb));
+}
+
+// ------------------------------------------------------------------ fold
+// Normalisation of an imported float32 quaternion with the reference's exponent rescale
+// (shaders/state.wgsl:31-40): components whose rescaled exponent would be subnormal become
+// signed zeros; the power-of-two scale itself cancels in the FP64 normalisation.
+__device__ __forceinline__ double4 flush_normalize(float4 a) {
+  const unsigned int bx = __float_as_uint(a.x), by = __float_as_uint(a.y);
+  const unsigned int bz = __float_as_uint(a.z), bw = __float_as_uint(a.w);
+  const int ex = (bx >> 23) & 255, ey = (by >> 23) & 255, ez = (bz >> 23) & 255, ew = (bw >> 23) & 255;
+  const int em = max(max(ex, ey), max(ez, ew));
+  auto keep = [em](float v, int e) -> double {
+    return (e > 0 && e + 127 - em > 0) ? (double)v : copysign(0.0, (double)v);
+  };
+  return normalize4(make_double4(keep(a.x, ex), keep(a.y, ey), keep(a.z, ez), keep(a.w, ew)));
+}
+
+// Every quaternion to its zone representative (shaders/state.wgsl:30-46, src/engine.zig:233).
+__global__ void k_fold(float4* __restrict__ q32, double4* __restrict__ q64, int n, int gid, int prec, int from_q32) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const bool fp64 = prec == kFP64;
+  double4 p = (from_q32 || !fp64) ? flush_normalize(q32[i]) : normalize4(q64[i]);
+  p = fold64(p, gid, !fp64);
+  q32[i] = to_f4(p);
+  if (fp64) q64[i] = p;
+}
+
+// ------------------------------------------------------------------ device-wide scan
+// Exclusive scan of uint32 counts in tiles of 4096 (1024 threads x 4), block totals
+// scanned by one block, then added back. out[count] receives the total.
+constexpr int kScanTile = 4096;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums, uint32_t& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t s = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    warp_sums[lane] = s;
+  }
+  __syncthreads();
+  total = warp_sums[(blockDim.x >> 5) - 1];
+  const uint32_t before = wid ? warp_sums[wid - 1] : 0u;
+  __syncthreads();
+  return before + x - v;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                      int max_count, const int* count_dev, uint32_t* block_sums) {
+  __shared__ uint32_t warp_sums[32];
+  const int count = count_dev ? min(*count_dev, max_count) : max_count;
+  const int base = blockIdx.x * kScanTile;
+  if (base >= count && !(blockIdx.x == 0)) return;
+  uint32_t v[4];
+  uint32_t local = 0;
+  for (int r = 0; r < 4; ++r) {
+    const int idx = base + threadIdx.x * 4 + r;
+    v[r] = idx < count ? in[idx] : 0u;
+    local += v[r];
+  }
+  uint32_t total;
+  uint32_t at = block_exclusive_scan(local, warp_sums, total);
+  for (int r = 0; r < 4; ++r) {
+    const int idx = base + threadIdx.x * 4 + r;
+    if (idx < count) out[idx] = at;
+    at += v[r];
+  }
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_sums(uint32_t* block_sums, uint32_t* __restrict__ out, int max_count,
+                                                     const int* count_dev) {
+  __shared__ uint32_t warp_sums[32];
+  const int count = count_dev ? min(*count_dev, max_count) : max_count;
+  const int blocks = (count + kScanTile - 1) / kScanTile;
+  uint32_t v[4];
+  uint32_t local = 0;
+  for (int r = 0; r < 4; ++r) {
+    const int idx = threadIdx.x * 4 + r;
+    v[r] = idx < blocks ? block_sums[idx] : 0u;
+    local += v[r];
+  }
+  uint32_t total;
+  uint32_t at = block_exclusive_scan(local, warp_sums, total);
+  for (int r = 0; r < 4; ++r) {
+    const int idx = threadIdx.x * 4 + r;
+    if (idx < blocks) block_sums[idx] = at;
+    at += v[r];
+  }
+  if (threadIdx.x == 0) out[count] = total;
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ out, int max_count, const int* count_dev,
+                           const uint32_t* __restrict__ block_sums) {
+  const int count = count_dev ? min(*count_dev, max_count) : max_count;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < count) out[idx] += block_sums[idx / kScanTile];
+}
+
+cudaError_t launch_scan(const uint32_t* in, uint32_t* out, int max_count, const int* count_dev, uint32_t* block_sums,
+                        cudaStream_t s) {
+  if (max_count > kScanTile * kScanTile) return cudaErrorInvalidValue;
+  const int tiles = max(1, (max_count + kScanTile - 1) / kScanTile);
+  k_scan_tiles<<<tiles, 1024, 0, s>>>(in, out, max_count, count_dev, block_sums);
+  k_scan_sums<<<1, 1024, 0, s>>>(block_sums, out, max_count, count_dev);
+  if (max_count > kScanTile) k_scan_add<<<(max_count + 255) / 256, 256, 0, s>>>(out, max_count, count_dev, block_sums);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ all-pairs rows
+constexpr int kPairBlock = 128;
+
+struct PairTile {
+  int k, j0, count;
+};
+__device__ __forceinline__ PairTile pair_tile(int tile, int jtiles, int n) {
+  PairTile t;
+  t.k = tile / jtiles;
+  t.j0 = (tile - t.k * jtiles) * kPairBlock;
+  t.count = min(kPairBlock, n - t.j0);
+  return t;
+}
+
+// FP32 rows (the relaxation's force pass, quey_partial semantics, shaders/pairs.wgsl:266-308):
+// force and energy over every image of every other source; nearest over every image
+// but the identity self pair. TRACK keeps the first image index of the nearest chord.
+template <bool TRACK, bool CHECK>
+__device__ __forceinline__ void pairs32_tile(const float4 x, const float4* tile, int count, int i, int j0, int k, int n,
+                                             float& s1, float& s2, float& s3, float& sc, float& se, float& best,
+                                             int& best_at) {
+#pragma unroll 2
+  for (int t = 0; t < count; ++t) {
+    const float4 y = tile[t];
+    const float mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
+    const float pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
+    const float dm2 = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
+    const float dp2 = fmaf(pw, pw, fmaf(px, px, fmaf(py, py, pz * pz)));
+    const float c = fminf(dm2, dp2);
+    const bool own = CHECK && (j0 + t == i);
+    if (!(own && k == 0)) {
+      if (TRACK) {
+        if (c < best) {
+          best = c;
+          best_at = k * n + j0 + t;
+        }
+      } else {
+        best = fminf(best, c);
+      }
+    }
+    if (own) continue;
+    const PairF p = quey_pair32(dm2, dp2);
+    float d1, d2, d3;
+    pair_direction(x, y, d1, d2, d3);
+    s1 = fmaf(p.coef, d1, s1);
+    s2 = fmaf(p.coef, d2, s2);
+    s3 = fmaf(p.coef, d3, s3);
+    sc += p.curv;
+    se += p.energy;
+  }
+}
+
+template <bool TRACK>
+__global__ void __launch_bounds__(kPairBlock) k_pairs32(const float4* __restrict__ q, int n, int op_off, int jtiles,
+                                                        int total_tiles, int tiles_per_chunk, Rows out, int stride) {
+  __shared__ float4 tile[kPairBlock];
+  const int i0 = blockIdx.x * kPairBlock;
+  const int i = i0 + threadIdx.x;
+  const bool live = i < n;
+  const float4 x = live ? q[i] : make_float4(1.f, 0.f, 0.f, 0.f);
+  double f1 = 0, f2 = 0, f3 = 0, fc = 0, fe = 0;
+  float best = 4.0f;
+  int best_at = -1;
+  const int t0 = blockIdx.y * tiles_per_chunk, t1 = min(total_tiles, t0 + tiles_per_chunk);
+  for (int tid = t0; tid < t1; ++tid) {
+    const PairTile pt = pair_tile(tid, jtiles, n);
+    __syncthreads();
+    if ((int)threadIdx.x < pt.count) tile[threadIdx.x] = image32(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0);
+    __syncthreads();
+    if (!live) continue;
+    float s1 = 0.f, s2 = 0.f, s3 = 0.f, sc = 0.f, se = 0.f;
+    if (pt.j0 < i0 + kPairBlock && i0 < pt.j0 + pt.count)
+      pairs32_tile<TRACK, true>(x, tile, pt.count, i, pt.j0, pt.k, n, s1, s2, s3, sc, se, best, best_at);
+    else
+      pairs32_tile<TRACK, false>(x, tile, pt.count, i, pt.j0, pt.k, n, s1, s2, s3, sc, se, best, best_at);
+    f1 += s1;
+    f2 += s2;
+    f3 += s3;
+    fc += sc;
+    fe += se;
+  }
+  if (!live) return;
+  const size_t at = (size_t)blockIdx.y * stride + i;
+  out.force[at] = make_double4(f1, f2, f3, fc);
+  out.energy[at] = fe;
+  out.nearest[at] = best;
+  if (TRACK) out.nearest_at[at] = best_at;
+}
+
+// The same rows in FP64 (the plain method).
+template <bool TRACK, bool CHECK>
+__device__ __forceinline__ void pairs64_tile(const double4 x, const double4* tile, int count, int i, int j0, int k, int n,
+                                             double& f1, double& f2, double& f3, double& fc, double& fe, double& best,
+                                             int& best_at) {
+  for (int t = 0; t < count; ++t) {
+    const double4 y = tile[t];
+    const double mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
+    const double pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
+    const double dm2 = mw * mw + mx * mx + my * my + mz * mz;
+    const double dp2 = pw * pw + px * px + py * py + pz * pz;
+    const double c = fmin(dm2, dp2);
+    const bool own = CHECK && (j0 + t == i);
+    if (!(own && k == 0)) {
+      if (c < best) {
+        best = c;
+        if (TRACK) best_at = k * n + j0 + t;
+      }
+    }
+    if (own) continue;
+    const PairD p = quey_pair64(dm2, dp2);
+    double d1, d2, d3;
+    pair_direction(x, y, d1, d2, d3);
+    f1 += p.coef * d1;
+    f2 += p.coef * d2;
+    f3 += p.coef * d3;
+    fc += p.curv;
+    fe += p.energy;
+  }
+}
+
+template <bool TRACK>
+__global__ void __launch_bounds__(kPairBlock) k_pairs64(const double4* __restrict__ q, int n, int op_off, int jtiles,
+                                                        int total_tiles, int tiles_per_chunk, Rows out, int stride) {
+  __shared__ double4 tile[kPairBlock];
+  const int i0 = blockIdx.x * kPairBlock;
+  const int i = i0 + threadIdx.x;
+  const bool live = i < n;
+  const double4 x = live ? q[i] : make_double4(1, 0, 0, 0);
+  double f1 = 0, f2 = 0, f3 = 0, fc = 0, fe = 0, best = 4.0;
+  int best_at = -1;
+  const int t0 = blockIdx.y * tiles_per_chunk, t1 = min(total_tiles, t0 + tiles_per_chunk);
+  for (int tid = t0; tid < t1; ++tid) {
+    const PairTile pt = pair_tile(tid, jtiles, n);
+    __syncthreads();
+    if ((int)threadIdx.x < pt.count) tile[threadIdx.x] = image64(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0);
+    __syncthreads();
+    if (!live) continue;
+    if (pt.j0 < i0 + kPairBlock && i0 < pt.j0 + pt.count)
+      pairs64_tile<TRACK, true>(x, tile, pt.count, i, pt.j0, pt.k, n, f1, f2, f3, fc, fe, best, best_at);
+    else
+      pairs64_tile<TRACK, false>(x, tile, pt.count, i, pt.j0, pt.k, n, f1, f2, f3, fc, fe, best, best_at);
+  }
+  if (!live) return;
+  const size_t at = (size_t)blockIdx.y * stride + i;
+  out.force[at] = make_double4(f1, f2, f3, fc);
+  out.energy[at] = fe;
+  out.nearest[at] = best;
+  if (TRACK) out.nearest_at[at] = best_at;
+}
+
+// Partial rows of `parts` chunks (or slices) summed in chunk order into rows indexed
+// by `dest` (identity when null): the sums do not depend on how blocks were scheduled.
+__global__ void k_rows_reduce(Rows part, int stride, int parts, int n, const int* __restrict__ dest, Rows out,
+                              int track) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  double4 f = make_double4(0, 0, 0, 0);
+  double e = 0, best = 4.0;
+  int best_at = -1;
+  for (int c = 0; c < parts; ++c) {
+    const size_t at = (size_t)c * stride + p;
+    const double4 g = part.force[at];
+    f.x += g.x;
+    f.y += g.y;
+    f.z += g.z;
+    f.w += g.w;
+    e += part.energy[at];
+    const double b = part.nearest[at];
+    if (b < best) {
+      best = b;
+      if (track) best_at = part.nearest_at[at];
+    }
+  }
+  const int i = dest ? dest[p] : p;
+  out.force[i] = f;
+  out.energy[i] = e;
+  out.nearest[i] = best;
+  if (track) out.nearest_at[i] = best_at;
+}
+
+PairsPlan plan_pairs(int n, int order, double budget_scale, int sms) {
+  PairsPlan pl;
+  pl.jtiles = (n + kPairBlock - 1) / kPairBlock;
+  pl.total_tiles = order * pl.jtiles;
+  const int blocks = pl.jtiles;
+  const int target = sms * 16;  // several resident blocks per SM, a few waves
+  int chunks = (target + blocks - 1) / blocks;
+  if (budget_scale > 0 && budget_scale < 1) chunks = (int)(chunks / budget_scale + 0.5);
+  chunks = max(1, min(chunks, pl.total_tiles));
+  pl.tiles_per_chunk = (pl.total_tiles + chunks - 1) / chunks;
+  pl.chunks = (pl.total_tiles + pl.tiles_per_chunk - 1) / pl.tiles_per_chunk;
+  return pl;
+}
+
+cudaError_t launch_pairs(int prec, bool track, const float4* q32, const double4* q64, int n, int gid, const PairsPlan& pl,
+                         Rows partial, Rows out, cudaStream_t s) {
+  const int op_off = host_group_offset(gid);
+  const dim3 grid(pl.jtiles, pl.chunks);
+  const bool direct = pl.chunks == 1;
+  Rows dst = direct ? out : partial;
+  if (prec == kFP64) {
+    if (track) k_pairs64<true><<<grid, kPairBlock, 0, s>>>(q64, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, n);
+    else k_pairs64<false><<<grid, kPairBlock, 0, s>>>(q64, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, n);
+  } else {
+    if (track) k_pairs32<true><<<grid, kPairBlock, 0, s>>>(q32, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, n);
+    else k_pairs32<false><<<grid, kPairBlock, 0, s>>>(q32, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, n);
+  }
+  if (!direct) k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(partial, n, pl.chunks, n, nullptr, out, track ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_haar(float4* q, int n, uint32_t seed, cudaStream_t s) {
+  // hash(seed) on the host side of the formula: base = hash(i ^ hash(seed)).
+  uint32_t x = seed;
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  k_haar<<<(n + 255) / 256, 256, 0, s>>>(q, n, x);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fold(float4* q32, double4* q64, int n, int gid, int prec, bool from_q32, cudaStream_t s) {
+  k_fold<<<(n + 255) / 256, 256, 0, s>>>(q32, q64, n, gid, prec, from_q32 ? 1 : 0);
+  return cudaGetLastError();
+}
+
+}  // namespace zo

@@ -1,0 +1,65 @@
+// The engine's CUDA kernels, compiled as one translation unit so that every kernel reads
+// the same constant-memory group tables. Parts:
+//   k_pairs.cuh  sampler, fold, scan, all-pairs force rows
+//   k_full.cuh   full pair measures (Riesz, Green, log)
+//   k_near.cuh   near-field shell, chart-grid sorts and gather
+//   k_relax.cuh  BB step, median, move+fold, row summaries
+#include <cuda_runtime.h>
+
+#include "qvm_shared.h"
+
+#include "k_pairs.cuh"
+#include "k_full.cuh"
+#include "k_near.cuh"
+#include "k_relax.cuh"
+
+namespace zo {
+
+cudaError_t launch_relax_stats(Rows rows, const double4* prev_f, const double4* prev_d, int n, int fixed,
+                               double* partials, RelaxDev* st, cudaStream_t s) {
+  k_relax_stats<<<reduce_blocks(n), kRelaxBlock, 0, s>>>(rows, prev_f, prev_d, n, fixed, partials, st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_median(int prec, Rows rows, int n, RelaxDev* st, unsigned int* hist, double alpha0, double radius,
+                          int sms, cudaStream_t s) {
+  const int blocks = max(1, min((n + 255) / 256, 2 * sms));
+  if (prec == kFP64) {
+    for (int r = 0; r < 8; ++r) k_median_round<true><<<blocks, 256, 0, s>>>(rows, n, r, st, hist, alpha0, radius);
+  } else {
+    for (int r = 0; r < 4; ++r) k_median_round<false><<<blocks, 256, 0, s>>>(rows, n, r, st, hist, alpha0, radius);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_move_fold(float4* q32, double4* q64, int n, int gid, int prec, Rows rows, double4* prev_f,
+                             double4* prev_d, RelaxDev* st, int fixed, double radius, double step_scale, cudaStream_t s) {
+  k_move_fold<<<(n + 127) / 128, 128, 0, s>>>(q32, q64, n, gid, prec, rows, prev_f, prev_d, st, fixed, radius,
+                                              step_scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_row_summary(Rows rows, int n, double* partials, double* near_partials, int* near_rows,
+                               RowSummary* out, cudaStream_t s) {
+  k_row_summary<<<reduce_blocks(n), kRelaxBlock, 0, s>>>(rows, n, partials, near_partials, near_rows, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_nearest_degrees(const double* nearest, int n, float* out, cudaStream_t s) {
+  k_nearest_degrees<<<(n + 255) / 256, 256, 0, s>>>(nearest, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_refine_nearest(const float4* q32, int n, int gid, Rows rows, bool near_sites, const uint32_t* scode,
+                                  const uint32_t* simg, int* neighbour, cudaStream_t s) {
+  k_refine_nearest<<<(n + 255) / 256, 256, 0, s>>>(q32, n, gid, rows, near_sites ? 1 : 0, scode, simg, neighbour);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_neighbour_index(Rows rows, int n, bool near_sites, const uint32_t* scode, int* neighbour,
+                                   cudaStream_t s) {
+  k_neighbour_index<<<(n + 255) / 256, 256, 0, s>>>(rows, n, near_sites ? 1 : 0, scode, neighbour);
+  return cudaGetLastError();
+}
+
+}  // namespace zo

@@ -1,0 +1,88 @@
+// Host-callable launchers of the CUDA kernels (kernels.cu). Plain pointers only.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "qvm_shared.h"
+
+namespace zo {
+
+struct HostTables {
+  double ops64[kMaxOperatorRows][4];
+  float ops32[kMaxOperatorRows][4];
+  double planes64[kMaxPlaneRows][4];
+  float planes32[kMaxPlaneRows][4];
+  int group_offset[11];
+  int group_order[11];
+  int plane_offset[11];
+};
+const HostTables& host_tables();
+int host_group_offset(int gid);
+int host_group_order(int gid);
+
+// Copies the group tables into the current device's constant memory (once per device).
+cudaError_t upload_tables(const HostTables& t);
+
+cudaError_t launch_haar(float4* q, int n, uint32_t seed, cudaStream_t s);
+cudaError_t launch_fold(float4* q32, double4* q64, int n, int gid, int prec, bool from_q32, cudaStream_t s);
+cudaError_t launch_scan(const uint32_t* in, uint32_t* out, int max_count, const int* count_dev, uint32_t* block_sums,
+                        cudaStream_t s);
+
+// All-pairs work split: 128 sources per block, `chunks` ranges of image tiles per source block.
+struct PairsPlan {
+  int jtiles = 0, total_tiles = 0, tiles_per_chunk = 0, chunks = 1;
+};
+PairsPlan plan_pairs(int n, int order, double budget_scale, int sms);
+
+// Force-pass rows over all pairs; `partial` holds chunks*n rows when chunks > 1.
+cudaError_t launch_pairs(int prec, bool track, const float4* q32, const double4* q64, int n, int gid, const PairsPlan& pl,
+                         Rows partial, Rows out, cudaStream_t s);
+// Full measure rows: `extra` 5 doubles per source (riesz1, riesz2, riesz3, green, log).
+cudaError_t launch_full(int prec, const float4* q32, const double4* q64, int n, int gid, const PairsPlan& pl,
+                        Rows partial, double* pextra, int* pdegen, Rows out, double* extra, int* degen, cudaStream_t s);
+
+// One near-field pass; every pointer is device memory sized by the host (Near workspace).
+struct NearLaunch {
+  int prec, gid, n, capacity, sdim_max, slices;
+  bool track;
+  double s_margin, cut2, chord, cut_z, cut_w;
+  const float4* q32;
+  const double4* q64;
+  uint32_t *counts, *offsets, *scan_tmp;
+  float4* site_q32;
+  double4* site_q64;
+  uint32_t *site_code, *site_img, *site_cell, *site_rank;
+  float4* site_pos;
+  uint32_t *cell_count, *cell_off, *perm;
+  float4* sq32;
+  double4* sq64;
+  uint32_t *scode, *simg;
+  uint32_t *src_key, *src_rank, *mcount, *moff, *src_perm;
+  NearGrid* grid;
+  int* cells;
+  Rows partial;  // slices * n rows
+  Rows out;
+};
+cudaError_t launch_near(const NearLaunch& L, cudaStream_t s);
+cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, int n, int gid, double s_margin,
+                               uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, cudaStream_t s);
+
+// Relaxation step pieces.
+cudaError_t launch_relax_stats(Rows rows, const double4* prev_f, const double4* prev_d, int n, int fixed,
+                               double* partials, RelaxDev* st, cudaStream_t s);
+cudaError_t launch_median(int prec, Rows rows, int n, RelaxDev* st, unsigned int* hist, double alpha0, double radius,
+                          int sms, cudaStream_t s);
+cudaError_t launch_move_fold(float4* q32, double4* q64, int n, int gid, int prec, Rows rows, double4* prev_f,
+                             double4* prev_d, RelaxDev* st, int fixed, double radius, double step_scale, cudaStream_t s);
+cudaError_t launch_row_summary(Rows rows, int n, double* partials, double* near_partials, int* near_rows,
+                               RowSummary* out, cudaStream_t s);
+cudaError_t launch_nearest_degrees(const double* nearest, int n, float* out, cudaStream_t s);
+cudaError_t launch_refine_nearest(const float4* q32, int n, int gid, Rows rows, bool near_sites, const uint32_t* scode,
+                                  const uint32_t* simg, int* neighbour, cudaStream_t s);
+cudaError_t launch_neighbour_index(Rows rows, int n, bool near_sites, const uint32_t* scode, int* neighbour,
+                                   cudaStream_t s);
+
+// Blocks used by the row-summary and stats reductions for n rows.
+inline int reduce_blocks(int n) { return (n + 255) / 256; }
+
+}  // namespace zo

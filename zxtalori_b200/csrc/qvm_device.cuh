@@ -1,0 +1,229 @@
+// Device-side arithmetic of the QVM repulsion path: quaternion helpers, the Quey pair in
+// FP32 (fast, hot loops) and FP64 (exact, plain method), the near-field window, and the
+// fundamental-zone fold. Quaternions are scalar first and live in float4/double4 as
+// (.x=w, .y=x, .z=y, .w=z); symmetry acts on the right (q*g).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "qvm_shared.h"
+
+namespace zo {
+
+constexpr float kPiF = 3.14159265358979323846f;
+constexpr double kPi = 3.14159265358979323846;
+
+// Operator tables of all eleven groups (rows kGroupOffset[g] .. +kGroupOrder[g]):
+// c_ops64 the FP64 table, c_ops32 the float32 rounding the reference uploads (as double).
+// Zone bisector planes (2|K|-1 per group, src/covering.zig:382-396): float32 rounding of the
+// planes built from the f32 table (FP32 mode) and FP64 planes of the f64 table (FP64 mode).
+// Defined here: every kernel is compiled in the one translation unit kernels.cu.
+__constant__ double4 c_ops64[kMaxOperatorRows];
+__constant__ double4 c_ops32[kMaxOperatorRows];
+__constant__ float4 c_planes32[kMaxPlaneRows];
+__constant__ double4 c_planes64[kMaxPlaneRows];
+__constant__ int c_group_offset[11];
+__constant__ int c_group_order[11];
+__constant__ int c_plane_offset[11];
+
+// ------------------------------------------------------------------ quaternion helpers
+__device__ __forceinline__ double4 qmul(double4 a, double4 b) {
+  return make_double4(a.x * b.x - a.y * b.y - a.z * b.z - a.w * b.w,
+                      a.x * b.y + a.y * b.x + a.z * b.w - a.w * b.z,
+                      a.x * b.z - a.y * b.w + a.z * b.x + a.w * b.y,
+                      a.x * b.w + a.y * b.z - a.z * b.y + a.w * b.x);
+}
+__device__ __forceinline__ double dot4(double4 a, double4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+__device__ __forceinline__ double4 scale4(double4 a, double s) { return make_double4(a.x * s, a.y * s, a.z * s, a.w * s); }
+__device__ __forceinline__ double4 neg4(double4 a) { return make_double4(-a.x, -a.y, -a.z, -a.w); }
+__device__ __forceinline__ double4 normalize4(double4 a) { return scale4(a, 1.0 / sqrt(dot4(a, a))); }
+__device__ __forceinline__ double4 to_d4(float4 a) { return make_double4(a.x, a.y, a.z, a.w); }
+__device__ __forceinline__ float4 to_f4(double4 a) {
+  return make_float4((float)a.x, (float)a.y, (float)a.z, (float)a.w);
+}
+
+// Image y = q g_k of a source (shaders/pairs.wgsl:181): the identity image is the source
+// itself bit for bit; the others are normalised. FP32 mode forms the product and the
+// normalisation in FP64 and rounds once (the correctly rounded image).
+__device__ __forceinline__ float4 image32(float4 q, int op_row, bool identity) {
+  if (identity) return q;
+  return to_f4(normalize4(qmul(to_d4(q), c_ops32[op_row])));
+}
+__device__ __forceinline__ double4 image64(double4 q, int op_row, bool identity) {
+  if (identity) return q;
+  return normalize4(qmul(q, c_ops64[op_row]));
+}
+
+// ------------------------------------------------------------------ approximate SFU ops
+// PTX rcp.approx / sqrt.approx: the documented MUFU approximations (max error ~1 ulp).
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// 2 atan(t) for t in [0,1]: t * P(t^2), P the degree-8 minimax fit of fit_atan.py (max
+// relative error 1.5e-8 with exact coefficients), doubled.
+__device__ __forceinline__ float two_atan_unit(float t, float t2) {
+  float p = 0x1.758a10p-8f;
+  p = fmaf(p, t2, -0x1.07448cp-5f);
+  p = fmaf(p, t2, 0x1.5dba7cp-4f);
+  p = fmaf(p, t2, -0x1.336030p-3f);
+  p = fmaf(p, t2, 0x1.b3da44p-3f);
+  p = fmaf(p, t2, -0x1.22e400p-2f);
+  p = fmaf(p, t2, 0x1.9972e8p-2f);
+  p = fmaf(p, t2, -0x1.5554a6p-1f);
+  p = fmaf(p, t2, 2.0f);
+  return t * p;
+}
+
+// Vector part of y * conj(x): the left-tangent direction of a pair (shaders/pairs.wgsl:258).
+template <class T, class V>
+__device__ __forceinline__ void pair_direction(const V& x, const V& y, T& d1, T& d2, T& d3) {
+  d1 = x.x * y.y - y.x * x.y + (x.z * y.w - x.w * y.z);
+  d2 = x.x * y.z - y.x * x.z + (x.w * y.y - x.y * y.w);
+  d3 = x.x * y.w - y.x * x.w + (x.y * y.z - x.z * y.y);
+}
+
+// One Quey pair (shaders/pairs.wgsl:250-262), FP32. With a = 2 atan(sqrt(near/far)) the
+// nearer S3 angle and b = pi - a:
+//   force = -sign (1/(a^2+e) - 1/(b^2+e)) / (sin a + e) * dir,  curvature = 1/(a^3+e) + 1/(b^3+e),
+//   energy = 1/a + 1/b = pi/(ab),  e = 1e-9,  sin a = 2t/(1+t^2).
+// The four divisions share two approximate reciprocals; `coef` multiplies the direction.
+struct PairF {
+  float coef, curv, energy, a, inv_sine;
+};
+__device__ __forceinline__ PairF quey_pair32(float dm2, float dp2) {
+  const float nearv = fmaxf(fminf(dm2, dp2), 1e-30f);
+  const float farv = fmaxf(fmaxf(dm2, dp2), 1e-30f);
+  const float t2 = nearv * rcp_approx(farv);
+  const float t = sqrt_approx(t2);
+  const float a = fmaxf(two_atan_unit(t, t2), 1e-12f);
+  const float b = kPiF - a;
+  const float aa = a * a, bb = b * b;
+  const float a2 = aa + 1e-9f, b2 = bb + 1e-9f;
+  const float a3 = fmaf(aa, a, 1e-9f), b3 = fmaf(bb, b, 1e-9f);
+  const float onept2 = 1.0f + t2;
+  const float sp = fmaf(1e-9f, onept2, t + t);  // (sine + 1e-9) * (1 + t^2)
+  const float a2b2 = a2 * b2;
+  const float r1 = rcp_approx(a2b2 * sp);
+  const float along = (b2 - a2) * onept2 * r1;
+  const float ab = a * b;
+  const float a3b3 = a3 * b3;
+  const float r2 = rcp_approx(a3b3 * ab);
+  PairF p;
+  p.coef = (dm2 <= dp2) ? -along : along;
+  p.curv = (a3 + b3) * ab * r2;
+  p.energy = kPiF * a3b3 * r2;
+  p.a = a;
+  p.inv_sine = onept2 * a2b2 * r1;
+  return p;
+}
+
+// The same pair in FP64 with IEEE division, sqrt and atan: the plain method's arithmetic.
+struct PairD {
+  double coef, curv, energy, a;
+};
+__device__ __forceinline__ PairD quey_pair64(double dm2, double dp2) {
+  const double nearv = fmax(fmin(dm2, dp2), 1e-30);
+  const double farv = fmax(fmax(dm2, dp2), 1e-30);
+  const double t = sqrt(nearv / farv);
+  const double a = fmax(2.0 * atan(t), 1e-12);
+  const double b = kPi - a;
+  const double a2 = a * a + 1e-9, b2 = b * b + 1e-9;
+  const double a3 = a * a * a + 1e-9, b3 = b * b * b + 1e-9;
+  const double sine = 2.0 * t / (1.0 + t * t) + 1e-9;
+  const double sign = (dm2 <= dp2) ? 1.0 : -1.0;
+  const double along = sign * (b2 - a2) / (a2 * b2 * sine);
+  PairD p;
+  p.coef = -along;
+  p.curv = (a3 + b3) / (a3 * b3);
+  p.energy = kPi / (a * b);
+  p.a = a;
+  return p;
+}
+
+// Near-field window (shaders/pairs.wgsl:352-361): the pair potential times
+// w = 1 - s^2 (3 - 2s), s = clamp((a - taper r) / ((1 - taper) r), 0, 1), and its exact force
+// (the window's slope adds sign E w'(a) / sin a along the direction). `cut_z` is taper*r,
+// `cut_w` 1/((1-taper) r). Evaluated branch-free: at s = 0 it is the plain pair.
+__device__ __forceinline__ void window32(PairF& p, float dm2, float dp2, float cut_z, float cut_w) {
+  const float s = __saturatef((p.a - cut_z) * cut_w);
+  const float w = fmaf(-s * s, fmaf(-2.0f, s, 3.0f), 1.0f);
+  const float slope = -6.0f * s * (1.0f - s) * cut_w;
+  float extra = p.energy * slope * p.inv_sine;
+  extra = (dm2 <= dp2) ? extra : -extra;
+  p.coef = fmaf(w, p.coef, extra);
+  p.curv *= w;
+  p.energy *= w;
+}
+__device__ __forceinline__ void window64(PairD& p, double dm2, double dp2, double cut_z, double cut_w) {
+  const double s = fmin(fmax((p.a - cut_z) * cut_w, 0.0), 1.0);
+  if (s <= 0.0) return;
+  const double w = 1.0 - s * s * (3.0 - 2.0 * s);
+  const double slope = -6.0 * s * (1.0 - s) * cut_w;
+  const double sign = (dm2 <= dp2) ? 1.0 : -1.0;
+  const double extra = sign * p.energy * slope / fmax(sin(p.a), 1e-9);
+  p.coef = w * p.coef + extra;
+  p.curv *= w;
+  p.energy *= w;
+}
+
+// ------------------------------------------------------------------ fundamental-zone fold
+// Homogeneous zone inequalities (shaders/state.wgsl:6-29) on a unit quaternion with w >= 0.
+__device__ __forceinline__ bool in_zone(double4 p, int gid, bool f32_ops) {
+  const double ax = fabs(p.y), ay = fabs(p.z), az = fabs(p.w), w = p.x;
+  const double t6 = 0.5773502691896258, t8 = 0.4142135623730951, t12 = 0.2679491924311227;
+  const double c6 = 0.8660254037844386, s45 = 0.7071067811865476;
+  switch (gid) {
+    case 0: return az <= w;
+    case 1: return az <= t6 * w;
+    case 2: return az <= t8 * w;
+    case 3: return az <= t12 * w;
+    case 4: return fmax(fmax(ax, ay), az) <= w;
+    case 5: return az <= t6 * w && fmax(ax, 0.5 * ax + c6 * ay) <= w;
+    case 6: return az <= t8 * w && fmax(fmax(ax, ay), s45 * (ax + ay)) <= w;
+    case 7: {
+      const double m = fmax(ax, ay), n = fmin(ax, ay);
+      return az <= t12 * w && fmax(m, c6 * m + 0.5 * n) <= w;
+    }
+    case 8: return ax + ay + az <= w;
+    case 9: return fmax(fmax(ax, ay), az) <= t8 * w && ax + ay + az <= w;
+    default: {
+      if (w > 0.9510566) return true;
+      if (w < 0.9256147) return false;
+      const int off = c_group_offset[gid], order = c_group_order[gid];
+      for (int k = 1; k < order; ++k) {
+        const double4 g = f32_ops ? c_ops32[off + k] : c_ops64[off + k];
+        if (fabs(fabs(g.x) - 0.8090169943749475) < 1e-5 && fabs(dot4(p, g)) > w) return false;
+      }
+      return true;
+    }
+  }
+}
+
+// Fold a unit quaternion into the zone (shaders/state.wgsl:30-46), FP64: w >= 0, keep it if
+// in the zone, else the image p g_k of largest |w| (first maximum), sign fixed, normalised.
+// `f32_ops` picks the float32 table (FP32 mode) or the FP64 one.
+__device__ __forceinline__ double4 fold64(double4 p, int gid, bool f32_ops) {
+  if (p.x < 0.0) p = neg4(p);
+  if (in_zone(p, gid, f32_ops)) return p;
+  const int off = c_group_offset[gid], order = c_group_order[gid];
+  double4 best = p;
+  double w = p.x;
+  for (int k = 0; k < order; ++k) {
+    const double4 c = qmul(p, f32_ops ? c_ops32[off + k] : c_ops64[off + k]);
+    if (fabs(c.x) > w) {
+      best = c.x >= 0.0 ? c : neg4(c);
+      w = fabs(c.x);
+    }
+  }
+  return normalize4(best);
+}
+
+}  // namespace zo

@@ -1,0 +1,63 @@
+// Types and limits shared by the host engine and the CUDA kernels.
+#pragma once
+#include <stdint.h>
+
+namespace zo {
+
+constexpr int kMaxOperatorRows = 141;   // sum of |K| over the eleven groups
+constexpr int kMaxPlaneRows = 271;      // sum of 2|K|-1 zone bisector planes
+constexpr uint32_t kIdentityBit = 0x80000000u;  // site code: the source's identity image
+constexpr int kMaxCellDim = 128;        // chart grid side (src/near.zig:135)
+constexpr int kMortonDim = 32;          // sources' Morton grid side (src/near.zig:23)
+
+// Precision of one sample's arithmetic.
+//  kFP32: FP32 pair arithmetic (approximate SFU reciprocals, own atan), FP64 row sums,
+//         BB inner products, move, renormalisation and fold; float32 state.
+//  kFP64: FP64 everywhere (IEEE division/sqrt/atan), FP64 master state.
+enum Precision : int { kFP32 = 0, kFP64 = 1 };
+
+// Per-source rows, structure of arrays (the reference's 48-byte Row, src/pairs.zig:11-15).
+struct Rows {
+  double4* force;     // xyz: left-tangent force, w: curvature
+  double* energy;     // Quey energy (own orbit excluded)
+  double* nearest;    // smallest squared chord to another orbit point
+  int* nearest_at;    // where it is: image index k*n+j (all pairs) or sorted site (near)
+};
+
+// Device-resident chart grid of one near pass, derived on the device from the shell.
+struct NearGrid {
+  float lower[3];
+  float cells_per_unit;     // sdim / width
+  float morton_per_unit;    // 32 / width
+  float width;
+  int sdim;
+  int sites;                // shell sites written (clamped to capacity)
+  unsigned int box_bits[6]; // ordered-bits min xyz, max xyz of site positions (next pass)
+  unsigned int overflow;    // a pass produced more sites than capacity
+  unsigned int pad;
+};
+
+// Device-resident BB step state (shaders/relax.wgsl:18-23), FP64 sums.
+struct RelaxDev {
+  int iteration;
+  unsigned int flags;               // 1 non-finite force, 2 duplicate orientation
+  unsigned long long step_bits;     // largest move (double bits, non-negative)
+  double sums[5];                   // s.y, y.y, s.s, f.f, energy
+  unsigned long long prefix[2];     // radix select: digit prefixes of the two middle ranks
+  unsigned long long rank[2];       // remaining ranks within the prefix
+  double median;
+  double alpha;
+  unsigned int ticket;              // last-block-done counter
+  unsigned int pad;
+};
+
+// Result of a row summary reduction (quick measures, src/pairs.zig:130-140).
+struct RowSummary {
+  double energy;     // sum of row energies
+  double force2;     // sum of |force|^2
+  double nearest;    // min nearest chord^2
+  int nearest_row;   // its source
+  unsigned int ticket;
+};
+
+}  // namespace zo
