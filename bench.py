@@ -1,0 +1,333 @@
+"""Benchmark of the QVM relaxation hot path on B200 (one JSON line on rank 0).
+
+Workload (the headline configuration): group O, N = 100,000 Haar-random orientations
+(seed 193, folded into the zone), near field of 20 mean orientation radii (~7,584
+neighbours per source, smooth fade from half the cutoff), Barzilai-Borwein steps with FP32
+pair arithmetic and FP64 BB products, sums and renormalisation. A step is one BB step over
+the resident sample: near-field force pass, BB statistics, exact median, move and fold.
+
+Metric: pair-evals/s counted as the reference counts them (src/engine.zig:905-907): per
+force pass N * min(N|K|, 0.94 delta^3 + 64). `value` is device time (CUDA events on the
+engine's stream, L2 flushed by a 256 MB memset before every step, outside the events);
+`e2e` goes through the public API with host buffers (import from pinned memory, relax,
+read the positions back). Multi-GPU: independent replicas, one per rank (weak scaling).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+GROUP, COUNT, SEED, DELTA, TAPER = "O", 100_000, 193, 20.0, 0.5
+ORDER = 24
+STEPS_PER_REQUEST = 100  # config: 100 BB steps
+FLUSH_BYTES = 256 * 1024 * 1024
+# Algorithmic FP32 operations of one windowed near-field Quey pair, counted from the
+# reference formulation (shaders/pairs.wgsl:250-262, 352-361, 403-409): chord tests and
+# dot products 23, near/far and the half-angle t 6, angle and the four powers 14, sine 5,
+# sign 2, direction 21, force/curvature/energy 14, window and its slope term 29,
+# accumulation 6; each add, multiply, divide, sqrt, atan, sin, min/max/select counts 1.
+FLOPS_PER_NEAR_PAIR = 120
+
+
+def neighbours(n, order, delta):
+    return min(n * order, 0.94 * delta ** 3 + 64) if delta > 0 else n * order
+
+
+EVALS_PER_PASS = COUNT * neighbours(COUNT, ORDER, DELTA)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- distributed plumbing
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import torch.distributed as dist
+            from datetime import timedelta
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group("gloo", timeout=timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def reduce(self, value, op):
+        if not self.pg:
+            return value
+        import torch
+
+        t = torch.tensor([float(value)], dtype=torch.float64)
+        self.pg.all_reduce(t, op={"max": self.pg.ReduceOp.MAX, "sum": self.pg.ReduceOp.SUM}[op])
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks during the timed region
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *_):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        loaded = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded or sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------- CPU baseline (the oracle port)
+def cpu_sample(budget_s=12.0, threads=None):
+    """Time the FP64 C restatement's near-field force rows on the host cores for a bounded
+    subset of the workload's sources; returns pair-evals/s and the sample description."""
+    from oracle import cref, qvm
+
+    ops = np.load(ROOT / "tests/golden/golden.npz")["ops_O"].astype(np.float32).astype(np.float64)
+    q = qvm.fold(qvm.haar(COUNT, SEED), qvm.GROUPS.index(GROUP), ops, f32=False)
+    threads = threads or cref.threads()
+    per = neighbours(COUNT, ORDER, DELTA)
+    probe = 256
+    t = time.perf_counter()
+    cref.near_rows(q, ops, DELTA, TAPER, nthreads=threads, count=probe)
+    t_probe = time.perf_counter() - t
+    count = int(min(COUNT, max(probe, probe * (budget_s / max(t_probe, 1e-3)) * 0.8)))
+    t = time.perf_counter()
+    cref.near_rows(q, ops, DELTA, TAPER, nthreads=threads, count=count)
+    dt = time.perf_counter() - t
+    return count * per / dt, threads, (f"FP64 near-field force rows of {count} of the {COUNT} sources "
+                                       f"(C/OpenMP restatement, shell+grid setup included), {dt:.1f} s")
+
+
+def run_reference(args, dist):
+    """Reference arm: the oracle port (the reference itself has no CPU path and cannot run
+    here), on the same workload, each step a bounded sample of one force pass."""
+    if dist.rank != 0:
+        return 0
+    from oracle import cref
+
+    budget = max(2.0, min(15.0, 150.0 / max(1, args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        cpu_sample(budget_s=budget / 4)
+    times, rates = [], []
+    desc, threads = "", cref.threads()
+    for _ in range(args.steps):
+        rate, threads, desc = cpu_sample(budget_s=budget)
+        rates.append(rate)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": "pair-evals/s", "value": value, "unit": "pair-evals/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": EVALS_PER_PASS / value * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config(args),
+        "cpu_baseline": {"value": value, "unit": "pair-evals/s", "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": "pair-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config(args):
+    return {"workload": f"QVM near-field relaxation, group {GROUP}, N={COUNT} Haar (seed {SEED}), "
+                        f"neighbourhood {DELTA:g} mean radii, taper {TAPER}",
+            "group": GROUP, "n": COUNT, "neighbourhood": DELTA, "steps_per_request": STEPS_PER_REQUEST,
+            "pair_evals_per_pass": EVALS_PER_PASS, "parallelism": f"replicas x{args.gpus}",
+            "l2": "flushed before every timed step (256 MB memset)",
+            "arithmetic": "FP32 pairs, FP64 sums/BB/renormalisation (fp32-refined)"}
+
+
+# ---------------------------------------------------------------- our arm
+def bench_engine(zo, precision, steps, warmup, seed):
+    grid = zo.haar(GROUP, COUNT, seed, precision=precision)
+    grid.relax(0, neighbourhood=DELTA)
+    out = np.zeros(4 + steps, np.float64)
+    grid._check(grid._lib.zo_bench(grid._handle, steps, warmup, float(FLUSH_BYTES),
+                                   out.ctypes.data_as(C.POINTER(C.c_double)), len(out)))
+    return grid, out
+
+
+def e2e_requests(zo, seed, requests):
+    """Public-API requests: import from pinned host memory, set the neighbourhood, relax
+    100 steps, read the positions back. Returns (pair-evals/s, latencies s, bytes)."""
+    import torch
+
+    base = zo.haar(GROUP, COUNT, seed)
+    start = base.quaternions
+    base.close()
+    pinned = torch.empty((COUNT, 4), dtype=torch.float32, pin_memory=True)
+    pinned.numpy()[:] = start
+    out = torch.empty((COUNT, 4), dtype=torch.float32, pin_memory=True)
+    grid = zo.Grid(GROUP, _empty=True)
+    lib, h = grid._lib, grid._handle
+    ptr = C.cast(pinned.data_ptr(), C.POINTER(C.c_float))
+
+    def request():
+        grid._check(lib.zo_set(h, 9, ptr, COUNT))
+        grid._check(lib.zo_relax_neighbourhood(h, DELTA))
+        grid._check(lib.zo_relax(h, STEPS_PER_REQUEST))
+        C.memmove(out.data_ptr(), lib.zo_quaternions(h), COUNT * 16)
+        return json.loads(lib.zo_stats(h))
+
+    request()  # warm-up
+    lat = []
+    for _ in range(requests):
+        t = time.perf_counter()
+        stats = request()
+        lat.append(time.perf_counter() - t)
+    grid.close()
+    evals = (STEPS_PER_REQUEST + 1) * EVALS_PER_PASS
+    return evals * len(lat) / sum(lat), lat, stats
+
+
+def traffic_from_profile():
+    """DRAM bytes per launch of the near-field row kernel from the committed ncu summary."""
+    path = ROOT / "profiles" / "near_rows_kernel.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def run_ours(args, dist):
+    os.environ["ZXTALORI_DEVICE"] = str(dist.local)
+    import zxtalori_b200 as zo
+
+    seed = SEED + dist.rank
+    # FP32-refined: the product path.
+    dist.barrier()
+    with Clocks(dist.local) as clocks:
+        grid, out = bench_engine(zo, "fp32", args.steps, args.warmup, seed)
+    total_ms = out[0]
+    per_step = out[4:4 + args.steps]
+    kernel_ms, kernel_launches, launches_per_step = out[1], out[2], out[3]
+    peak = grid._lib.zo_fp32_peak(grid._handle)
+    separation = grid.measure()["separation_deg"]
+    grid.close()
+    dist.barrier()
+    t_max = dist.reduce(total_ms, "max")
+    work = dist.reduce(args.steps * EVALS_PER_PASS, "sum")
+    value = work / (t_max / 1e3)
+    # Plain FP64 method on the same workload (fewer steps).
+    k64 = max(1, min(args.steps, 3))
+    g64, out64 = bench_engine(zo, "fp64", k64, 1, seed)
+    g64.close()
+    t64 = dist.reduce(out64[0], "max")
+    fp64_value = dist.reduce(k64 * EVALS_PER_PASS, "sum") / (t64 / 1e3)
+    # End to end through the public API.
+    e2e_value, lat, _ = e2e_requests(zo, seed, requests=2)
+    e2e_value = dist.reduce(e2e_value, "sum")
+    if dist.rank != 0:
+        return 0
+    kernel_avg_s = kernel_ms / max(1, kernel_launches) / 1e3
+    achieved = EVALS_PER_PASS * FLOPS_PER_NEAR_PAIR / kernel_avg_s / 1e12
+    traffic = traffic_from_profile()
+    cpu_value, cpu_threads, cpu_desc = cpu_sample() if args.gpus == 1 else (None, None, "rank 0 only at N=1")
+    line = {
+        "metric": "pair-evals/s", "value": value, "unit": "pair-evals/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config(args),
+        "latency_ms": {"step_p50": float(np.percentile(per_step, 50)), "step_p99": float(np.percentile(per_step, 99)),
+                       "request_p50": 1e3 * float(np.percentile(lat, 50)),
+                       "request_p99": 1e3 * float(np.percentile(lat, 99))},
+        "fp64_plain": {"value": fp64_value, "ms_per_step": t64 / k64, "steps": k64,
+                       "ratio_fp32_refined_over_fp64": value / fp64_value},
+        "separation_deg": separation,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "k_near32 (near-field rows)",
+                     "peak_source": "FP32 FMA probe on this GPU (zo_fp32_peak); MEASURED_PEAKS.json has no FP32 figure",
+                     "flops_per_pair": FLOPS_PER_NEAR_PAIR, "kernel_ms_avg": kernel_avg_s * 1e3},
+        "cpu_baseline": {"value": cpu_value, "unit": "pair-evals/s", "cores": cpu_threads, "kind": "port",
+                         "sample": cpu_desc},
+        "e2e": {"value": e2e_value, "unit": "pair-evals/s", "h2d_bytes_per_step": COUNT * 16,
+                "d2h_bytes_per_step": COUNT * 16,
+                "step": f"one request: import N quaternions from pinned host memory, relax {STEPS_PER_REQUEST} "
+                        f"steps (+1 closing force pass), read N quaternions back"},
+        "gpu_launches": int(round(launches_per_step * args.steps)),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, dist)
+        return run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

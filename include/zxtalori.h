@@ -107,6 +107,15 @@ const int32_t* zo_point_neighbours(void* h);
  *   Riesz 1, 2, 3, Green, log sums (the self pair's antipode not yet added), degenerate
  *   flag (width 12). */
 int zo_debug_rows(void* h, uint32_t what, double* out);
+/* Measurement hook (no reference counterpart): `steps` relaxation steps of the current
+ * sample after `warmup`, each timed with CUDA events on the engine's stream and preceded,
+ * outside its events, by a memset of flush_bytes (an L2 flush when larger than L2).
+ * out[0] total step ms, out[1] ms of the force pass's row kernel, out[2] its launches,
+ * out[3] kernel launches per step, out[4 ..] per-step ms while out_len allows. */
+int zo_bench(void* h, uint32_t steps, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len);
+/* Measurement hook (no reference counterpart): FP32 FMA throughput of the engine's device
+ * in TFLOP/s (2 flops per FMA), the denominator of the pair kernels' roofline; -1 on error. */
+double zo_fp32_peak(void* h);
 
 #ifdef __cplusplus
 }

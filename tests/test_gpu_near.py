@@ -1,0 +1,99 @@
+"""Near-field force pass on the GPU against the oracle (tests/test_near_field.py's checks).
+
+FP64 mode matches the dense FP64 near-field rows to 1e-10; FP32 mode to 2e-5 in force and
+curvature (relative to the largest), 1e-6 in energy, 1e-5 in the nearest chord. The stats
+energy of a near-field pass matches the reference's own dense model within its 2e-6.
+"""
+import numpy as np
+import pytest
+
+from conftest import GROUPS
+from oracle import cref, qvm
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp32": (2e-5, 2e-5, 1e-6, 1e-5), "fp64": (1e-10, 1e-10, 1e-10, 1e-10)}
+
+
+def compare(rows, o, precision):
+    tf, tc, te, tn = TOL[precision]
+    scale = np.linalg.norm(o["force"], axis=1).max()
+    assert np.linalg.norm(rows[:, :3] - o["force"], axis=1).max() / scale < tf
+    assert np.max(np.abs(rows[:, 3] - o["curvature"]) / o["curvature"].max()) < tc
+    assert np.max(np.abs(rows[:, 4] - o["energy"]) / np.maximum(o["energy"], 1e-300)) < te
+    assert np.max(np.abs(rows[:, 5] - o["nearest"]) / o["nearest"]) < tn
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("group,count", [("O", 600), ("D6", 500), ("C2", 400), ("I", 300), ("T", 400), ("D3", 400)])
+def test_near_rows_match_dense_oracle(engine, ops32, ops64, group, count, precision):
+    gid = GROUPS.index(group)
+    ops = ops32[group] if precision == "fp32" else ops64[group]
+    with engine.haar(group, count, 11, precision=precision) as grid:
+        grid.relax(0, neighbourhood=20)
+        rows = grid.debug_rows(0)
+        q = grid.quaternions.astype(np.float64) if precision == "fp32" else qvm.fold(qvm.haar(count, 11), gid, ops,
+                                                                                     f32=False)
+    compare(rows, qvm.near_rows(q, ops, 20), precision)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_near_rows_large_against_c_oracle(engine, ops32, ops64, precision):
+    group, count, gid = "O", 30000, 9
+    ops = ops32[group] if precision == "fp32" else ops64[group]
+    with engine.haar(group, count, 21, precision=precision) as grid:
+        grid.relax(0, neighbourhood=20)
+        rows = grid.debug_rows(0)
+        q = grid.quaternions.astype(np.float64) if precision == "fp32" else qvm.fold(qvm.haar(count, 21), gid, ops,
+                                                                                     f32=False)
+    compare(rows, cref.near_rows(q, ops, 20), precision)
+
+
+@pytest.mark.parametrize("group,count", [("O", 1000), ("D6", 1000), ("C2", 800)])
+def test_near_sums_match_dense_reference(engine, ops32, group, count):
+    """test_near_field.py:43-54 with its tolerances."""
+    with engine.haar(group, count, 11) as grid:
+        grid.relax(20)
+        grid.relax(1, neighbourhood=20)
+        stats = grid.stats
+        assert stats["energy_neighbourhood"] == 20 and stats["relax_neighbourhood"] == 20
+        q = grid.quaternions.astype(np.float64)
+        rows = qvm.near_rows(q, ops32[group], 20)
+        n, order = len(q), len(ops32[group])
+        assert stats["energy"] == pytest.approx(rows["energy"].sum() / (n * order * (n - 1)), rel=2e-6)
+        assert stats["separation_deg"] == pytest.approx(qvm.separation_deg(rows["nearest"].min()), rel=1e-4)
+        grid.relax(1, neighbourhood=0)
+        assert grid.stats["energy_neighbourhood"] is None
+
+
+def test_near_relaxation_approaches_all_pairs(engine):
+    """test_near_field.py:57-65."""
+    outcomes = {}
+    for delta in (0, 20):
+        with engine.haar("O", 1000, 7) as grid:
+            grid.relax(200, neighbourhood=delta)
+            grid.relax(0, neighbourhood=0)
+            grid.measure()
+            outcomes[delta] = grid.stats
+    assert outcomes[20]["energy"] == pytest.approx(outcomes[0]["energy"], rel=1e-5)
+    assert outcomes[20]["separation_deg"] > 0.95 * outcomes[0]["separation_deg"]
+
+
+def test_neighbourhood_range(engine):
+    with engine.haar("O", 200, 3) as grid:
+        with pytest.raises(RuntimeError, match="NeighbourhoodOutside2To1000"):
+            grid.relax(1, neighbourhood=1)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_near_relax_fp32_vs_fp64(engine, precision):
+    """The same 20 near-field steps in both modes: FP32 mode within 1e-6 of FP64 mode."""
+    results = {}
+    for mode in ("fp64", precision):
+        with engine.haar("O", 5000, 5, precision=mode) as grid:
+            grid.relax(20, neighbourhood=20)
+            results[mode] = (grid.stats, grid.quaternions.astype(np.float64))
+    (s64, q64), (s, q) = results["fp64"], results[precision]
+    assert s["energy"] == pytest.approx(s64["energy"], rel=1e-6)
+    assert s["separation_deg"] == pytest.approx(s64["separation_deg"], rel=1e-5)
+    assert np.minimum(np.linalg.norm(q - q64, axis=1), np.linalg.norm(q + q64, axis=1)).max() < 2e-5

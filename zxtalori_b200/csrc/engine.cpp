@@ -711,6 +711,60 @@ void Engine::debug_rows(uint32_t what, double* out) {
   }
 }
 
+void Engine::bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len) {
+  if (n_ < 2) throw Failure("TooFewOrientations");
+  if (steps == 0 || out_len < 4) throw Failure("InvalidBench");
+  ZO_CUDA(cudaSetDevice(device_));
+  sync_neighbourhood();
+  relax_state_.prepare((int)n_, prec_);
+  for (uint32_t w = 0; w < warmup; ++w)
+    relax_state_.step(stream_, prec_, q32(), q64(), (int)n_, group_, fixed_arg(), budget_scale_, sms_);
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  DeviceBuffer flush;
+  const size_t fbytes = flush_bytes > 0 ? (size_t)flush_bytes : 0;
+  if (fbytes) flush.ensure(fbytes);
+  std::vector<cudaEvent_t> ev(4 * (size_t)steps);
+  for (auto& e : ev) ZO_CUDA(cudaEventCreate(&e));
+  LaunchProbe probe;
+  probe.events = ev.data() + 2 * (size_t)steps;
+  probe.capacity = 2 * (int)steps;
+  t_probe = &probe;
+  try {
+    for (uint32_t k = 0; k < steps; ++k) {
+      if (fbytes) ZO_CUDA(cudaMemsetAsync(flush.as<void>(), (int)(k & 0xff), fbytes, stream_));
+      ZO_CUDA(cudaEventRecord(ev[2 * k], stream_));
+      relax_state_.step(stream_, prec_, q32(), q64(), (int)n_, group_, fixed_arg(), budget_scale_, sms_);
+      ZO_CUDA(cudaEventRecord(ev[2 * k + 1], stream_));
+    }
+  } catch (...) {
+    t_probe = nullptr;
+    throw;
+  }
+  t_probe = nullptr;
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  double total = 0, kernel = 0;
+  for (uint32_t k = 0; k < steps; ++k) {
+    float ms = 0;
+    ZO_CUDA(cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]));
+    total += ms;
+    if (4 + k < out_len) out[4 + k] = ms;
+  }
+  for (int k = 0; k + 1 < probe.used; k += 2) {
+    float ms = 0;
+    ZO_CUDA(cudaEventElapsedTime(&ms, probe.events[k], probe.events[k + 1]));
+    kernel += ms;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  out[0] = total;
+  out[1] = kernel;
+  out[2] = probe.used / 2;
+  out[3] = (double)probe.launches / steps;
+  iteration_ += warmup + steps;
+  relax_state_.current = false;
+  measures_.reset();
+  fetch();
+}
+
 const float* Engine::point_values(uint32_t kind) const {
   if (kind != 0 || !point_separation_iteration_ || point_separation_.size() != n_) return nullptr;
   return point_separation_.data();

@@ -152,6 +152,18 @@ class Engine {
   // Development: one pass's raw rows to host. what 0: force pass of the relaxation
   // (8 doubles per source), 1: full measure rows (12 doubles per source).
   void debug_rows(uint32_t what, double* out);
+  // Measurement: `steps` relaxation steps after `warmup`, each bracketed by CUDA events on
+  // the engine's stream with an L2 flush (a memset of flush_bytes) before it, outside the
+  // events. out[0] total step ms, out[1] dominant-kernel ms, out[2] its launches, out[3]
+  // kernel launches per step, out[4 ..] each step's ms (as room allows).
+  void bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len);
+  // Measured FP32 FMA throughput of this engine's device, TFLOP/s.
+  double fp32_peak() {
+    ZO_CUDA(cudaSetDevice(device_));
+    double t = 0;
+    ZO_CUDA(measure_fp32_peak(sms_, &t));
+    return t;
+  }
 
   int group() const { return group_; }
   uint32_t count() const { return n_; }

@@ -152,4 +152,14 @@ int zo_debug_rows(void* h, uint32_t what, double* out) {
   return guarded(h, "Rows", [&](Engine& e) { e.debug_rows(what, out); });
 }
 
+int zo_bench(void* h, uint32_t steps, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len) {
+  return guarded(h, "Bench", [&](Engine& e) { e.bench(steps, warmup, flush_bytes, out, out_len); });
+}
+
+double zo_fp32_peak(void* h) {
+  double value = -1.0;
+  if (guarded(h, "Probe", [&](Engine& e) { value = e.fp32_peak(); }) != 0) return -1.0;
+  return value;
+}
+
 }  // extern "C"

@@ -275,7 +275,10 @@ struct WarpBox {
 };
 
 // The warp's chart box and the cells within chart reach d of it (pairs.wgsl:368-379):
-// chart distance = chord/2 sqrt((1+|p|^2)(1+|p'|^2)), bounded by fixed-point iteration.
+// chart distance = chord/2 sqrt((1+|p|^2)(1+|p'|^2)), bounded by fixed-point iteration from
+// below. When the cutoff is wide (C2 at small N, r near 1.5) the iteration has no fixed point
+// and four steps fall short; then the bound with |p'| at the chart box's farthest corner
+// (every site lies in the box) is used instead.
 __device__ __forceinline__ bool warp_box(float3 pos, bool live, const NearGrid& g, float chord, WarpBox& b) {
   float v[6] = {live ? pos.x : 3e38f, live ? pos.y : 3e38f, live ? pos.z : 3e38f,
                 live ? pos.x : -3e38f, live ? pos.y : -3e38f, live ? pos.z : -3e38f};
@@ -292,6 +295,14 @@ __device__ __forceinline__ bool warp_box(float3 pos, bool live, const NearGrid& 
   const float reach = sqrtf(r2), lift = 1.0f + reach * reach;
   float d = 0.5f * chord * lift;
   for (int k = 0; k < 4; ++k) d = 0.5f * chord * sqrtf(lift * (1.0f + (reach + d) * (reach + d)));
+  if (0.5f * chord * sqrtf(lift * (1.0f + (reach + d) * (reach + d))) > d * 1.001f) {
+    float p2 = 0.f;
+    for (int a = 0; a < 3; ++a) {
+      const float m = fmaxf(fabsf(g.lower[a]), fabsf(g.lower[a] + g.width));
+      p2 += m * m;
+    }
+    d = 0.5f * chord * sqrtf(lift * (1.0f + p2));
+  }
   d = d * 1.01f + 1e-6f;
   b.d = d;
   for (int a = 0; a < 3; ++a) {
@@ -535,6 +546,7 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   const dim3 grid((warps + kNearWarps - 1) / kNearWarps, L.slices);
   NearCut cut{L.cut2, L.chord, L.cut_z, L.cut_w};
   const Rows dst = L.partial;
+  probe_mark(s);
   if (fp64) {
     if (L.track) k_near64<true><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
     else k_near64<false><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
@@ -542,7 +554,11 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
     if (L.track) k_near32<true><<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
     else k_near32<false><<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
   }
+  probe_mark(s);
   k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(L.partial, n, L.slices, n, (const int*)L.src_perm, L.out, L.track ? 1 : 0);
+  // shell count, shell write, grid, cell count, scatter, bucket sort, site gather, source
+  // count, scatter, bucket sort, gather, reduce (scans counted by launch_scan; memsets aside)
+  probe_count(12);
   return cudaGetLastError();
 }
 

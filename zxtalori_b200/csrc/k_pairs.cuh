@@ -179,6 +179,7 @@ cudaError_t launch_scan(const uint32_t* in, uint32_t* out, int max_count, const 
   k_scan_tiles<<<tiles, 1024, 0, s>>>(in, out, max_count, count_dev, block_sums);
   k_scan_sums<<<1, 1024, 0, s>>>(block_sums, out, max_count, count_dev);
   if (max_count > kScanTile) k_scan_add<<<(max_count + 255) / 256, 256, 0, s>>>(out, max_count, count_dev, block_sums);
+  probe_count(max_count > kScanTile ? 3 : 2);
   return cudaGetLastError();
 }
 
@@ -382,6 +383,7 @@ cudaError_t launch_pairs(int prec, bool track, const float4* q32, const double4*
   const dim3 grid(pl.jtiles, pl.chunks);
   const bool direct = pl.chunks == 1;
   Rows dst = direct ? out : partial;
+  probe_mark(s);
   if (prec == kFP64) {
     if (track) k_pairs64<true><<<grid, kPairBlock, 0, s>>>(q64, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, n);
     else k_pairs64<false><<<grid, kPairBlock, 0, s>>>(q64, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, n);
@@ -389,6 +391,8 @@ cudaError_t launch_pairs(int prec, bool track, const float4* q32, const double4*
     if (track) k_pairs32<true><<<grid, kPairBlock, 0, s>>>(q32, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, n);
     else k_pairs32<false><<<grid, kPairBlock, 0, s>>>(q32, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, n);
   }
+  probe_mark(s);
+  probe_count(direct ? 1 : 2);
   if (!direct) k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(partial, n, pl.chunks, n, nullptr, out, track ? 1 : 0);
   return cudaGetLastError();
 }
@@ -402,11 +406,13 @@ cudaError_t launch_haar(float4* q, int n, uint32_t seed, cudaStream_t s) {
   x *= 0x846ca68bu;
   x ^= x >> 16;
   k_haar<<<(n + 255) / 256, 256, 0, s>>>(q, n, x);
+  probe_count();
   return cudaGetLastError();
 }
 
 cudaError_t launch_fold(float4* q32, double4* q64, int n, int gid, int prec, bool from_q32, cudaStream_t s) {
   k_fold<<<(n + 255) / 256, 256, 0, s>>>(q32, q64, n, gid, prec, from_q32 ? 1 : 0);
+  probe_count();
   return cudaGetLastError();
 }
 

@@ -15,9 +15,12 @@
 
 namespace zo {
 
+thread_local LaunchProbe* t_probe = nullptr;
+
 cudaError_t launch_relax_stats(Rows rows, const double4* prev_f, const double4* prev_d, int n, int fixed,
                                double* partials, RelaxDev* st, cudaStream_t s) {
   k_relax_stats<<<reduce_blocks(n), kRelaxBlock, 0, s>>>(rows, prev_f, prev_d, n, fixed, partials, st);
+  probe_count();
   return cudaGetLastError();
 }
 
@@ -26,8 +29,10 @@ cudaError_t launch_median(int prec, Rows rows, int n, RelaxDev* st, unsigned int
   const int blocks = max(1, min((n + 255) / 256, 2 * sms));
   if (prec == kFP64) {
     for (int r = 0; r < 8; ++r) k_median_round<true><<<blocks, 256, 0, s>>>(rows, n, r, st, hist, alpha0, radius);
+    probe_count(8);
   } else {
     for (int r = 0; r < 4; ++r) k_median_round<false><<<blocks, 256, 0, s>>>(rows, n, r, st, hist, alpha0, radius);
+    probe_count(4);
   }
   return cudaGetLastError();
 }
@@ -36,6 +41,7 @@ cudaError_t launch_move_fold(float4* q32, double4* q64, int n, int gid, int prec
                              double4* prev_d, RelaxDev* st, int fixed, double radius, double step_scale, cudaStream_t s) {
   k_move_fold<<<(n + 127) / 128, 128, 0, s>>>(q32, q64, n, gid, prec, rows, prev_f, prev_d, st, fixed, radius,
                                               step_scale);
+  probe_count();
   return cudaGetLastError();
 }
 
@@ -53,6 +59,45 @@ cudaError_t launch_nearest_degrees(const double* nearest, int n, float* out, cud
 cudaError_t launch_refine_nearest(const float4* q32, int n, int gid, Rows rows, bool near_sites, const uint32_t* scode,
                                   const uint32_t* simg, int* neighbour, cudaStream_t s) {
   k_refine_nearest<<<(n + 255) / 256, 256, 0, s>>>(q32, n, gid, rows, near_sites ? 1 : 0, scode, simg, neighbour);
+  return cudaGetLastError();
+}
+
+// FP32 FMA throughput probe: 8 independent FMA chains per thread (latency hidden by ILP and
+// occupancy), the result stored so nothing is eliminated. 16 flops per thread per iteration.
+__global__ void __launch_bounds__(256) k_fma_probe(float* out, int iterations, float seed) {
+  float a[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) a[c] = seed + (float)(threadIdx.x + c);
+  const float m = 0.999999f, b = 1e-7f;
+  for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) a[c] = fmaf(a[c], m, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) s += a[c];
+  if (s == 12345.678f) out[blockIdx.x] = s;
+}
+
+cudaError_t measure_fp32_peak(int sms, double* tflops) {
+  float* out = nullptr;
+  cudaError_t e = cudaMalloc(&out, sizeof(float) * sms * 64);
+  if (e) return e;
+  const int blocks = sms * 8, iterations = 1 << 16;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  k_fma_probe<<<blocks, 256>>>(out, 1024, 1.0f);
+  cudaEventRecord(a);
+  for (int r = 0; r < 4; ++r) k_fma_probe<<<blocks, 256>>>(out, iterations, 1.0f + r);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  *tflops = 4.0 * blocks * 256.0 * iterations * 16.0 / (ms * 1e-3) / 1e12;
   return cudaGetLastError();
 }
 

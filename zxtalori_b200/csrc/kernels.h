@@ -82,7 +82,27 @@ cudaError_t launch_refine_nearest(const float4* q32, int n, int gid, Rows rows, 
 cudaError_t launch_neighbour_index(Rows rows, int n, bool near_sites, const uint32_t* scode, int* neighbour,
                                    cudaStream_t s);
 
+// Measured FP32 FMA throughput of the current device (TFLOP/s, 2 flops per FMA).
+cudaError_t measure_fp32_peak(int sms, double* tflops);
+
 // Blocks used by the row-summary and stats reductions for n rows.
 inline int reduce_blocks(int n) { return (n + 255) / 256; }
+
+// Measurement hook: while set (on the launching thread), launchers count their kernel
+// launches and bracket the pass's dominant kernel (the all-pairs or near-field row kernel)
+// with the next pair of events from `events`.
+struct LaunchProbe {
+  long long launches = 0;
+  cudaEvent_t* events = nullptr;
+  int capacity = 0;  // events available (pairs * 2)
+  int used = 0;
+};
+extern thread_local LaunchProbe* t_probe;
+inline void probe_count(int k = 1) {
+  if (t_probe) t_probe->launches += k;
+}
+inline void probe_mark(cudaStream_t s) {
+  if (t_probe && t_probe->events && t_probe->used < t_probe->capacity) cudaEventRecord(t_probe->events[t_probe->used++], s);
+}
 
 }  // namespace zo
