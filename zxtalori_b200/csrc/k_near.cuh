@@ -8,7 +8,7 @@
 //      counted, scanned and written in (source, image) order - deterministic sites;
 //   2. the sites' stereographic chart box, a grid of sdim^3 cells, a counting sort of the
 //      sites into row-major cells with each cell ordered by site index;
-//   3. sources counting-sorted into a 32^3 Morton grid (then by index), so 32 consecutive
+//   3. sources counting-sorted into a 64^3 Morton grid (then by index), so 32 consecutive
 //      sources are close together;
 //   4. one warp per 32 sources and slice: the warp's chart box, the cell rows within the
 //      chart reach of the cutoff chord, each row's x-run trimmed; runs stream through shared
@@ -238,7 +238,8 @@ __global__ void k_site_gather(const uint32_t* __restrict__ perm, const NearGrid*
 }
 
 // ------------------------------------------------------------------ 3. sources in Morton order
-__device__ __forceinline__ uint32_t spread5(uint32_t v) {
+// Bits of v moved three apart (a Morton code's interleave), for up to 10-bit coordinates.
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
   uint32_t x = v & 0x3ffu;
   x = (x | (x << 16)) & 0x030000ffu;
   x = (x | (x << 8)) & 0x0300f00fu;
@@ -256,7 +257,7 @@ __global__ void k_source_count(const float4* __restrict__ q32, const double4* __
   const float u = gp->morton_per_unit;
   const uint32_t cx = cell_axis(p.x, gp->lower[0], u, kMortonDim), cy = cell_axis(p.y, gp->lower[1], u, kMortonDim),
                  cz = cell_axis(p.z, gp->lower[2], u, kMortonDim);
-  const uint32_t m = spread5(cx) | (spread5(cy) << 1) | (spread5(cz) << 2);
+  const uint32_t m = spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2);
   code[i] = m;
   rank[i] = atomicAdd(&counts[m], 1u);
 }
@@ -332,6 +333,12 @@ __device__ __forceinline__ bool row_run(const WarpBox& b, const NearGrid& g, con
   return start < end;
 }
 
+// The gather (pairs.wgsl:363-416). Each lane holds one source; the warp streams its
+// cell-row runs through shared memory 32 sites at a time (quaternion, |y|^2 and code) and
+// every lane tests its source against each site. For a site within the cutoff chord the
+// windowed pair runs with dp2 = 2(|x|^2+|y|^2) - dm2 (parallelogram law; the site is the
+// near twin), and the force is kept as sum c (x - y), turned into a force once per source.
+// Tile sums are FP32 (FP64 in FP64 mode), merged into FP64 per tile.
 template <bool TRACK>
 __global__ void __launch_bounds__(kNearWarps * 32) k_near32(const float4* __restrict__ q, int n,
                                                               const uint32_t* __restrict__ src_perm,
@@ -341,7 +348,7 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near32(const float4* __rest
                                                               const NearGrid* __restrict__ gp, NearCut cut, int slices,
                                                               Rows out, int stride) {
   __shared__ float4 tq[kNearWarps][32];
-  __shared__ uint32_t tc[kNearWarps][32];
+  __shared__ float2 tm[kNearWarps][32];  // |y|^2, code bits
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int warp = blockIdx.x * kNearWarps + w;
   const int slice = blockIdx.y;
@@ -354,7 +361,8 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near32(const float4* __rest
   WarpBox box;
   if (!warp_box(chart(x), live, g, (float)cut.chord, box)) return;
   const float cut2 = (float)cut.cut2, cz = (float)cut.cut_z, cw = (float)cut.cut_w;
-  double f1 = 0, f2 = 0, f3 = 0, fc = 0, fe = 0;
+  const float nx2 = 2.0f * fmaf(x.x, x.x, fmaf(x.y, x.y, fmaf(x.z, x.z, x.w * x.w)));
+  double yw = 0, yx = 0, yy = 0, yz = 0, fc = 0, fe = 0;
   float best = 4.0f;
   int best_at = -1;
   const int ny = box.chi[1] - box.clo[1] + 1, nz = box.chi[2] - box.clo[2] + 1;
@@ -366,18 +374,21 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near32(const float4* __rest
       const int count = (int)min(32u, end - base);
       __syncwarp();
       if (lane < count) {
-        tq[w][lane] = sq[base + lane];
-        tc[w][lane] = scode[base + lane];
+        const float4 s = sq[base + lane];
+        tq[w][lane] = s;
+        tm[w][lane] = make_float2(2.0f * fmaf(s.x, s.x, fmaf(s.y, s.y, fmaf(s.z, s.z, s.w * s.w))),
+                                  __uint_as_float(scode[base + lane]));
       }
       __syncwarp();
       if (!live) continue;
-      float s1 = 0.f, s2 = 0.f, s3 = 0.f, sc = 0.f, se = 0.f;
+      float sw = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, sc = 0.f, se = 0.f;
       for (int t = 0; t < count; ++t) {
         const float4 y = tq[w][t];
         const float mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
         const float dm2 = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
         if (dm2 > cut2) continue;
-        const uint32_t code = tc[w][t];
+        const float2 m = tm[w][t];
+        const uint32_t code = __float_as_uint(m.y);
         if ((code & ~kIdentityBit) == i) {
           if (code == i && dm2 < best) {
             best = dm2;
@@ -385,32 +396,35 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near32(const float4* __rest
           }
           continue;
         }
-        if (dm2 < best) {
-          best = dm2;
-          if (TRACK) best_at = (int)(base + t);
+        if (TRACK) {
+          if (dm2 < best) {
+            best = dm2;
+            best_at = (int)(base + t);
+          }
+        } else {
+          best = fminf(best, dm2);
         }
-        const float pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
-        const float dp2 = fmaf(pw, pw, fmaf(px, px, fmaf(py, py, pz * pz)));
-        PairF pr = quey_pair32(dm2, dp2);
-        window32(pr, dm2, dp2, cz, cw);
-        float d1, d2, d3;
-        pair_direction(x, y, d1, d2, d3);
-        s1 = fmaf(pr.coef, d1, s1);
-        s2 = fmaf(pr.coef, d2, s2);
-        s3 = fmaf(pr.coef, d3, s3);
-        sc += pr.curv;
-        se += pr.energy;
+        float c, cv, e;
+        near_pair32(dm2, nx2 + m.x - dm2, cz, cw, c, cv, e);
+        sw = fmaf(c, mw, sw);
+        sx = fmaf(c, mx, sx);
+        sy = fmaf(c, my, sy);
+        sz = fmaf(c, mz, sz);
+        sc += cv;
+        se += e;
       }
-      f1 += s1;
-      f2 += s2;
-      f3 += s3;
+      yw += sw;
+      yx += sx;
+      yy += sy;
+      yz += sz;
       fc += sc;
       fe += se;
     }
   }
   if (!live) return;
+  const double3 f = force_from_differences(to_d4(x), make_double4(yw, yx, yy, yz));
   const size_t at = (size_t)slice * stride + p;
-  out.force[at] = make_double4(f1, f2, f3, fc);
+  out.force[at] = make_double4(f.x, f.y, f.z, fc);
   out.energy[at] = fe;
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;
@@ -425,6 +439,7 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near64(const double4* __res
                                                               const NearGrid* __restrict__ gp, NearCut cut, int slices,
                                                               Rows out, int stride) {
   __shared__ double4 tq[kNearWarps][32];
+  __shared__ double tn[kNearWarps][32];
   __shared__ uint32_t tc[kNearWarps][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int warp = blockIdx.x * kNearWarps + w;
@@ -437,7 +452,8 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near64(const double4* __res
   const NearGrid g = *gp;
   WarpBox box;
   if (!warp_box(chart(x), live, g, (float)cut.chord, box)) return;
-  double f1 = 0, f2 = 0, f3 = 0, fc = 0, fe = 0, best = 4.0;
+  const double nx2 = 2.0 * dot4(x, x);
+  double yw = 0, yx = 0, yy = 0, yz = 0, fc = 0, fe = 0, best = 4.0;
   int best_at = -1;
   const int ny = box.chi[1] - box.clo[1] + 1, nz = box.chi[2] - box.clo[2] + 1;
   const int rows = ny * nz;
@@ -448,7 +464,9 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near64(const double4* __res
       const int count = (int)min(32u, end - base);
       __syncwarp();
       if (lane < count) {
-        tq[w][lane] = sq[base + lane];
+        const double4 s = sq[base + lane];
+        tq[w][lane] = s;
+        tn[w][lane] = 2.0 * dot4(s, s);
         tc[w][lane] = scode[base + lane];
       }
       __syncwarp();
@@ -470,23 +488,22 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near64(const double4* __res
           best = dm2;
           if (TRACK) best_at = (int)(base + t);
         }
-        const double pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
-        const double dp2 = pw * pw + px * px + py * py + pz * pz;
+        const double dp2 = nx2 + tn[w][t] - dm2;
         PairD pr = quey_pair64(dm2, dp2);
         window64(pr, dm2, dp2, cut.cut_z, cut.cut_w);
-        double d1, d2, d3;
-        pair_direction(x, y, d1, d2, d3);
-        f1 += pr.coef * d1;
-        f2 += pr.coef * d2;
-        f3 += pr.coef * d3;
+        yw += pr.coef * mw;
+        yx += pr.coef * mx;
+        yy += pr.coef * my;
+        yz += pr.coef * mz;
         fc += pr.curv;
         fe += pr.energy;
       }
     }
   }
   if (!live) return;
+  const double3 f = force_from_differences(x, make_double4(yw, yx, yy, yz));
   const size_t at = (size_t)slice * stride + p;
-  out.force[at] = make_double4(f1, f2, f3, fc);
+  out.force[at] = make_double4(f.x, f.y, f.z, fc);
   out.energy[at] = fe;
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;

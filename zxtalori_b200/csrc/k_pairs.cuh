@@ -202,8 +202,8 @@ __device__ __forceinline__ PairTile pair_tile(int tile, int jtiles, int n) {
 // but the identity self pair. TRACK keeps the first image index of the nearest chord.
 template <bool TRACK, bool CHECK>
 __device__ __forceinline__ void pairs32_tile(const float4 x, const float4* tile, int count, int i, int j0, int k, int n,
-                                             float& s1, float& s2, float& s3, float& sc, float& se, float& best,
-                                             int& best_at) {
+                                             float& sw, float& sx, float& sy, float& sz, float& sc, float& se,
+                                             float& best, int& best_at) {
 #pragma unroll 2
   for (int t = 0; t < count; ++t) {
     const float4 y = tile[t];
@@ -225,11 +225,14 @@ __device__ __forceinline__ void pairs32_tile(const float4 x, const float4* tile,
     }
     if (own) continue;
     const PairF p = quey_pair32(dm2, dp2);
-    float d1, d2, d3;
-    pair_direction(x, y, d1, d2, d3);
-    s1 = fmaf(p.coef, d1, s1);
-    s2 = fmaf(p.coef, d2, s2);
-    s3 = fmaf(p.coef, d3, s3);
+    // dir(y) = -dir(x - y) = dir(x + y): accumulate the near twin's short difference,
+    // c (x - y) or -c (x + y), turned into -dir(sum) per source (force_from_differences).
+    const bool minus = dm2 <= dp2;
+    const float cs = minus ? p.coef : -p.coef;
+    sw = fmaf(cs, minus ? mw : pw, sw);
+    sx = fmaf(cs, minus ? mx : px, sx);
+    sy = fmaf(cs, minus ? my : py, sy);
+    sz = fmaf(cs, minus ? mz : pz, sz);
     sc += p.curv;
     se += p.energy;
   }
@@ -243,7 +246,7 @@ __global__ void __launch_bounds__(kPairBlock) k_pairs32(const float4* __restrict
   const int i = i0 + threadIdx.x;
   const bool live = i < n;
   const float4 x = live ? q[i] : make_float4(1.f, 0.f, 0.f, 0.f);
-  double f1 = 0, f2 = 0, f3 = 0, fc = 0, fe = 0;
+  double yw = 0, yx = 0, yy = 0, yz = 0, fc = 0, fe = 0;
   float best = 4.0f;
   int best_at = -1;
   const int t0 = blockIdx.y * tiles_per_chunk, t1 = min(total_tiles, t0 + tiles_per_chunk);
@@ -253,20 +256,22 @@ __global__ void __launch_bounds__(kPairBlock) k_pairs32(const float4* __restrict
     if ((int)threadIdx.x < pt.count) tile[threadIdx.x] = image32(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0);
     __syncthreads();
     if (!live) continue;
-    float s1 = 0.f, s2 = 0.f, s3 = 0.f, sc = 0.f, se = 0.f;
+    float sw = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, sc = 0.f, se = 0.f;
     if (pt.j0 < i0 + kPairBlock && i0 < pt.j0 + pt.count)
-      pairs32_tile<TRACK, true>(x, tile, pt.count, i, pt.j0, pt.k, n, s1, s2, s3, sc, se, best, best_at);
+      pairs32_tile<TRACK, true>(x, tile, pt.count, i, pt.j0, pt.k, n, sw, sx, sy, sz, sc, se, best, best_at);
     else
-      pairs32_tile<TRACK, false>(x, tile, pt.count, i, pt.j0, pt.k, n, s1, s2, s3, sc, se, best, best_at);
-    f1 += s1;
-    f2 += s2;
-    f3 += s3;
+      pairs32_tile<TRACK, false>(x, tile, pt.count, i, pt.j0, pt.k, n, sw, sx, sy, sz, sc, se, best, best_at);
+    yw += sw;
+    yx += sx;
+    yy += sy;
+    yz += sz;
     fc += sc;
     fe += se;
   }
   if (!live) return;
   const size_t at = (size_t)blockIdx.y * stride + i;
-  out.force[at] = make_double4(f1, f2, f3, fc);
+  const double3 f = force_from_differences(to_d4(x), make_double4(yw, yx, yy, yz));
+  out.force[at] = make_double4(f.x, f.y, f.z, fc);
   out.energy[at] = fe;
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;

@@ -125,6 +125,45 @@ __device__ __forceinline__ PairF quey_pair32(float dm2, float dp2) {
   return p;
 }
 
+// Windowed near-field pair, FP32, for a site that is the near twin (dm2 <= cut < 2 <= dp2,
+// so the sign is +1, near = dm2 and far = dp2): the coefficient c of the pair's direction
+// (force contribution c * dir), its windowed curvature and energy. Same arithmetic as
+// quey_pair32 followed by window32.
+__device__ __forceinline__ void near_pair32(float dm2, float dp2, float cut_z, float cut_w, float& coef, float& curv,
+                                            float& energy) {
+  const float t2 = fmaxf(dm2, 1e-30f) * rcp_approx(dp2);
+  const float t = sqrt_approx(t2);
+  const float a = fmaxf(two_atan_unit(t, t2), 1e-12f);
+  const float b = kPiF - a;
+  const float aa = a * a, bb = b * b;
+  const float a2 = aa + 1e-9f, b2 = bb + 1e-9f;
+  const float a3 = fmaf(aa, a, 1e-9f), b3 = fmaf(bb, b, 1e-9f);
+  const float onept2 = 1.0f + t2;
+  const float sp = fmaf(1e-9f, onept2, t + t);
+  const float a2b2 = a2 * b2;
+  const float r1 = rcp_approx(a2b2 * sp);
+  const float along = (b2 - a2) * onept2 * r1;
+  const float ab = a * b;
+  const float a3b3 = a3 * b3;
+  const float r2 = rcp_approx(a3b3 * ab);
+  const float e = kPiF * a3b3 * r2;
+  const float s = __saturatef((a - cut_z) * cut_w);
+  const float w = fmaf(-s * s, fmaf(-2.0f, s, 3.0f), 1.0f);
+  const float slope = -6.0f * s * (1.0f - s) * cut_w;
+  coef = fmaf(-w, along, e * slope * (onept2 * a2b2 * r1));
+  curv = (a3 + b3) * ab * r2 * w;
+  energy = e * w;
+}
+
+// The force of a source from the accumulated sum Y = sum_k c_k (x - y_k): the direction
+// vec(y x^-1) is linear in y and vanishes at y = x, so sum_k c_k dir_k = -dir(Y). Summing
+// the short difference vectors keeps the precision of summing the directions themselves.
+__device__ __forceinline__ double3 force_from_differences(double4 x, double4 y) {
+  double d1, d2, d3;
+  pair_direction(x, y, d1, d2, d3);
+  return make_double3(-d1, -d2, -d3);
+}
+
 // The same pair in FP64 with IEEE division, sqrt and atan: the plain method's arithmetic.
 struct PairD {
   double coef, curv, energy, a;

@@ -8,7 +8,9 @@ constexpr int kMaxOperatorRows = 141;   // sum of |K| over the eleven groups
 constexpr int kMaxPlaneRows = 271;      // sum of 2|K|-1 zone bisector planes
 constexpr uint32_t kIdentityBit = 0x80000000u;  // site code: the source's identity image
 constexpr int kMaxCellDim = 128;        // chart grid side (src/near.zig:135)
-constexpr int kMortonDim = 32;          // sources' Morton grid side (src/near.zig:23)
+// Sources' Morton grid side. The reference uses 32 (src/near.zig:23); 64 keeps 32
+// consecutive sources (one warp) about half as wide at N = 100k, so fewer candidate sites.
+constexpr int kMortonDim = 64;
 
 // Precision of one sample's arithmetic.
 //  kFP32: FP32 pair arithmetic (approximate SFU reciprocals, own atan), FP64 row sums,
