@@ -117,6 +117,25 @@ int zo_bench(void* h, uint32_t steps, uint32_t warmup, double flush_bytes, doubl
  * in TFLOP/s (2 flops per FMA), the denominator of the pair kernels' roofline; -1 on error. */
 double zo_fp32_peak(void* h);
 
+/* No counterpart in the reference. The all-pairs force pass (FP32 pair arithmetic, FP64
+ * sums) for callers that cannot allocate device memory: a framework that owns every
+ * allocation through its own pool, a caller with a fixed pre-reserved budget, or a thread
+ * that must not risk an allocation's synchronisation. It needs no engine handle and
+ * allocates nothing; its scratch (the per-chunk partial rows) is a fixed array compiled
+ * into the library, 3 MiB per GPU that loads the library, held until the process exits.
+ *   q_device:    n float32 quaternions [n][4] on the current device (16-byte aligned),
+ *                zone representatives as zo_quaternions returns them;
+ *   rows_device: n * 6 doubles on the device (32-byte aligned), written as: [0, 4n) per
+ *                source force x, y, z and curvature; [4n, 5n) Quey energy; [5n, 6n)
+ *                smallest squared chord to another orbit point;
+ *   stream:      the cudaStream_t to run on (NULL: the default stream).
+ * Returns 0, or -1 bad argument, -2 n outside 1..65,536 (the scratch's limit), -3 CUDA
+ * error; the message goes to `error` (error_len bytes) when given. The first call on a
+ * device sets it up (scratch address, group tables); make it before any stream capture.
+ * Calls share the scratch: calls that overlap on the GPU race and must be serialised. */
+int zo_pair_rows_noalloc(uint32_t group, const float* q_device, uint32_t n, double* rows_device, void* stream,
+                         char* error, size_t error_len);
+
 #ifdef __cplusplus
 }
 #endif
