@@ -99,7 +99,7 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   cap = std::max<uint64_t>(cap, (uint64_t)total);
   if (cap > (1ull << 31) - 1) throw Failure("NearShellTooLarge");
   capacity_ = (int)cap;
-  sdim_max_ = (int)std::lround(std::cbrt((double)capacity_ / 8.0));
+  sdim_max_ = (int)std::lround(std::cbrt((double)capacity_ / kSitesPerCell));
   sdim_max_ = std::max(1, std::min(sdim_max_, kMaxCellDim));
   const size_t cells = (size_t)sdim_max_ * sdim_max_ * sdim_max_ + 1;
   const size_t qsize = prec == kFP64 ? sizeof(double4) : sizeof(float4);
@@ -115,7 +115,7 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   sq_.ensure(capacity_ * qsize);
   scode_.ensure(capacity_ * 4ull);
   simg_.ensure(capacity_ * 4ull);
-  const size_t mcells = (size_t)kMortonDim * kMortonDim * kMortonDim + 1;
+  const size_t mcells = (size_t)kOrderDim * kOrderDim * kOrderDim + 1;
   src_key_.ensure((size_t)n * 4);
   src_rank_.ensure((size_t)n * 4);
   mcount_.ensure(mcells * 4);
@@ -148,6 +148,7 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
   L.sdim_max = sdim_max_;
   L.slices = slices_;
   L.track = track;
+  L.short_atan = radius_ <= 0.4;
   L.s_margin = s_margin_;
   L.cut2 = chord_ * chord_;
   L.chord = chord_;

@@ -10,8 +10,8 @@ qvm_device.cuh:  python zxtalori_b200/csrc/fit_atan.py
 import numpy as np
 
 
-def fit(degree=8, iterations=60):
-    s = np.cos(np.linspace(0, np.pi, 4000)) * 0.5 + 0.5
+def fit(degree=8, iterations=60, t_max=1.0):
+    s = (np.cos(np.linspace(0, np.pi, 4000)) * 0.5 + 0.5) * t_max * t_max
 
     def target(v):
         t = np.sqrt(v)
@@ -25,13 +25,16 @@ def fit(degree=8, iterations=60):
         c, *_ = np.linalg.lstsq(a, target(s) * scale, rcond=None)
         err = np.vander(s, degree + 1, increasing=True) @ c / target(s) - 1
         w = w * (1 + 4 * np.abs(err) / np.abs(err).max())
-    grid = np.linspace(0, 1, 2_000_001)
+    grid = np.linspace(0, t_max * t_max, 2_000_001)
     worst = np.abs(np.polyval(c[::-1], grid) / target(grid) - 1).max()
     return c, worst
 
 
 if __name__ == "__main__":
-    coeffs, worst = fit()
-    print(f"max relative error (exact coefficients): {worst:.3e}")
-    for k, v in enumerate(coeffs):
-        print(f"  c{k} = {float(np.float32(2 * v)).hex()}f  // 2 * {v:+.10e}")
+    # The full range (any cutoff) and the short range used when the near-field cutoff
+    # r <= 0.4 rad keeps t = tan(a/2) <= tan(0.2) < 0.21.
+    for degree, t_max in ((8, 1.0), (3, 0.21)):
+        coeffs, worst = fit(degree, t_max=t_max)
+        print(f"t in [0, {t_max}], degree {degree} in t^2: max relative error {worst:.3e}")
+        for k, v in enumerate(coeffs):
+            print(f"  c{k} = {float(np.float32(2 * v)).hex()}f  // 2 * {v:+.10e}")

@@ -8,8 +8,8 @@
 //      counted, scanned and written in (source, image) order - deterministic sites;
 //   2. the sites' stereographic chart box, a grid of sdim^3 cells, a counting sort of the
 //      sites into row-major cells with each cell ordered by site index;
-//   3. sources counting-sorted into a 64^3 Morton grid (then by index), so 32 consecutive
-//      sources are close together;
+//   3. sources counting-sorted along a Hilbert curve of a 64^3 grid (then by index), so 32
+//      consecutive sources are close together;
 //   4. one warp per 32 sources and slice: the warp's chart box, the cell rows within the
 //      chart reach of the cutoff chord, each row's x-run trimmed; runs stream through shared
 //      memory 32 sites at a time and every lane tests its source against each site;
@@ -148,7 +148,9 @@ __global__ void __launch_bounds__(256) k_shell_write(const float4* __restrict__ 
 
 // ------------------------------------------------------------------ 2. grid and site sort
 // Chart grid from the box (near.zig:124-137): a 5% margin, width 1.1x the largest extent,
-// sdim = clamp(round(cbrt(sites/8)), 1, sdim_max). The box is reset for the next pass.
+// sdim = clamp(round(cbrt(sites/kSitesPerCell)), 1, sdim_max). The reference aims at 8 sites
+// per cell; 3 trims the candidate runs closer to the cutoff ball (rows are cheap on B200).
+// The box is reset for the next pass.
 __global__ void k_grid_setup(NearGrid* g, const uint32_t* __restrict__ total, int capacity, int sdim_max,
                              int* __restrict__ cells) {
   const uint32_t s = *total;
@@ -164,12 +166,12 @@ __global__ void k_grid_setup(NearGrid* g, const uint32_t* __restrict__ total, in
   }
   for (int a = 0; a < 3; ++a) g->lower[a] = lo[a] - 0.05f * width;
   width *= 1.1f;
-  int sdim = (int)rint(cbrt((double)g->sites / 8.0));
+  int sdim = (int)rint(cbrt((double)g->sites / kSitesPerCell));
   sdim = max(1, min(sdim, sdim_max));
   g->width = width;
   g->sdim = sdim;
   g->cells_per_unit = (float)sdim / width;
-  g->morton_per_unit = (float)kMortonDim / width;
+  g->order_per_unit = (float)kOrderDim / width;
   *cells = sdim * sdim * sdim;
   for (int a = 0; a < 3; ++a) {
     g->box_bits[a] = 0xffffffffu;
@@ -237,14 +239,37 @@ __global__ void k_site_gather(const uint32_t* __restrict__ perm, const NearGrid*
   simg[p] = img[s];
 }
 
-// ------------------------------------------------------------------ 3. sources in Morton order
-// Bits of v moved three apart (a Morton code's interleave), for up to 10-bit coordinates.
-__device__ __forceinline__ uint32_t spread3(uint32_t v) {
-  uint32_t x = v & 0x3ffu;
-  x = (x | (x << 16)) & 0x030000ffu;
-  x = (x | (x << 8)) & 0x0300f00fu;
-  x = (x | (x << 4)) & 0x030c30c3u;
-  return (x | (x << 2)) & 0x09249249u;
+// ------------------------------------------------------------------ 3. sources in Hilbert order
+// Index of cell (x, y, z) along the Hilbert curve of a 2^bits grid: J. Skilling's transpose
+// algorithm ("Programming the Hilbert curve", AIP Conf. Proc. 707, 381, 2004), the three
+// transposed words then interleaved most significant bit first. Consecutive indices are
+// face-adjacent cells, so 32 consecutive sources (one warp) form a compact blob; a Morton
+// order (the reference's, near.wgsl:224-229) jumps at every power-of-two boundary.
+__device__ __forceinline__ uint32_t hilbert3(uint32_t x, uint32_t y, uint32_t z, int bits) {
+  uint32_t X[3] = {x, y, z};
+  const uint32_t m = 1u << (bits - 1);
+  for (uint32_t q = m; q > 1; q >>= 1) {
+    const uint32_t p = q - 1;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & q) {
+        X[0] ^= p;
+      } else {
+        const uint32_t t = (X[0] ^ X[i]) & p;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  X[1] ^= X[0];
+  X[2] ^= X[1];
+  uint32_t t = 0;
+  for (uint32_t q = m; q > 1; q >>= 1)
+    if (X[2] & q) t ^= q - 1;
+  uint32_t h = 0;
+  for (int b = bits - 1; b >= 0; --b)
+    h = (h << 3) | ((((X[0] ^ t) >> b) & 1u) << 2) | ((((X[1] ^ t) >> b) & 1u) << 1) | (((X[2] ^ t) >> b) & 1u);
+  return h;
 }
 
 template <bool FP64>
@@ -254,10 +279,10 @@ __global__ void k_source_count(const float4* __restrict__ q32, const double4* __
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float3 p = FP64 ? chart(q64[i]) : chart(q32[i]);
-  const float u = gp->morton_per_unit;
-  const uint32_t cx = cell_axis(p.x, gp->lower[0], u, kMortonDim), cy = cell_axis(p.y, gp->lower[1], u, kMortonDim),
-                 cz = cell_axis(p.z, gp->lower[2], u, kMortonDim);
-  const uint32_t m = spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2);
+  const float u = gp->order_per_unit;
+  const uint32_t cx = cell_axis(p.x, gp->lower[0], u, kOrderDim), cy = cell_axis(p.y, gp->lower[1], u, kOrderDim),
+                 cz = cell_axis(p.z, gp->lower[2], u, kOrderDim);
+  const uint32_t m = hilbert3(cx, cy, cz, kOrderBits);
   code[i] = m;
   rank[i] = atomicAdd(&counts[m], 1u);
 }
@@ -339,8 +364,8 @@ __device__ __forceinline__ bool row_run(const WarpBox& b, const NearGrid& g, con
 // windowed pair runs with dp2 = 2(|x|^2+|y|^2) - dm2 (parallelogram law; the site is the
 // near twin), and the force is kept as sum c (x - y), turned into a force once per source.
 // Tile sums are FP32 (FP64 in FP64 mode), merged into FP64 per tile.
-template <bool TRACK>
-__global__ void __launch_bounds__(kNearWarps * 32) k_near32(const float4* __restrict__ q, int n,
+template <bool TRACK, bool SHORT>
+__global__ void __launch_bounds__(kNearWarps * 32, 8) k_near32(const float4* __restrict__ q, int n,
                                                               const uint32_t* __restrict__ src_perm,
                                                               const float4* __restrict__ sq,
                                                               const uint32_t* __restrict__ scode,
@@ -405,7 +430,7 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near32(const float4* __rest
           best = fminf(best, dm2);
         }
         float c, cv, e;
-        near_pair32(dm2, nx2 + m.x - dm2, cz, cw, c, cv, e);
+        near_pair32<SHORT>(dm2, nx2 + m.x - dm2, cz, cw, c, cv, e);
         sw = fmaf(c, mw, sw);
         sx = fmaf(c, mx, sx);
         sy = fmaf(c, my, sy);
@@ -548,8 +573,8 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   else
     k_site_gather<false><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_code,
                                                                    L.site_img, L.sq32, L.sq64, L.scode, L.simg);
-  // 3. sources in Morton order
-  const int mcells = kMortonDim * kMortonDim * kMortonDim;
+  // 3. sources in Hilbert order
+  const int mcells = kOrderDim * kOrderDim * kOrderDim;
   cudaMemsetAsync(L.mcount, 0, sizeof(uint32_t) * (mcells + 1), s);
   if (fp64)
     k_source_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.grid, L.src_key, L.src_rank, L.mcount);
@@ -568,8 +593,10 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
     if (L.track) k_near64<true><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
     else k_near64<false><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
   } else {
-    if (L.track) k_near32<true><<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
-    else k_near32<false><<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
+    auto kernel = L.track ? (L.short_atan ? k_near32<true, true> : k_near32<true, false>)
+                          : (L.short_atan ? k_near32<false, true> : k_near32<false, false>);
+    kernel<<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, L.slices,
+                                            dst, n);
   }
   probe_mark(s);
   k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(L.partial, n, L.slices, n, (const int*)L.src_perm, L.out, L.track ? 1 : 0);

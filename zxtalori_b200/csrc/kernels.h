@@ -45,6 +45,7 @@ cudaError_t launch_full(int prec, const float4* q32, const double4* q64, int n, 
 struct NearLaunch {
   int prec, gid, n, capacity, sdim_max, slices;
   bool track;
+  bool short_atan;  // cutoff r <= 0.4 rad: the short-range arctangent applies
   double s_margin, cut2, chord, cut_z, cut_w;
   const float4* q32;
   const double4* q64;

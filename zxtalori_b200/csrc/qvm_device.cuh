@@ -82,6 +82,16 @@ __device__ __forceinline__ float two_atan_unit(float t, float t2) {
   return t * p;
 }
 
+// 2 atan(t) for t in [0, 0.21] (near-field cutoffs r <= 0.4 rad, t = tan(a/2) <= tan 0.2):
+// degree-3 minimax fit in t^2 from fit_atan.py, max relative error 3.0e-9.
+__device__ __forceinline__ float two_atan_short(float t, float t2) {
+  float p = -0x1.117a86p-2f;
+  p = fmaf(p, t2, 0x1.991528p-2f);
+  p = fmaf(p, t2, -0x1.5554c2p-1f);
+  p = fmaf(p, t2, 2.0f);
+  return t * p;
+}
+
 // Vector part of y * conj(x): the left-tangent direction of a pair (shaders/pairs.wgsl:258).
 template <class T, class V>
 __device__ __forceinline__ void pair_direction(const V& x, const V& y, T& d1, T& d2, T& d3) {
@@ -128,12 +138,13 @@ __device__ __forceinline__ PairF quey_pair32(float dm2, float dp2) {
 // Windowed near-field pair, FP32, for a site that is the near twin (dm2 <= cut < 2 <= dp2,
 // so the sign is +1, near = dm2 and far = dp2): the coefficient c of the pair's direction
 // (force contribution c * dir), its windowed curvature and energy. Same arithmetic as
-// quey_pair32 followed by window32.
+// quey_pair32 followed by window32. SHORT: the cutoff is at most 0.4 rad (two_atan_short).
+template <bool SHORT>
 __device__ __forceinline__ void near_pair32(float dm2, float dp2, float cut_z, float cut_w, float& coef, float& curv,
                                             float& energy) {
   const float t2 = fmaxf(dm2, 1e-30f) * rcp_approx(dp2);
   const float t = sqrt_approx(t2);
-  const float a = fmaxf(two_atan_unit(t, t2), 1e-12f);
+  const float a = fmaxf(SHORT ? two_atan_short(t, t2) : two_atan_unit(t, t2), 1e-12f);
   const float b = kPiF - a;
   const float aa = a * a, bb = b * b;
   const float a2 = aa + 1e-9f, b2 = bb + 1e-9f;

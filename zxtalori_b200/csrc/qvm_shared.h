@@ -8,9 +8,12 @@ constexpr int kMaxOperatorRows = 141;   // sum of |K| over the eleven groups
 constexpr int kMaxPlaneRows = 271;      // sum of 2|K|-1 zone bisector planes
 constexpr uint32_t kIdentityBit = 0x80000000u;  // site code: the source's identity image
 constexpr int kMaxCellDim = 128;        // chart grid side (src/near.zig:135)
-// Sources' Morton grid side. The reference uses 32 (src/near.zig:23); 64 keeps 32
-// consecutive sources (one warp) about half as wide at N = 100k, so fewer candidate sites.
-constexpr int kMortonDim = 64;
+// Sources are ordered along a Hilbert curve over a 64^3 grid of the chart box (the
+// reference sorts them into a 32^3 Morton grid, src/near.zig:23).
+constexpr int kOrderBits = 6;
+constexpr int kOrderDim = 1 << kOrderBits;
+// Target sites per cell of the chart grid (the reference uses 8, src/near.zig:135).
+constexpr double kSitesPerCell = 3.0;
 
 // Precision of one sample's arithmetic.
 //  kFP32: FP32 pair arithmetic (approximate SFU reciprocals, own atan), FP64 row sums,
@@ -30,7 +33,7 @@ struct Rows {
 struct NearGrid {
   float lower[3];
   float cells_per_unit;     // sdim / width
-  float morton_per_unit;    // 32 / width
+  float order_per_unit;     // kOrderDim / width
   float width;
   int sdim;
   int sites;                // shell sites written (clamped to capacity)
