@@ -113,6 +113,19 @@ int zo_debug_rows(void* h, uint32_t what, double* out);
  * out[0] total step ms, out[1] ms of the force pass's row kernel, out[2] its launches,
  * out[3] kernel launches per step, out[4 ..] per-step ms while out_len allows. */
 int zo_bench(void* h, uint32_t steps, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len);
+/* Extensions (no reference counterpart): relaxation in two halves, so many engines relax
+ * concurrently. zo_relax_async enqueues `steps` BB steps on the engine's stream and returns
+ * at once (in FP32 mode each step replays a CUDA graph captured from the first one);
+ * zo_relax_finish waits, runs the closing force pass and reads back positions and measures
+ * exactly as zo_relax does at its end. zo_idle: 1 when no work is pending, 0 while busy,
+ * -1 on error. zo_graphs(h, 0) turns graph replay off (direct kernel launches). */
+int zo_relax_async(void* h, uint32_t steps);
+int zo_relax_finish(void* h);
+int zo_idle(void* h);
+int zo_graphs(void* h, uint32_t enabled);
+/* Extension: relax `count` engines by `steps` each, side by side on their own streams, then
+ * finish each; status[k] is 0 or -1 (message in zo_error(handles[k])). Returns failures. */
+int zo_batch_relax(void* const* handles, uint32_t count, uint32_t steps, int32_t* status);
 /* Measurement hook (no reference counterpart): FP32 FMA throughput of the engine's device
  * in TFLOP/s (2 flops per FMA), the denominator of the pair kernels' roofline; -1 on error. */
 double zo_fp32_peak(void* h);

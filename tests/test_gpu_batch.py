@@ -1,0 +1,80 @@
+"""Batched and served relaxation: every sample's result is the same alone and in the mix.
+
+Each sample's kernels read only its own buffers and sum in a fixed order, and a captured
+step graph replays exactly the launches it captured, so the comparisons are exact
+(tolerance 0); the energies are also checked against the oracle's measure of the result.
+"""
+import numpy as np
+import pytest
+
+from oracle import qvm
+
+pytestmark = pytest.mark.gpu
+
+SAMPLES = [("O", 3000, 1, 20.0), ("I", 1500, 2, 20.0), ("C4", 900, 3, 0.0), ("D6", 6000, 4, 20.0), ("T", 700, 5, 0.0)]
+
+
+def test_graph_replay_equals_direct_launches(engine):
+    out = []
+    for graphs in (1, 0):
+        with engine.haar("O", 4000, 8) as grid:
+            grid._check(grid._lib.zo_graphs(grid._handle, graphs))
+            grid.relax(12, neighbourhood=20)
+            out.append((grid.quaternions, grid.stats))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1]["energy"] == out[1][1]["energy"]
+
+
+def test_batch_matches_alone(engine, ops32):
+    from zxtalori_b200 import batch
+
+    specs = [batch.Sample(g, n, s, d) for g, n, s, d in SAMPLES]
+    grids = batch.make_grids(specs)
+    try:
+        stats = batch.relax_batch(grids, 10)
+        mixed = [g.quaternions for g in grids]
+    finally:
+        for g in grids:
+            g.close()
+    for spec, q_mix, s_mix in zip(specs, mixed, stats):
+        with engine.haar(spec.group, spec.count, spec.seed) as grid:
+            grid.relax(10, neighbourhood=spec.neighbourhood)
+            assert np.array_equal(grid.quaternions, q_mix), spec
+            assert grid.stats["energy"] == s_mix["energy"]
+        assert s_mix["iteration"] == 10
+
+
+def test_server_results_same_alone_and_in_mix(engine):
+    from zxtalori_b200 import serve
+
+    requests = [serve.Request(k, g, n, 8 + 3 * k, 100 + k, d, arrival=0.01 * k) for k, (g, n, _, d) in enumerate(SAMPLES)]
+    mixed = serve.Server(keep_quaternions=True, chunk_seconds=0.001).run(requests)
+    assert sorted(r.id for r in mixed) == list(range(len(requests)))
+    by_id = {r.id: r for r in mixed}
+    for req in requests:
+        alone = serve.Server(keep_quaternions=True).run([serve.Request(req.id, req.group, req.count, req.steps, req.seed,
+                                                                       req.neighbourhood, 0.0)])[0]
+        assert np.array_equal(alone.quaternions, by_id[req.id].quaternions), req
+        assert alone.stats["energy"] == by_id[req.id].stats["energy"]
+        assert by_id[req.id].stats["iteration"] == req.steps
+    info = serve.summary(mixed)
+    assert info["requests"] == len(requests) and info["latency_p99_s"] >= info["latency_p50_s"] > 0
+
+
+def test_served_energy_matches_oracle(engine, ops32):
+    from zxtalori_b200 import serve
+
+    req = serve.Request(0, "C4", 900, 6, 77, 0.0)
+    res = serve.Server(keep_quaternions=True).run([req])[0]
+    q = res.quaternions.astype(np.float64)
+    expected = qvm.quick_measures(qvm.pair_rows(q, ops32["C4"]), 4)
+    assert res.stats["energy"] == pytest.approx(expected["quey_energy"], rel=1e-6)
+
+
+def test_plain_one_at_a_time(engine):
+    from zxtalori_b200 import serve
+
+    reqs = [serve.Request(0, "O", 1048, 5, 193, 0.0), serve.Request(1, "D3", 800, 4, 5, 0.0, 0.001)]
+    res = serve.serve_one_at_a_time(reqs)
+    assert [r.id for r in res] == [0, 1]
+    assert all(r.stats["arithmetic"] == "fp64" for r in res)

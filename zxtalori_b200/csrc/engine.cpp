@@ -79,6 +79,7 @@ Rows RowBuffers::ensure(size_t n) {
 // ------------------------------------------------------------------ near field
 void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_r, int sms) {
   ready_ = false;
+  ++generation_;
   n_ = n;
   prec_ = prec;
   radius_ = std::min(1.5, delta_ * mean_r);
@@ -197,6 +198,7 @@ bool NearField::overflowed(cudaStream_t s) {
 
 // ------------------------------------------------------------------ relaxation state
 void RelaxState::reset() {
+  ++generation_;
   n_ = 0;
   prec_ = -1;
   current = false;
@@ -209,15 +211,18 @@ void RelaxState::set_near(int gid, std::optional<double> delta) {
     if (delta && near_->gid() == gid && near_->delta() == *delta) return;
     near_.reset();
     current = false;
+    ++generation_;
   }
   if (delta) {
     near_ = std::make_unique<NearField>(gid, *delta);
     current = false;
+    ++generation_;
   }
 }
 
 void RelaxState::prepare(int n, int prec) {
   if (n_ == n && prec_ == prec) return;
+  ++generation_;
   n_ = n;
   prec_ = prec;
   current = false;
@@ -337,7 +342,102 @@ Engine::Engine() {
 Engine::~Engine() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);
+  drop_graph();
   if (stream_) cudaStreamDestroy(stream_);
+}
+
+// ------------------------------------------------------------------ graph-captured steps
+uint64_t Engine::graph_key() const {
+  uint64_t k = relax_state_.generation();
+  k = k * 1000033ull + config_gen_;
+  k = k * 1000037ull + (uint64_t)(fixed_arg() + 1);
+  k = k * 1000039ull + n_;
+  return k;
+}
+
+void Engine::drop_graph() {
+  if (step_graph_) cudaGraphExecDestroy(step_graph_);
+  step_graph_ = nullptr;
+}
+
+// Captures one BB step (force pass, statistics, median, move and fold) of the current
+// sample. Every kernel reads its parameters from the sample's buffers, so the graph replays
+// step after step until the buffers or settings change (graph_key).
+void Engine::capture_step_graph() {
+  drop_graph();
+  cudaGraph_t graph = nullptr;
+  ZO_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  try {
+    relax_state_.current = false;
+    relax_state_.step(stream_, prec_, q32(), q64(), (int)n_, group_, fixed_arg(), budget_scale_, sms_);
+  } catch (...) {
+    cudaStreamEndCapture(stream_, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  ZO_CUDA(cudaStreamEndCapture(stream_, &graph));
+  const cudaError_t e = cudaGraphInstantiate(&step_graph_, graph, 0);
+  cudaGraphDestroy(graph);
+  ZO_CUDA(e);
+  graph_key_ = graph_key();
+}
+
+// One BB step: the captured graph when it is current, else direct launches (which also
+// size the workspace) followed by a capture for the next steps. FP64 mode, the plain
+// method, always launches kernel by kernel.
+void Engine::step_once() {
+  if (fix_identity_ && !fixed_index_) throw Failure("IdentityMissingEnableAddIdentity");
+  const bool graphable = use_graphs_ && prec_ == kFP32;
+  if (graphable && step_graph_ && !relax_state_.current && graph_key_ == graph_key() &&
+      relax_state_.sized((int)n_, prec_)) {
+    ZO_CUDA(cudaGraphLaunch(step_graph_, stream_));
+  } else {
+    relax_state_.step(stream_, prec_, q32(), q64(), (int)n_, group_, fixed_arg(), budget_scale_, sms_);
+    if (graphable && relax_state_.sized((int)n_, prec_) && (!step_graph_ || graph_key_ != graph_key()))
+      capture_step_graph();
+  }
+  ++iteration_;
+}
+
+void Engine::relax_async(uint32_t steps) {
+  if (n_ < 2) throw Failure("TooFewOrientations");
+  ZO_CUDA(cudaSetDevice(device_));
+  if (!relaxing_) {
+    cancelled_.store(false);
+    sync_neighbourhood();
+    relaxing_ = true;
+  }
+  for (uint32_t k = 0; k < steps; ++k) {
+    step_once();
+    recorded_ = true;
+  }
+}
+
+void Engine::relax_finish() {
+  ZO_CUDA(cudaSetDevice(device_));
+  if (!relaxing_) sync_neighbourhood();
+  relaxing_ = false;
+  measures_.reset();
+  std::optional<StepResult> last;
+  const bool recorded = recorded_;
+  recorded_ = false;
+  if (recorded) last = relax_state_.finish(stream_);
+  Measures m = relax_state_measure();
+  fetch();
+  if (last) {
+    step_deg_ = last->max_step_deg;
+    force_rms_ = last->force_rms;
+  }
+  measures_ = m;
+  full_measures_ = false;
+  measure_iteration_ = iteration_;
+}
+
+bool Engine::idle() {
+  const cudaError_t e = cudaStreamQuery(stream_);
+  if (e == cudaErrorNotReady) return false;
+  ZO_CUDA(e);
+  return true;
 }
 
 uint32_t Engine::ratio_limit() const {
@@ -594,11 +694,11 @@ void Engine::relax(uint32_t steps) {
   const uint64_t sync_every = (uint64_t)std::max(1.0, std::floor(2e10 / (n * neighbours)));
   const uint32_t run = std::min<uint32_t>(steps, 1000);
   bool recorded = false;
+  relaxing_ = false;
+  recorded_ = false;
   for (uint32_t index = 0; index < run; ++index) {
     if (cancelled_.load()) break;
-    if (fix_identity_ && !fixed_index_) throw Failure("IdentityMissingEnableAddIdentity");
-    relax_state_.step(stream_, prec_, q32(), q64(), (int)n_, group_, fixed_arg(), budget_scale_, sms_);
-    ++iteration_;
+    step_once();
     recorded = true;
     if ((index + 1) % sync_every == 0 && index + 1 < run) {
       const StepResult r = relax_state_.finish(stream_);
@@ -718,14 +818,25 @@ void Engine::bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* 
   ZO_CUDA(cudaSetDevice(device_));
   sync_neighbourhood();
   relax_state_.prepare((int)n_, prec_);
-  for (uint32_t w = 0; w < warmup; ++w)
-    relax_state_.step(stream_, prec_, q32(), q64(), (int)n_, group_, fixed_arg(), budget_scale_, sms_);
+  relax_state_.current = false;
+  for (uint32_t w = 0; w < std::max<uint32_t>(warmup, 1); ++w) step_once();
   ZO_CUDA(cudaStreamSynchronize(stream_));
   DeviceBuffer flush;
   const size_t fbytes = flush_bytes > 0 ? (size_t)flush_bytes : 0;
   if (fbytes) flush.ensure(fbytes);
   std::vector<cudaEvent_t> ev(4 * (size_t)steps);
   for (auto& e : ev) ZO_CUDA(cudaEventCreate(&e));
+  // The timed steps take the product path: graph replays in FP32 mode, kernel by kernel in
+  // FP64 mode.
+  for (uint32_t k = 0; k < steps; ++k) {
+    if (fbytes) ZO_CUDA(cudaMemsetAsync(flush.as<void>(), (int)(k & 0xff), fbytes, stream_));
+    ZO_CUDA(cudaEventRecord(ev[2 * k], stream_));
+    step_once();
+    ZO_CUDA(cudaEventRecord(ev[2 * k + 1], stream_));
+  }
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  // The dominant kernel's own time and the launch count come from the same number of
+  // direct steps, each kernel bracketed by events.
   LaunchProbe probe;
   probe.events = ev.data() + 2 * (size_t)steps;
   probe.capacity = 2 * (int)steps;
@@ -733,9 +844,7 @@ void Engine::bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* 
   try {
     for (uint32_t k = 0; k < steps; ++k) {
       if (fbytes) ZO_CUDA(cudaMemsetAsync(flush.as<void>(), (int)(k & 0xff), fbytes, stream_));
-      ZO_CUDA(cudaEventRecord(ev[2 * k], stream_));
       relax_state_.step(stream_, prec_, q32(), q64(), (int)n_, group_, fixed_arg(), budget_scale_, sms_);
-      ZO_CUDA(cudaEventRecord(ev[2 * k + 1], stream_));
     }
   } catch (...) {
     t_probe = nullptr;
@@ -760,7 +869,7 @@ void Engine::bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* 
   out[1] = kernel;
   out[2] = probe.used / 2;
   out[3] = (double)probe.launches / steps;
-  iteration_ += warmup + steps;
+  iteration_ += steps;  // the direct steps (step_once counts its own)
   relax_state_.current = false;
   measures_.reset();
   fetch();

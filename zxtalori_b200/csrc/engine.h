@@ -80,8 +80,12 @@ class NearField {
   const uint32_t* sorted_images() const { return simg_.as<uint32_t>(); }
   int capacity() const { return capacity_; }
   int slices() const { return slices_; }
+  // Changes whenever the workspace is sized again (buffers move): captured graphs go stale.
+  uint64_t generation() const { return generation_; }
+  bool ready() const { return ready_; }
 
  private:
+  uint64_t generation_ = 0;
   void setup(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_radius, int sms);
   int gid_;
   double delta_;
@@ -118,8 +122,13 @@ class RelaxState {
                      int gid);
   bool near_overflowed(cudaStream_t s) { return near_ && near_->overflowed(s); }
   NearField* near_field() { return near_.get(); }
+  // Identifies the buffers and settings a captured step reads; any change makes it stale.
+  uint64_t generation() const { return generation_ * 1000003ull + (near_ ? near_->generation() * 7 + 1 : 0); }
+  // Whether a step would run without sizing anything (so it can be captured in a graph).
+  bool sized(int n, int prec) const { return n_ == n && prec_ == prec && (!near_ || near_->ready()); }
 
  private:
+  uint64_t generation_ = 0;
   StepResult step_result(const RelaxDev& st) const;
   int n_ = 0, prec_ = -1, order_ = 0;
   RowBuffers rows_, partial_;
@@ -148,7 +157,21 @@ class Engine {
   // Extensions.
   void set_precision(int prec);
   int precision() const { return prec_; }
-  void set_pair_budget(double scale) { budget_scale_ = scale; }
+  void set_pair_budget(double scale) {
+    budget_scale_ = scale;
+    ++config_gen_;
+  }
+  // Relaxation split in two: enqueue `steps` BB steps on the engine's stream and return
+  // (FP32 mode replays a CUDA graph of one step), then finish with the closing force pass
+  // and readback of relax(). Several engines relax concurrently this way.
+  void relax_async(uint32_t steps);
+  void relax_finish();
+  // Whether the engine's stream has no work pending.
+  bool idle();
+  void set_graphs(bool enabled) {
+    use_graphs_ = enabled;
+    drop_graph();
+  }
   // Development: one pass's raw rows to host. what 0: force pass of the relaxation
   // (8 doubles per source), 1: full measure rows (12 doubles per source).
   void debug_rows(uint32_t what, double* out);
@@ -173,6 +196,15 @@ class Engine {
   char err[2048] = {0};
 
  private:
+  void step_once();
+  void capture_step_graph();
+  void drop_graph();
+  uint64_t graph_key() const;
+  cudaGraphExec_t step_graph_ = nullptr;
+  uint64_t graph_key_ = 0;
+  uint64_t config_gen_ = 0;
+  bool use_graphs_ = true;
+  bool relaxing_ = false, recorded_ = false;
   void adopt(uint32_t n);
   void reset_run();
   void sync_neighbourhood();

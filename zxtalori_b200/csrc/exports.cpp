@@ -156,6 +156,36 @@ int zo_bench(void* h, uint32_t steps, uint32_t warmup, double flush_bytes, doubl
   return guarded(h, "Bench", [&](Engine& e) { e.bench(steps, warmup, flush_bytes, out, out_len); });
 }
 
+int zo_relax_async(void* h, uint32_t steps) {
+  return guarded(h, "Relaxation failed", [&](Engine& e) { e.relax_async(steps); });
+}
+
+int zo_relax_finish(void* h) { return guarded(h, "Relaxation failed", [](Engine& e) { e.relax_finish(); }); }
+
+int zo_idle(void* h) {
+  int idle = 0;
+  if (guarded(h, "Relaxation failed", [&](Engine& e) { idle = e.idle() ? 1 : 0; }) != 0) return -1;
+  return idle;
+}
+
+int zo_graphs(void* h, uint32_t enabled) {
+  return guarded(h, "Graphs", [&](Engine& e) { e.set_graphs(enabled != 0); });
+}
+
+int zo_batch_relax(void* const* handles, uint32_t count, uint32_t steps, int32_t* status) {
+  int failures = 0;
+  // Enqueue every sample's steps first (each engine has its own stream, so the samples'
+  // kernels run side by side), then close each one with its force pass and readback.
+  for (uint32_t k = 0; k < count; ++k) {
+    status[k] = guarded(handles[k], "Relaxation failed", [&](Engine& e) { e.relax_async(steps); });
+  }
+  for (uint32_t k = 0; k < count; ++k) {
+    if (status[k] == 0) status[k] = zo_relax_finish(handles[k]);
+    failures += status[k] != 0;
+  }
+  return failures;
+}
+
 double zo_fp32_peak(void* h) {
   double value = -1.0;
   if (guarded(h, "Probe", [&](Engine& e) { value = e.fp32_peak(); }) != 0) return -1.0;
