@@ -16,6 +16,7 @@ constexpr uint32_t kMaxCount = 10000000;          // hopf.max_count (src/hopf.zi
 constexpr double kFullMeasurePairs = 5e10;        // src/engine.zig:1123
 constexpr uint32_t kSpacingAllPairs = 20000;      // src/engine.zig:1126
 constexpr double kSpacingDelta = 4;               // src/engine.zig:1127
+constexpr double kDenseRadius = 0.5;              // cutoffs from here on use the dense near field
 constexpr const char* kVersion = "0.3.0";
 
 std::mutex g_tables_mutex;
@@ -85,6 +86,15 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   radius_ = std::min(1.5, delta_ * mean_r);
   s_margin_ = std::sin(radius_ + 1e-4);
   chord_ = 2.0 * std::sin(radius_ / 2.0);
+  // Wide cutoffs: every image is tested (the shell holds most images anyway, and images
+  // near the chart's far pole spread the chart box until the grid degenerates).
+  dense_ = radius_ >= kDenseRadius;
+  if (dense_) {
+    plan_ = plan_pairs(n, host_group_order(gid_), 1.0, sms);
+    if (plan_.chunks > 1) partial_.ensure((size_t)plan_.chunks * n);
+    ready_ = true;
+    return;
+  }
   counts_.ensure((size_t)(n + 1) * 4);
   offsets_.ensure((size_t)(n + 1) * 4);
   scan_tmp_.ensure(4096 * 4);
@@ -141,6 +151,12 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
 void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_r, bool track,
                      Rows out, int sms) {
   if (!ready_ || n != n_ || prec != prec_) setup(s, prec, q32, q64, n, mean_r, sms);
+  if (dense_) {
+    ZO_CUDA(launch_dense_near(prec, track, radius_ <= 0.4, q32, q64, n, gid_, plan_, chord_ * chord_, chord_,
+                              taper_ * radius_, 1.0 / std::max(1e-9, (1.0 - taper_) * radius_),
+                              plan_.chunks > 1 ? partial_.rows() : Rows{}, out, s));
+    return;
+  }
   NearLaunch L{};
   L.prec = prec;
   L.gid = gid_;
@@ -187,7 +203,7 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
 }
 
 bool NearField::overflowed(cudaStream_t s) {
-  if (!ready_) return false;
+  if (!ready_ || dense_) return false;
   unsigned int flag = 0;
   ZO_CUDA(cudaMemcpyAsync(&flag, &grid_.as<NearGrid>()->overflow, 4, cudaMemcpyDeviceToHost, s));
   ZO_CUDA(cudaStreamSynchronize(s));
@@ -298,7 +314,7 @@ StepResult RelaxState::finish(cudaStream_t s) {
 Measures RelaxState::summarize(cudaStream_t s, int n, int order, float* degrees, int* neighbours, int prec,
                                const float4* q32, int gid) {
   const Rows r = rows_.rows();
-  const bool near_sites = near_ != nullptr;
+  const bool near_sites = near_ != nullptr && !near_->dense();
   const uint32_t* scode = near_sites ? near_->sorted_codes() : nullptr;
   const uint32_t* simg = near_sites ? near_->sorted_images() : nullptr;
   if (prec == kFP32) ZO_CUDA(launch_refine_nearest(q32, n, gid, r, near_sites, scode, simg, neighbours_.as<int>(), s));

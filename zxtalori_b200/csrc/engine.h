@@ -83,9 +83,13 @@ class NearField {
   // Changes whenever the workspace is sized again (buffers move): captured graphs go stale.
   uint64_t generation() const { return generation_; }
   bool ready() const { return ready_; }
+  // Summed over every image instead of the shell and chart grid (wide cutoffs).
+  bool dense() const { return dense_; }
 
  private:
   uint64_t generation_ = 0;
+  bool dense_ = false;
+  PairsPlan plan_;
   void setup(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_radius, int sms);
   int gid_;
   double delta_;

@@ -534,6 +534,171 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near64(const double4* __res
   if (TRACK) out.nearest_at[at] = best_at;
 }
 
+// ------------------------------------------------------------------ dense near field
+// Wide cutoffs (r >= 0.5 rad: few images, or low-order groups at small N, where the chart
+// grid degenerates because images near the far pole spread the chart box) are summed over
+// every image like all pairs, with the same near-field semantics: the near twin of each
+// image (y or -y) counts when its chord is within the cutoff, the windowed pair applies, the
+// own orbit is excluded from forces and its non-identity images bound the nearest.
+template <bool TRACK, bool CHECK, bool SHORT>
+__device__ __forceinline__ void dense32_tile(const float4 x, const float4* tile, int count, int i, int j0, int k, int n,
+                                             float cut2, float cz, float cw, float& sw, float& sx, float& sy, float& sz,
+                                             float& sc, float& se, float& best, int& best_at) {
+  for (int t = 0; t < count; ++t) {
+    const float4 y = tile[t];
+    const float mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
+    const float pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
+    const float dm2 = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
+    const float dp2 = fmaf(pw, pw, fmaf(px, px, fmaf(py, py, pz * pz)));
+    const bool minus = dm2 <= dp2;
+    const float nearv = minus ? dm2 : dp2;
+    if (nearv > cut2) continue;
+    if (CHECK && j0 + t == i) {
+      if (k != 0 && nearv < best) {
+        best = nearv;
+        if (TRACK) best_at = k * n + j0 + t;
+      }
+      continue;
+    }
+    if (nearv < best) {
+      best = nearv;
+      if (TRACK) best_at = k * n + j0 + t;
+    }
+    float c, cv, e;
+    near_pair32<SHORT>(nearv, minus ? dp2 : dm2, cz, cw, c, cv, e);
+    sw = fmaf(c, minus ? mw : pw, sw);
+    sx = fmaf(c, minus ? mx : px, sx);
+    sy = fmaf(c, minus ? my : py, sy);
+    sz = fmaf(c, minus ? mz : pz, sz);
+    sc += cv;
+    se += e;
+  }
+}
+
+template <bool TRACK, bool SHORT>
+__global__ void __launch_bounds__(kPairBlock) k_dense32(const float4* __restrict__ q, int n, int op_off, int jtiles,
+                                                        int total_tiles, int tiles_per_chunk, NearCut cut, Rows out,
+                                                        int stride) {
+  __shared__ float4 tile[kPairBlock];
+  const int i0 = blockIdx.x * kPairBlock;
+  const int i = i0 + threadIdx.x;
+  const bool live = i < n;
+  const float4 x = live ? q[i] : make_float4(1.f, 0.f, 0.f, 0.f);
+  const float cut2 = (float)cut.cut2, cz = (float)cut.cut_z, cw = (float)cut.cut_w;
+  double yw = 0, yx = 0, yy = 0, yz = 0, fc = 0, fe = 0;
+  float best = 4.0f;
+  int best_at = -1;
+  const int t0 = blockIdx.y * tiles_per_chunk, t1 = min(total_tiles, t0 + tiles_per_chunk);
+  for (int tid = t0; tid < t1; ++tid) {
+    const PairTile pt = pair_tile(tid, jtiles, n);
+    __syncthreads();
+    if ((int)threadIdx.x < pt.count) tile[threadIdx.x] = image32(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0);
+    __syncthreads();
+    if (!live) continue;
+    float sw = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, sc = 0.f, se = 0.f;
+    if (pt.j0 < i0 + kPairBlock && i0 < pt.j0 + pt.count)
+      dense32_tile<TRACK, true, SHORT>(x, tile, pt.count, i, pt.j0, pt.k, n, cut2, cz, cw, sw, sx, sy, sz, sc, se, best,
+                                       best_at);
+    else
+      dense32_tile<TRACK, false, SHORT>(x, tile, pt.count, i, pt.j0, pt.k, n, cut2, cz, cw, sw, sx, sy, sz, sc, se,
+                                        best, best_at);
+    yw += sw;
+    yx += sx;
+    yy += sy;
+    yz += sz;
+    fc += sc;
+    fe += se;
+  }
+  if (!live) return;
+  const size_t at = (size_t)blockIdx.y * stride + i;
+  const double3 f = force_from_differences(to_d4(x), make_double4(yw, yx, yy, yz));
+  out.force[at] = make_double4(f.x, f.y, f.z, fc);
+  out.energy[at] = fe;
+  out.nearest[at] = best;
+  if (TRACK) out.nearest_at[at] = best_at;
+}
+
+template <bool TRACK>
+__global__ void __launch_bounds__(kPairBlock) k_dense64(const double4* __restrict__ q, int n, int op_off, int jtiles,
+                                                        int total_tiles, int tiles_per_chunk, NearCut cut, Rows out,
+                                                        int stride) {
+  __shared__ double4 tile[kPairBlock];
+  const int i0 = blockIdx.x * kPairBlock;
+  const int i = i0 + threadIdx.x;
+  const bool live = i < n;
+  const double4 x = live ? q[i] : make_double4(1, 0, 0, 0);
+  double yw = 0, yx = 0, yy = 0, yz = 0, fc = 0, fe = 0, best = 4.0;
+  int best_at = -1;
+  const int t0 = blockIdx.y * tiles_per_chunk, t1 = min(total_tiles, t0 + tiles_per_chunk);
+  for (int tid = t0; tid < t1; ++tid) {
+    const PairTile pt = pair_tile(tid, jtiles, n);
+    __syncthreads();
+    if ((int)threadIdx.x < pt.count) tile[threadIdx.x] = image64(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0);
+    __syncthreads();
+    if (!live) continue;
+    for (int t = 0; t < pt.count; ++t) {
+      const double4 y = tile[t];
+      const double mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
+      const double pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
+      const double dm2 = mw * mw + mx * mx + my * my + mz * mz;
+      const double dp2 = pw * pw + px * px + py * py + pz * pz;
+      const bool minus = dm2 <= dp2;
+      const double nearv = minus ? dm2 : dp2;
+      if (nearv > cut.cut2) continue;
+      if (pt.j0 + t == i) {
+        if (pt.k != 0 && nearv < best) {
+          best = nearv;
+          if (TRACK) best_at = pt.k * n + pt.j0 + t;
+        }
+        continue;
+      }
+      if (nearv < best) {
+        best = nearv;
+        if (TRACK) best_at = pt.k * n + pt.j0 + t;
+      }
+      PairD pr = quey_pair64(nearv, minus ? dp2 : dm2);
+      window64(pr, nearv, minus ? dp2 : dm2, cut.cut_z, cut.cut_w);
+      const double c = pr.coef;
+      yw += c * (minus ? mw : pw);
+      yx += c * (minus ? mx : px);
+      yy += c * (minus ? my : py);
+      yz += c * (minus ? mz : pz);
+      fc += pr.curv;
+      fe += pr.energy;
+    }
+  }
+  if (!live) return;
+  const size_t at = (size_t)blockIdx.y * stride + i;
+  const double3 f = force_from_differences(x, make_double4(yw, yx, yy, yz));
+  out.force[at] = make_double4(f.x, f.y, f.z, fc);
+  out.energy[at] = fe;
+  out.nearest[at] = best;
+  if (TRACK) out.nearest_at[at] = best_at;
+}
+
+cudaError_t launch_dense_near(int prec, bool track, bool short_atan, const float4* q32, const double4* q64, int n,
+                              int gid, const PairsPlan& pl, double cut2, double chord, double cut_z, double cut_w,
+                              Rows partial, Rows out, cudaStream_t s) {
+  const int op_off = host_group_offset(gid);
+  const dim3 grid(pl.jtiles, pl.chunks);
+  const bool direct = pl.chunks == 1;
+  const Rows dst = direct ? out : partial;
+  const NearCut cut{cut2, chord, cut_z, cut_w};
+  probe_mark(s);
+  if (prec == kFP64) {
+    if (track) k_dense64<true><<<grid, kPairBlock, 0, s>>>(q64, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, cut, dst, n);
+    else k_dense64<false><<<grid, kPairBlock, 0, s>>>(q64, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, cut, dst, n);
+  } else {
+    auto kernel = track ? (short_atan ? k_dense32<true, true> : k_dense32<true, false>)
+                        : (short_atan ? k_dense32<false, true> : k_dense32<false, false>);
+    kernel<<<grid, kPairBlock, 0, s>>>(q32, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, cut, dst, n);
+  }
+  probe_mark(s);
+  probe_count(direct ? 1 : 2);
+  if (!direct) k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(partial, n, pl.chunks, n, nullptr, out, track ? 1 : 0);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ the pass
 // Site count of a shell pass (offsets[n] after the scan), for sizing the workspace.
 cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, int n, int gid, double s_margin,

@@ -65,6 +65,11 @@ struct NearLaunch {
   Rows out;
 };
 cudaError_t launch_near(const NearLaunch& L, cudaStream_t s);
+// The near field for wide cutoffs, summed over every image (all-pairs tiles, near-field
+// cutoff and window); `partial` holds chunks*n rows when chunks > 1.
+cudaError_t launch_dense_near(int prec, bool track, bool short_atan, const float4* q32, const double4* q64, int n,
+                              int gid, const PairsPlan& pl, double cut2, double chord, double cut_z, double cut_w,
+                              Rows partial, Rows out, cudaStream_t s);
 cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, int n, int gid, double s_margin,
                                uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, cudaStream_t s);
 
