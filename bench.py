@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the batched (config 4) and served (config 5) sections")
     return p.parse_args()
 
 
@@ -243,6 +245,48 @@ def e2e_requests(zo, seed, requests):
     return evals * len(lat) / sum(lat), lat, stats
 
 
+def batched_section(zo, samples=256, steps=50):
+    """Config 4: 256 samples (groups uniform over the eleven, N log-uniform in [1e3, 2e5],
+    seeds 0..255, neighbourhood 20), 50 BB steps each, relaxed side by side; pair-evals/s
+    over the whole batch (steps plus each sample's closing force pass), wall clock."""
+    from zxtalori_b200 import batch, serve
+
+    specs = batch.random_samples(samples)
+    t = time.perf_counter()
+    grids = batch.make_grids(specs)
+    setup = time.perf_counter() - t
+    evals = sum(batch.pair_evals(s.count, serve.ORDER[s.group], s.neighbourhood, steps) for s in specs)
+    try:
+        t = time.perf_counter()
+        batch.relax_batch(grids, steps)
+        dt = time.perf_counter() - t
+    finally:
+        for g in grids:
+            g.close()
+    return {"samples": samples, "steps": steps, "sum_n": sum(s.count for s in specs), "pair_evals_per_s": evals / dt,
+            "seconds": dt, "setup_seconds": setup,
+            "timing": "wall clock of zo_batch_relax (all steps and closing passes), samples created beforehand"}
+
+
+def served_section(zo, rate=0.8, duration=20.0, plain_requests=4):
+    """Config 5: Poisson arrivals (rate/s over `duration` s) of relax+measure requests, group
+    uniform, N log-uniform in [500, 1e6], steps uniform in [10, 200], all pairs below 5,000
+    orientations else neighbourhood 20; continuous batching in FP32-refined mode, and the
+    plain FP64 path one request at a time on the first requests of the same stream."""
+    from zxtalori_b200 import serve
+
+    reqs = serve.poisson_requests(rate, duration, seed=5)
+    t = time.perf_counter()
+    served = serve.Server().run(reqs)
+    wall = time.perf_counter() - t
+    info = serve.summary(served)
+    first = sorted(reqs, key=lambda r: r.arrival)[:plain_requests]
+    plain = serve.summary(serve.serve_one_at_a_time([serve.Request(r.id, r.group, r.count, r.steps, r.seed,
+                                                                   r.neighbourhood, 0.0) for r in first]))
+    return {"rate_per_s": rate, "arrival_window_s": duration, "wall_s": wall, **info,
+            "plain_fp64_one_at_a_time": plain, "plain_requests": plain_requests}
+
+
 def traffic_from_profile():
     """DRAM bytes per launch of the near-field row kernel from the committed ncu summary."""
     path = ROOT / "profiles" / "near_rows_kernel.md"
@@ -287,6 +331,11 @@ def run_ours(args, dist):
     e2e_value = dist.reduce(e2e_value, "sum")
     if dist.rank != 0:
         return 0
+    # Batched and served workloads (configs 4 and 5), one GPU only.
+    extras = {}
+    if args.gpus == 1 and not args.no_extras:
+        extras["batched"] = batched_section(zo)
+        extras["served"] = served_section(zo)
     kernel_avg_s = kernel_ms / max(1, kernel_launches) / 1e3
     achieved = EVALS_PER_PASS * FLOPS_PER_NEAR_PAIR / kernel_avg_s / 1e12
     traffic = traffic_from_profile()
@@ -313,6 +362,7 @@ def run_ours(args, dist):
                         f"steps (+1 closing force pass), read N quaternions back"},
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": clocks.summary(),
+        **extras,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -311,8 +311,8 @@ StepResult RelaxState::finish(cudaStream_t s) {
   return step_result(st);
 }
 
-Measures RelaxState::summarize(cudaStream_t s, int n, int order, float* degrees, int* neighbours, int prec,
-                               const float4* q32, int gid) {
+void RelaxState::summarize_async(cudaStream_t s, int n, int order, RowSummary* summary, float* degrees,
+                                 int* neighbours, int prec, const float4* q32, int gid) {
   const Rows r = rows_.rows();
   const bool near_sites = near_ != nullptr && !near_->dense();
   const uint32_t* scode = near_sites ? near_->sorted_codes() : nullptr;
@@ -322,12 +322,21 @@ Measures RelaxState::summarize(cudaStream_t s, int n, int order, float* degrees,
   ZO_CUDA(launch_row_summary(r, n, summary_partials_.as<double>(), near_partials_.as<double>(), near_rows_.as<int>(),
                              summary_.as<RowSummary>(), s));
   ZO_CUDA(launch_nearest_degrees(r.nearest, n, degrees_.as<float>(), s));
-  RowSummary sum;
-  ZO_CUDA(cudaMemcpyAsync(&sum, summary_.as<RowSummary>(), sizeof sum, cudaMemcpyDeviceToHost, s));
+  ZO_CUDA(cudaMemcpyAsync(summary, summary_.as<RowSummary>(), sizeof(RowSummary), cudaMemcpyDeviceToHost, s));
   if (degrees) ZO_CUDA(cudaMemcpyAsync(degrees, degrees_.as<float>(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
   if (neighbours) ZO_CUDA(cudaMemcpyAsync(neighbours, neighbours_.as<int>(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
-  ZO_CUDA(cudaStreamSynchronize(s));
   order_ = order;
+}
+
+Measures RelaxState::summarize(cudaStream_t s, int n, int order, float* degrees, int* neighbours, int prec,
+                               const float4* q32, int gid) {
+  RowSummary sum;
+  summarize_async(s, n, order, &sum, degrees, neighbours, prec, q32, gid);
+  ZO_CUDA(cudaStreamSynchronize(s));
+  return measures_of(sum, n, order);
+}
+
+Measures RelaxState::measures_of(const RowSummary& sum, int n, int order) const {
   if (!(sum.nearest > 0)) throw Failure("DuplicateOrientations");
   Measures m;
   m.count_extended = 2.0 * order * n;
@@ -430,16 +439,83 @@ void Engine::relax_async(uint32_t steps) {
 }
 
 void Engine::relax_finish() {
+  finish_async();
+  finish_collect();
+}
+
+void Engine::Staging::ensure(size_t n) {
+  if (n <= capacity && summary) return;
+  release();
+  const size_t cap = std::max<size_t>(n, 1);
+  ZO_CUDA(cudaMallocHost(&summary, sizeof(RowSummary)));
+  ZO_CUDA(cudaMallocHost(&state, sizeof(RelaxDev)));
+  ZO_CUDA(cudaMallocHost(&overflow, sizeof(unsigned int)));
+  ZO_CUDA(cudaMallocHost(&degrees, cap * sizeof(float)));
+  ZO_CUDA(cudaMallocHost(&neighbours, cap * sizeof(int)));
+  ZO_CUDA(cudaMallocHost(&positions, cap * 4 * sizeof(float)));
+  capacity = cap;
+}
+
+void Engine::Staging::release() {
+  for (void* p : {(void*)summary, (void*)state, (void*)overflow, (void*)degrees, (void*)neighbours, (void*)positions})
+    if (p) cudaFreeHost(p);
+  summary = nullptr;
+  state = nullptr;
+  overflow = nullptr;
+  degrees = nullptr;
+  neighbours = nullptr;
+  positions = nullptr;
+  capacity = 0;
+}
+
+// The closing force pass of a relaxation (RelaxState.complete, src/pairs.zig:377-399),
+// enqueued with the copies of the last step's state, the summary, nearest degrees and
+// neighbours, the overflow flag and the positions into pinned host memory.
+void Engine::finish_async() {
   ZO_CUDA(cudaSetDevice(device_));
   if (!relaxing_) sync_neighbourhood();
   relaxing_ = false;
   measures_.reset();
-  std::optional<StepResult> last;
-  const bool recorded = recorded_;
+  finish_recorded_ = recorded_;
   recorded_ = false;
-  if (recorded) last = relax_state_.finish(stream_);
-  Measures m = relax_state_measure();
-  fetch();
+  const int n = (int)n_;
+  stage_.ensure(n_);
+  relax_state_.prepare(n, prec_);
+  if (finish_recorded_)
+    ZO_CUDA(cudaMemcpyAsync(stage_.state, relax_state_.state_device(), sizeof(RelaxDev), cudaMemcpyDeviceToHost,
+                            stream_));
+  relax_state_.current = false;
+  relax_state_.record_forces(stream_, prec_, q32(), q64(), n, group_, true, budget_scale_, sms_);
+  const NearField* nf = relax_state_.near_field();
+  const unsigned int* flag = nf ? nf->overflow_flag() : nullptr;
+  finish_has_overflow_ = flag != nullptr;
+  if (flag) ZO_CUDA(cudaMemcpyAsync(stage_.overflow, flag, 4, cudaMemcpyDeviceToHost, stream_));
+  relax_state_.summarize_async(stream_, n, (int)order(), stage_.summary, stage_.degrees, stage_.neighbours, prec_,
+                               q32(), group_);
+  ZO_CUDA(cudaMemcpyAsync(stage_.positions, q32(), (size_t)n * 16, cudaMemcpyDeviceToHost, stream_));
+  finishing_ = true;
+}
+
+void Engine::finish_collect() {
+  if (!finishing_) throw Failure("NoFinishPending");
+  finishing_ = false;
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  std::optional<StepResult> last;
+  if (finish_recorded_) last = relax_state_.result_of(*stage_.state);
+  Measures m;
+  if (finish_has_overflow_ && *stage_.overflow) {
+    // The shell outgrew its workspace: size it again and redo the pass synchronously.
+    relax_state_.near_field()->invalidate();
+    m = relax_state_measure();
+    fetch();
+  } else {
+    m = relax_state_.measures_of(*stage_.summary, (int)n_, (int)order());
+    point_separation_.assign(stage_.degrees, stage_.degrees + n_);
+    point_neighbours_.assign(stage_.neighbours, stage_.neighbours + n_);
+    point_separation_iteration_ = iteration_;
+    host_.assign(stage_.positions, stage_.positions + 4 * (size_t)n_);
+    relax_state_.current = true;
+  }
   if (last) {
     step_deg_ = last->max_step_deg;
     force_rms_ = last->force_rms;
@@ -726,17 +802,10 @@ void Engine::relax(uint32_t steps) {
   measures_.reset();
   // One wait ends the batch: the last step, positions, energy and separation, whose forces
   // start the next step (RelaxState.complete, src/pairs.zig:377-399).
-  std::optional<StepResult> last;
-  if (recorded) last = relax_state_.finish(stream_);
-  Measures m = relax_state_measure();
-  fetch();
-  if (last) {
-    step_deg_ = last->max_step_deg;
-    force_rms_ = last->force_rms;
-  }
-  measures_ = m;
-  full_measures_ = false;
-  measure_iteration_ = iteration_;
+  relaxing_ = true;
+  recorded_ = recorded;
+  finish_async();
+  finish_collect();
 }
 
 void Engine::identity(bool add, bool fixed) {

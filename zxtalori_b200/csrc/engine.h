@@ -85,6 +85,12 @@ class NearField {
   bool ready() const { return ready_; }
   // Summed over every image instead of the shell and chart grid (wide cutoffs).
   bool dense() const { return dense_; }
+  // Device word set when a pass produced more sites than the workspace holds (null when dense).
+  const unsigned int* overflow_flag() const {
+    return dense_ || !ready_ ? nullptr : &grid_.as<NearGrid>()->overflow;
+  }
+  // The next pass sizes the workspace again (after an observed overflow).
+  void invalidate() { ready_ = false; }
 
  private:
   uint64_t generation_ = 0;
@@ -124,6 +130,13 @@ class RelaxState {
   // Quick measures of `rows()` (after a force pass), nearest degrees and neighbours to host.
   Measures summarize(cudaStream_t s, int n, int order, float* degrees, int* neighbours, int prec, const float4* q32,
                      int gid);
+  // The same, split: enqueue the kernels and the copies of the summary, degrees and
+  // neighbours into host memory; then, after the stream is synchronised, the measures.
+  void summarize_async(cudaStream_t s, int n, int order, RowSummary* summary, float* degrees, int* neighbours,
+                       int prec, const float4* q32, int gid);
+  Measures measures_of(const RowSummary& sum, int n, int order) const;
+  const RelaxDev* state_device() const { return state_.as<RelaxDev>(); }
+  StepResult result_of(const RelaxDev& st) const { return step_result(st); }
   bool near_overflowed(cudaStream_t s) { return near_ && near_->overflowed(s); }
   NearField* near_field() { return near_.get(); }
   // Identifies the buffers and settings a captured step reads; any change makes it stale.
@@ -170,6 +183,10 @@ class Engine {
   // and readback of relax(). Several engines relax concurrently this way.
   void relax_async(uint32_t steps);
   void relax_finish();
+  // relax_finish in two halves for batches: enqueue the closing force pass and the copies
+  // of its results into pinned host memory, then collect them after one wait.
+  void finish_async();
+  void finish_collect();
   // Whether the engine's stream has no work pending.
   bool idle();
   void set_graphs(bool enabled) {
@@ -200,6 +217,21 @@ class Engine {
   char err[2048] = {0};
 
  private:
+  // Pinned host copies of a closing pass's results (asynchronous finish).
+  struct Staging {
+    RowSummary* summary = nullptr;
+    RelaxDev* state = nullptr;
+    unsigned int* overflow = nullptr;
+    float* degrees = nullptr;
+    int* neighbours = nullptr;
+    float* positions = nullptr;
+    size_t capacity = 0;
+    void ensure(size_t n);
+    void release();
+    ~Staging() { release(); }
+  };
+  Staging stage_;
+  bool finishing_ = false, finish_recorded_ = false, finish_has_overflow_ = false;
   void step_once();
   void capture_step_graph();
   void drop_graph();

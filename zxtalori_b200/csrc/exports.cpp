@@ -173,14 +173,19 @@ int zo_graphs(void* h, uint32_t enabled) {
 }
 
 int zo_batch_relax(void* const* handles, uint32_t count, uint32_t steps, int32_t* status) {
+  // Every engine has its own stream, so the samples' kernels run side by side. Steps are
+  // enqueued round-robin (one step of every sample, then the next), so samples that share
+  // a hardware queue interleave instead of waiting for each other; then every closing pass
+  // is enqueued before any is waited for.
+  for (uint32_t k = 0; k < count; ++k) status[k] = 0;
+  for (uint32_t s = 0; s < steps; ++s)
+    for (uint32_t k = 0; k < count; ++k)
+      if (status[k] == 0) status[k] = guarded(handles[k], "Relaxation failed", [&](Engine& e) { e.relax_async(1); });
+  for (uint32_t k = 0; k < count; ++k)
+    if (status[k] == 0) status[k] = guarded(handles[k], "Relaxation failed", [](Engine& e) { e.finish_async(); });
   int failures = 0;
-  // Enqueue every sample's steps first (each engine has its own stream, so the samples'
-  // kernels run side by side), then close each one with its force pass and readback.
   for (uint32_t k = 0; k < count; ++k) {
-    status[k] = guarded(handles[k], "Relaxation failed", [&](Engine& e) { e.relax_async(steps); });
-  }
-  for (uint32_t k = 0; k < count; ++k) {
-    if (status[k] == 0) status[k] = zo_relax_finish(handles[k]);
+    if (status[k] == 0) status[k] = guarded(handles[k], "Relaxation failed", [](Engine& e) { e.finish_collect(); });
     failures += status[k] != 0;
   }
   return failures;
