@@ -43,6 +43,10 @@ FLUSH_BYTES = 256 * 1024 * 1024
 # sign 2, direction 21, force/curvature/energy 14, window and its slope term 29,
 # accumulation 6; each add, multiply, divide, sqrt, atan, sin, min/max/select counts 1.
 FLOPS_PER_NEAR_PAIR = 120
+# The same count for one all-pairs Quey pair (shaders/pairs.wgsl:250-262, 293-300): chord
+# tests and dot products 22, nearest 2, near/far and t 6, angle and powers 14, sine 5, sign
+# 2, direction 21, force/curvature/energy 14, accumulation 5.
+FLOPS_PER_PAIR = 91
 
 
 def neighbours(n, order, delta):
@@ -59,7 +63,9 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-extras", action="store_true",
-                   help="skip the batched (config 4) and served (config 5) sections")
+                   help="skip the all-pairs, spacing, batched and served sections")
+    p.add_argument("--large", action="store_true",
+                   help="also time the default measures of group I at N=1M (all pairs, about a minute)")
     return p.parse_args()
 
 
@@ -287,6 +293,78 @@ def served_section(zo, rate=0.8, duration=20.0, plain_requests=4):
             "plain_fp64_one_at_a_time": plain, "plain_requests": plain_requests}
 
 
+def _device_seconds(lib, handle, steps, warmup):
+    out = np.zeros(4 + steps, np.float64)
+    rc = lib.zo_bench(handle, steps, warmup, float(FLUSH_BYTES), out.ctypes.data_as(C.POINTER(C.c_double)), len(out))
+    if rc != 0:
+        raise RuntimeError(lib.zo_error(handle).decode())
+    return out
+
+
+def allpairs_section(zo, peak, count=1048, steps=30, kernel_count=16384):
+    """Config 1 (group O, N=1,048 Haar seed 193, all pairs, 30 steps then every measure) as
+    requests through the public API in both precision modes, and the all-pairs row kernel
+    on the FP32 roofline at N=16,384 (6.4e9 pairs per pass)."""
+    result = {"workload": f"O, N={count} Haar (seed {SEED}), all pairs, {steps} steps + measure"}
+    evals = (steps + 1) * count * count * ORDER
+    for precision in ("fp64", "fp32"):
+        lat = []
+        for rep in range(4):
+            t = time.perf_counter()
+            g = zo.haar(GROUP, count, SEED, precision=precision)
+            g.relax(steps)
+            m = g.measure()
+            dt = time.perf_counter() - t
+            g.close()
+            if rep:
+                lat.append(dt)
+        result[precision] = {"request_s_p50": float(np.median(lat)), "pair_evals_per_s": evals / float(np.median(lat)),
+                             "quey_energy": m["quey_energy"], "separation_deg": m["separation_deg"],
+                             "riesz_2": m["riesz_2"], "log_ratio": m["log_ratio"]}
+    g = zo.haar(GROUP, kernel_count, SEED)
+    g.relax(0, neighbourhood=0)
+    out = _device_seconds(g._lib, g._handle, 5, 3)
+    g.close()
+    avg = out[1] / max(1, out[2]) / 1e3
+    pairs = kernel_count * kernel_count * ORDER
+    achieved = pairs * FLOPS_PER_PAIR / avg / 1e12
+    result["kernel"] = {"kernel": "k_pairs32 (all-pairs rows)", "n": kernel_count, "pairs_per_pass": pairs,
+                        "kernel_ms_avg": avg * 1e3, "pair_evals_per_s": pairs / avg, "achieved_tflops": achieved,
+                        "peak_tflops": peak, "frac": achieved / peak, "flops_per_pair": FLOPS_PER_PAIR,
+                        "step_ms": out[0] / 5}
+    return result
+
+
+def spacing_section(zo, count=10_000_000, seed=7, measure_count=None):
+    """Config 3: the spacing pass (per-orientation nearest SO(3) angle and neighbour index;
+    neighbourhood 4 above 20,000 orientations) over group I, N=10M Haar seed 7, wall clock
+    through the public API (the second of two calls: the first sizes the workspace); with
+    `measure_count`, the default measures of I at that size (all pairs, FP32)."""
+    g = zo.haar("I", count, seed)
+    t = time.perf_counter()
+    g.spacing()
+    first = time.perf_counter() - t
+    t = time.perf_counter()
+    sep = g.spacing()["separation_deg"]
+    dt = time.perf_counter() - t
+    degrees = g.point_values("separation")
+    g.close()
+    n_pairs = count * neighbours(count, 60, 4.0)
+    result = {"workload": f"I, N={count} Haar (seed {seed}), spacing with neighbourhood 4",
+              "seconds": dt, "first_call_seconds": first, "pair_evals_per_s": n_pairs / dt,
+              "separation_deg": sep, "median_nearest_deg": float(np.median(degrees))}
+    if measure_count:
+        g = zo.haar("I", measure_count, seed)
+        t = time.perf_counter()
+        m = g.measure()
+        dt = time.perf_counter() - t
+        g.close()
+        pairs = measure_count * measure_count * 60
+        result["measure"] = {"n": measure_count, "seconds": dt, "pair_evals_per_s": pairs / dt,
+                             "quey_energy": m["quey_energy"], "separation_deg": m["separation_deg"]}
+    return result
+
+
 def traffic_from_profile():
     """DRAM bytes per launch of the near-field row kernel from the committed ncu summary."""
     path = ROOT / "profiles" / "near_rows_kernel.md"
@@ -331,9 +409,11 @@ def run_ours(args, dist):
     e2e_value = dist.reduce(e2e_value, "sum")
     if dist.rank != 0:
         return 0
-    # Batched and served workloads (configs 4 and 5), one GPU only.
+    # All pairs, spacing, batched and served workloads (configs 1, 3, 4, 5), one GPU only.
     extras = {}
     if args.gpus == 1 and not args.no_extras:
+        extras["allpairs"] = allpairs_section(zo, peak)
+        extras["spacing"] = spacing_section(zo, measure_count=1_000_000 if args.large else None)
         extras["batched"] = batched_section(zo)
         extras["served"] = served_section(zo)
     kernel_avg_s = kernel_ms / max(1, kernel_launches) / 1e3

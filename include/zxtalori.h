@@ -129,6 +129,13 @@ int zo_batch_relax(void* const* handles, uint32_t count, uint32_t steps, int32_t
 /* Measurement hook (no reference counterpart): FP32 FMA throughput of the engine's device
  * in TFLOP/s (2 flops per FMA), the denominator of the pair kernels' roofline; -1 on error. */
 double zo_fp32_peak(void* h);
+/* Rows of the inverse-Hopf product grid of frequency `freq` before the zone fold, on the
+ * host (src/hopf.zig:528-607 points(); zo_generate folds them on the GPU): 4 floats per
+ * row, scalar first, in the reference's row order. With out == NULL returns the row count
+ * (src/hopf.zig:78 count()); else writes the rows when capacity (in rows) suffices. Returns
+ * the row count, -1 for an unknown group, a frequency outside 1..512 or a grid above ten
+ * million rows, -2 when capacity is too small. Needs no GPU. */
+int64_t zo_hopf_points(uint32_t group, uint32_t freq, float* out, uint64_t capacity);
 
 /* No counterpart in the reference. The all-pairs force pass (FP32 pair arithmetic, FP64
  * sums) for callers that cannot allocate device memory: a framework that owns every

@@ -9,6 +9,6 @@ import os as _os
 # when CUDA initialises, so it must be set before the first CUDA call of the process.
 _os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
-from .api import GROUPS, PRECISIONS, Grid, from_quaternions, generate, haar, load, library_path  # noqa: E402
+from .api import GROUPS, PRECISIONS, Grid, from_quaternions, generate, haar, hopf_points, load, library_path  # noqa: E402
 
-__all__ = ["GROUPS", "PRECISIONS", "Grid", "generate", "from_quaternions", "load", "haar", "library_path"]
+__all__ = ["GROUPS", "PRECISIONS", "Grid", "generate", "from_quaternions", "load", "haar", "hopf_points", "library_path"]

@@ -1,5 +1,6 @@
 // Engine: sample state and the reference's policies over the CUDA kernels.
 #include "engine.h"
+#include "hopf.h"
 
 #include <algorithm>
 #include <cmath>
@@ -218,16 +219,22 @@ void RelaxState::reset() {
   n_ = 0;
   prec_ = -1;
   current = false;
-  // The near-field settings stay; its buffers are sized again on the next pass.
-  if (near_) near_ = std::make_unique<NearField>(near_->gid(), near_->delta());
+  // The near-field settings stay; the workspace is sized again on the next pass, reusing
+  // its allocations where they are large enough (a new sample of similar size frees and
+  // allocates nothing).
+  if (near_) near_->invalidate();
 }
 
 void RelaxState::set_near(int gid, std::optional<double> delta) {
   if (near_) {
     if (delta && near_->gid() == gid && near_->delta() == *delta) return;
-    near_.reset();
     current = false;
     ++generation_;
+    if (delta) {
+      near_->reconfigure(gid, *delta);  // keeps the allocations
+      return;
+    }
+    near_.reset();
   }
   if (delta) {
     near_ = std::make_unique<NearField>(gid, *delta);
@@ -236,7 +243,7 @@ void RelaxState::set_near(int gid, std::optional<double> delta) {
   }
 }
 
-void RelaxState::prepare(int n, int prec) {
+void RelaxState::prepare(cudaStream_t s, int n, int prec) {
   if (n_ == n && prec_ == prec) return;
   ++generation_;
   n_ = n;
@@ -245,16 +252,16 @@ void RelaxState::prepare(int n, int prec) {
   rows_.ensure(n);
   prev_f_.ensure((size_t)n * sizeof(double4));
   prev_d_.ensure((size_t)n * sizeof(double4));
-  ZO_CUDA(cudaMemset(prev_f_.as<void>(), 0, (size_t)n * sizeof(double4)));
-  ZO_CUDA(cudaMemset(prev_d_.as<void>(), 0, (size_t)n * sizeof(double4)));
+  ZO_CUDA(cudaMemsetAsync(prev_f_.as<void>(), 0, (size_t)n * sizeof(double4), s));
+  ZO_CUDA(cudaMemsetAsync(prev_d_.as<void>(), 0, (size_t)n * sizeof(double4), s));
   state_.ensure(sizeof(RelaxDev));
-  ZO_CUDA(cudaMemset(state_.as<void>(), 0, sizeof(RelaxDev)));
+  ZO_CUDA(cudaMemsetAsync(state_.as<void>(), 0, sizeof(RelaxDev), s));
   const int blocks = reduce_blocks(n);
   stats_partials_.ensure((size_t)blocks * 5 * sizeof(double));
   hist_.ensure(512 * 4);
-  ZO_CUDA(cudaMemset(hist_.as<void>(), 0, 512 * 4));
+  ZO_CUDA(cudaMemsetAsync(hist_.as<void>(), 0, 512 * 4, s));
   summary_.ensure(sizeof(RowSummary));
-  ZO_CUDA(cudaMemset(summary_.as<void>(), 0, sizeof(RowSummary)));
+  ZO_CUDA(cudaMemsetAsync(summary_.as<void>(), 0, sizeof(RowSummary), s));
   summary_partials_.ensure((size_t)blocks * 2 * sizeof(double));
   near_partials_.ensure((size_t)blocks * sizeof(double));
   near_rows_.ensure((size_t)blocks * sizeof(int));
@@ -277,7 +284,7 @@ void RelaxState::record_forces(cudaStream_t s, int prec, const float4* q32, cons
 
 void RelaxState::step(cudaStream_t s, int prec, float4* q32, double4* q64, int n, int gid, int fixed,
                       double budget_scale, int sms) {
-  prepare(n, prec);
+  prepare(s, n, prec);
   if (!current) record_forces(s, prec, q32, q64, n, gid, false, budget_scale, sms);
   current = false;
   order_ = host_group_order(gid);
@@ -480,7 +487,7 @@ void Engine::finish_async() {
   recorded_ = false;
   const int n = (int)n_;
   stage_.ensure(n_);
-  relax_state_.prepare(n, prec_);
+  relax_state_.prepare(stream_, n, prec_);
   if (finish_recorded_)
     ZO_CUDA(cudaMemcpyAsync(stage_.state, relax_state_.state_device(), sizeof(RelaxDev), cudaMemcpyDeviceToHost,
                             stream_));
@@ -591,6 +598,9 @@ void Engine::set(int gid, const float* values, size_t count) {
   fetch();
   adopt(n);
   generator_ = "Imported quaternions";
+  grid_kind_.clear();
+  h_ = 0;
+  base_count_ = n;
 }
 
 void Engine::generate_random(int gid, uint32_t count, uint32_t seed) {
@@ -605,12 +615,35 @@ void Engine::generate_random(int gid, uint32_t count, uint32_t seed) {
   fetch();
   adopt(count);
   generator_ = "Haar random";
+  grid_kind_.clear();
+  h_ = 0;
+  base_count_ = count;
   seed_ = seed;
 }
 
+// src/engine.zig:244-281: freq = 0 takes the frequency whose count is nearest the target;
+// counts are never cut. The rows are orbit images: the zone fold picks each one's
+// representative. FCC transports (kind 2) are not part of this engine.
 void Engine::generate_grid(int gid, uint32_t freq, uint32_t target, uint32_t seed, uint32_t kind) {
-  (void)gid, (void)freq, (void)target, (void)seed, (void)kind;
-  throw Failure("HopfGridNotAvailable");
+  if (target > hopf::kMaxCount) throw Failure("GridTooLarge");
+  if (kind == 2) throw Failure(gid < 8 ? "TransportNeedsTOrOOrI" : "TransportNotAvailable");
+  const uint32_t f = freq == 0 ? hopf::nearest_frequency(gid, target == 0 ? 2048 : target) : freq;
+  const std::vector<float> rows = hopf::points(gid, f);
+  const uint32_t n = (uint32_t)(rows.size() / 4);
+  ZO_CUDA(cudaSetDevice(device_));
+  q32_.ensure((size_t)n * 16);
+  ZO_CUDA(cudaMemcpyAsync(q32_.as<float4>(), rows.data(), (size_t)n * 16, cudaMemcpyHostToDevice, stream_));
+  if (prec_ == kFP64) q64_.ensure((size_t)n * 32);
+  ZO_CUDA(launch_fold(q32_.as<float4>(), q64(), (int)n, gid, prec_, true, stream_));
+  group_ = gid;
+  n_ = n;
+  fetch();
+  adopt(n);
+  generator_ = hopf::generator_name(gid);
+  grid_kind_ = "hopf";
+  h_ = f;
+  base_count_ = n;
+  seed_ = seed;
 }
 
 void Engine::set_precision(int prec) {
@@ -639,7 +672,7 @@ void Engine::sync_neighbourhood() {
 }
 
 Measures Engine::relax_state_measure() {
-  relax_state_.prepare((int)n_, prec_);
+  relax_state_.prepare(stream_, (int)n_, prec_);
   for (int attempt = 0; attempt < 4; ++attempt) {
     relax_state_.current = false;
     relax_state_.record_forces(stream_, prec_, q32(), q64(), (int)n_, group_, true, budget_scale_, sms_);
@@ -743,7 +776,7 @@ void Engine::spacing() {
   if (n_ < 2) throw Failure("TooFewOrientations");
   ZO_CUDA(cudaSetDevice(device_));
   spacing_state_.set_near(group_, n_ > kSpacingAllPairs ? std::optional<double>(kSpacingDelta) : std::nullopt);
-  spacing_state_.prepare((int)n_, prec_);
+  spacing_state_.prepare(stream_, (int)n_, prec_);
   point_separation_.resize(n_);
   point_neighbours_.resize(n_);
   point_separation_iteration_ = iteration_;
@@ -814,9 +847,13 @@ void Engine::identity(bool add, bool fixed) {
   if (add && !index) {
     std::vector<float> values(host_);
     values.insert(values.end(), {1.f, 0.f, 0.f, 0.f});
-    const std::string generator = generator_;
+    const std::string generator = generator_, grid_kind = grid_kind_;
+    const uint32_t h = h_, base_count = base_count_;
     set(group_, values.data(), values.size() / 4);
     generator_ = generator;
+    grid_kind_ = grid_kind;
+    h_ = h;
+    base_count_ = base_count;
     index = n_ - 1;
   }
   if (fixed && !index) throw Failure("IdentityMissingEnableAddIdentity");
@@ -847,7 +884,7 @@ void Engine::debug_rows(uint32_t what, double* out) {
   std::vector<int> degen;
   if (what == 0) {
     sync_neighbourhood();
-    relax_state_.prepare(n, prec_);
+    relax_state_.prepare(stream_, n, prec_);
     relax_state_.current = false;
     relax_state_.record_forces(stream_, prec_, q32(), q64(), n, group_, true, budget_scale_, sms_);
     r = relax_state_.rows();
@@ -902,7 +939,7 @@ void Engine::bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* 
   if (steps == 0 || out_len < 4) throw Failure("InvalidBench");
   ZO_CUDA(cudaSetDevice(device_));
   sync_neighbourhood();
-  relax_state_.prepare((int)n_, prec_);
+  relax_state_.prepare(stream_, (int)n_, prec_);
   relax_state_.current = false;
   for (uint32_t w = 0; w < std::max<uint32_t>(warmup, 1); ++w) step_once();
   ZO_CUDA(cudaStreamSynchronize(stream_));
@@ -1030,14 +1067,15 @@ const char* Engine::stats() {
   j.integer("count", n_);
   j.integer("count_extended", 2ll * order() * n_);
   j.str("generator", generator_);
-  j.null("grid");
-  j.integer("h", 0);
+  if (grid_kind_.empty()) j.null("grid");
+  else j.str("grid", grid_kind_);
+  j.integer("h", h_);
   j.integer("seed", seed_);
   j.integer("iteration", iteration_);
   j.boolean("fixed_identity", fix_identity_);
   if (auto idx = identity_index()) j.integer("identity_index", *idx);
   else j.null("identity_index");
-  j.integer("base_count", n_);
+  j.integer("base_count", base_count_);
   j.integer("inserted_count", 0);
   j.str("triangulation_backend", "none");
   j.null("covering_radius_deg");

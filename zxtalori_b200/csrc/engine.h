@@ -89,8 +89,14 @@ class NearField {
   const unsigned int* overflow_flag() const {
     return dense_ || !ready_ ? nullptr : &grid_.as<NearGrid>()->overflow;
   }
-  // The next pass sizes the workspace again (after an observed overflow).
+  // The next pass sizes the workspace again (after an observed overflow, or for a new
+  // sample); allocations large enough are reused.
   void invalidate() { ready_ = false; }
+  void reconfigure(int gid, double delta) {
+    gid_ = gid;
+    delta_ = delta;
+    ready_ = false;
+  }
 
  private:
   uint64_t generation_ = 0;
@@ -122,7 +128,7 @@ class RelaxState {
   Rows rows() const { return rows_.rows(); }
   bool current = false;
 
-  void prepare(int n, int prec);
+  void prepare(cudaStream_t s, int n, int prec);
   void record_forces(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, int gid, bool track,
                      double budget_scale, int sms);
   void step(cudaStream_t s, int prec, float4* q32, double4* q64, int n, int gid, int fixed, double budget_scale, int sms);
@@ -262,6 +268,10 @@ class Engine {
   uint32_t iteration_ = 0;
   uint32_t seed_ = 0;
   std::string generator_ = "none";
+  // Construction of a generated grid ("hopf"), its frequency and its row count before any
+  // identity was added; empty, 0 and the count for imported or random samples.
+  std::string grid_kind_;
+  uint32_t h_ = 0, base_count_ = 0;
   std::optional<Measures> measures_;
   uint32_t measure_iteration_ = 0;
   bool full_measures_ = false;

@@ -7,6 +7,7 @@
 #include <new>
 
 #include "engine.h"
+#include "hopf.h"
 #include "zxtalori.h"
 
 using zo::Engine;
@@ -189,6 +190,20 @@ int zo_batch_relax(void* const* handles, uint32_t count, uint32_t steps, int32_t
     failures += status[k] != 0;
   }
   return failures;
+}
+
+int64_t zo_hopf_points(uint32_t group, uint32_t freq, float* out, uint64_t capacity) {
+  if (group >= 11) return -1;
+  try {
+    const uint64_t n = zo::hopf::count((int)group, freq);
+    if (!out) return (int64_t)n;
+    if (capacity < n) return -2;
+    const std::vector<float> rows = zo::hopf::points((int)group, freq);
+    std::memcpy(out, rows.data(), rows.size() * sizeof(float));
+    return (int64_t)n;
+  } catch (const std::exception&) {
+    return -1;
+  }
 }
 
 double zo_fp32_peak(void* h) {
