@@ -129,6 +129,8 @@ int zo_batch_relax(void* const* handles, uint32_t count, uint32_t steps, int32_t
 /* Measurement hook (no reference counterpart): FP32 FMA throughput of the engine's device
  * in TFLOP/s (2 flops per FMA), the denominator of the pair kernels' roofline; -1 on error. */
 double zo_fp32_peak(void* h);
+/* The same probe with packed f32x2 FMAs (two FMAs per instruction); -1 on error. */
+double zo_fp32x2_peak(void* h);
 /* Rows of the inverse-Hopf product grid of frequency `freq` before the zone fold, on the
  * host (src/hopf.zig:528-607 points(); zo_generate folds them on the GPU): 4 floats per
  * row, scalar first, in the reference's row order. With out == NULL returns the row count

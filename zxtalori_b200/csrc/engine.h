@@ -207,12 +207,13 @@ class Engine {
   // events. out[0] total step ms, out[1] dominant-kernel ms, out[2] its launches, out[3]
   // kernel launches per step, out[4 ..] each step's ms (as room allows).
   void bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len);
-  // Measured FP32 FMA throughput of this engine's device, TFLOP/s.
-  double fp32_peak() {
+  // Measured FP32 FMA throughput of this engine's device, TFLOP/s, with scalar FMAs or
+  // with packed (f32x2) FMAs.
+  double fp32_peak(bool packed = false) {
     ZO_CUDA(cudaSetDevice(device_));
-    double t = 0;
-    ZO_CUDA(measure_fp32_peak(sms_, &t));
-    return t;
+    double t = 0, t2 = 0;
+    ZO_CUDA(measure_fp32_peak(sms_, &t, packed ? &t2 : nullptr));
+    return packed ? t2 : t;
   }
 
   int group() const { return group_; }

@@ -212,4 +212,10 @@ double zo_fp32_peak(void* h) {
   return value;
 }
 
+double zo_fp32x2_peak(void* h) {
+  double value = -1.0;
+  if (guarded(h, "Probe", [&](Engine& e) { value = e.fp32_peak(true); }) != 0) return -1.0;
+  return value;
+}
+
 }  // extern "C"

@@ -358,12 +358,51 @@ __device__ __forceinline__ bool row_run(const WarpBox& b, const NearGrid& g, con
   return start < end;
 }
 
+// Per-warp data of the row walk, kept in shared memory (it is warp-uniform) so the hot
+// loop's registers go to the pair arithmetic.
+struct NearWalk {
+  WarpBox box;
+  float lower[3], cells_per_unit;
+  int sdim;
+};
+
+// row_run from the warp's shared walk data.
+__device__ __forceinline__ bool walk_row(const NearWalk& W, const uint32_t* cell_off, int r, uint32_t& start,
+                                         uint32_t& end) {
+  const WarpBox& b = W.box;
+  const int ny = b.chi[1] - b.clo[1] + 1;
+  const int y = b.clo[1] + r % ny, z = b.clo[2] + r / ny;
+  const float width = 1.0f / W.cells_per_unit;
+  const float cy = W.lower[1] + (float)y * width, cz = W.lower[2] + (float)z * width;
+  const float gy = fmaxf(0.f, fmaxf(cy - b.hi[1], b.lo[1] - (cy + width)));
+  const float gz = fmaxf(0.f, fmaxf(cz - b.hi[2], b.lo[2] - (cz + width)));
+  const float rest = b.d * b.d - gy * gy - gz * gz;
+  if (rest < 0.f) return false;
+  const float span = sqrtf(rest);
+  const int x0 = cell_axis(b.lo[0] - span, W.lower[0], W.cells_per_unit, W.sdim);
+  const int x1 = cell_axis(b.hi[0] + span, W.lower[0], W.cells_per_unit, W.sdim);
+  const int row = W.sdim * (y + W.sdim * z);
+  start = cell_off[row + x0];
+  end = cell_off[row + x1 + 1];
+  return start < end;
+}
+
 // The gather (pairs.wgsl:363-416). Each lane holds one source; the warp streams its
-// cell-row runs through shared memory 32 sites at a time (quaternion, |y|^2 and code) and
-// every lane tests its source against each site. For a site within the cutoff chord the
-// windowed pair runs with dp2 = 2(|x|^2+|y|^2) - dm2 (parallelogram law; the site is the
-// near twin), and the force is kept as sum c (x - y), turned into a force once per source.
-// Tile sums are FP32 (FP64 in FP64 mode), merged into FP64 per tile.
+// cell-row runs through shared memory 32 sites at a time and every lane tests its source
+// against each site, two sites per iteration with packed FP32 arithmetic: the tile holds
+// the sites as pairs, component by component, with 2|y|^2 and the code of each. For a site
+// within the cutoff chord the windowed pair runs with dp2 = 2(|x|^2+|y|^2) - dm2
+// (parallelogram law; the site is the near twin); sites beyond it contribute exactly zero
+// through the window, and the nearest chord is taken over every site and reset to 4 when
+// it exceeds the cutoff (no site within it), which is the same as testing each site. The
+// force is kept as sum c (x - y), turned into a force once per source. Tile sums are FP32,
+// merged into FP64 per tile.
+struct NearSlots {
+  float4 wx[16];  // (w, w', x, x') of sites 2u and 2u+1
+  float4 yz[16];  // (y, y', z, z')
+  float4 nc[16];  // (2|y|^2, 2|y'|^2, code bits, code' bits)
+};
+
 template <bool TRACK, bool SHORT>
 __global__ void __launch_bounds__(kNearWarps * 32, 8) k_near32(const float4* __restrict__ q, int n,
                                                               const uint32_t* __restrict__ src_perm,
@@ -372,9 +411,12 @@ __global__ void __launch_bounds__(kNearWarps * 32, 8) k_near32(const float4* __r
                                                               const uint32_t* __restrict__ cell_off,
                                                               const NearGrid* __restrict__ gp, NearCut cut, int slices,
                                                               Rows out, int stride) {
-  __shared__ float4 tq[kNearWarps][32];
-  __shared__ float2 tm[kNearWarps][32];  // |y|^2, code bits
+  __shared__ NearSlots tiles[kNearWarps];
+  __shared__ NearWalk walks[kNearWarps];
+  __shared__ double sums[6][kNearWarps * 32];  // FP64 row sums: force differences, curvature, energy
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  NearSlots& T = tiles[w];
+  NearWalk& W = walks[w];
   const int warp = blockIdx.x * kNearWarps + w;
   const int slice = blockIdx.y;
   if (warp * 32 >= n) return;
@@ -382,75 +424,118 @@ __global__ void __launch_bounds__(kNearWarps * 32, 8) k_near32(const float4* __r
   const bool live = p < n;
   const uint32_t i = live ? src_perm[p] : 0u;
   const float4 x = q[i];
-  const NearGrid g = *gp;
-  WarpBox box;
-  if (!warp_box(chart(x), live, g, (float)cut.chord, box)) return;
-  const float cut2 = (float)cut.cut2, cz = (float)cut.cut_z, cw = (float)cut.cut_w;
+  {
+    const NearGrid g = *gp;
+    WarpBox box;
+    if (!warp_box(chart(x), live, g, (float)cut.chord, box)) return;
+    if (lane == 0) {
+      W.box = box;
+      for (int a = 0; a < 3; ++a) W.lower[a] = g.lower[a];
+      W.cells_per_unit = g.cells_per_unit;
+      W.sdim = g.sdim;
+    }
+  }
+  for (int k = 0; k < 6; ++k) sums[k][threadIdx.x] = 0.0;
+  __syncwarp();
+  const float cut2 = (float)cut.cut2, cw = (float)cut.cut_w, czw = (float)(cut.cut_z * cut.cut_w);
   const float nx2 = 2.0f * fmaf(x.x, x.x, fmaf(x.y, x.y, fmaf(x.z, x.z, x.w * x.w)));
-  double yw = 0, yx = 0, yy = 0, yz = 0, fc = 0, fe = 0;
+  const float2 xw = splat(x.x), xx = splat(x.y), xy = splat(x.z), xz = splat(x.w), xn = splat(nx2);
   float best = 4.0f;
   int best_at = -1;
-  const int ny = box.chi[1] - box.clo[1] + 1, nz = box.chi[2] - box.clo[2] + 1;
-  const int rows = ny * nz;
+  const int rows = (W.box.chi[1] - W.box.clo[1] + 1) * (W.box.chi[2] - W.box.clo[2] + 1);
+  const int slot = lane >> 1, half = lane & 1;
   for (int r = slice; r < rows; r += slices) {
     uint32_t start, end;
-    if (!row_run(box, g, cell_off, r, start, end)) continue;
+    if (!walk_row(W, cell_off, r, start, end)) continue;
     for (uint32_t base = start; base < end; base += 32) {
       const int count = (int)min(32u, end - base);
       __syncwarp();
-      if (lane < count) {
-        const float4 s = sq[base + lane];
-        tq[w][lane] = s;
-        tm[w][lane] = make_float2(2.0f * fmaf(s.x, s.x, fmaf(s.y, s.y, fmaf(s.z, s.z, s.w * s.w))),
-                                  __uint_as_float(scode[base + lane]));
+      {
+        // A lane past the run's end writes a blank site: at the origin, dm2 = |x|^2 ~ 1 lies
+        // beyond every cutoff of the chart-grid path (r < 0.5 rad, cut2 < 0.25), and its
+        // code matches no source.
+        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t code = 0xffffffffu;
+        if (lane < count) {
+          s = sq[base + lane];
+          code = scode[base + lane];
+        }
+        float* a = reinterpret_cast<float*>(&T.wx[slot]);
+        float* b = reinterpret_cast<float*>(&T.yz[slot]);
+        float* c = reinterpret_cast<float*>(&T.nc[slot]);
+        a[half] = s.x;
+        a[2 + half] = s.y;
+        b[half] = s.z;
+        b[2 + half] = s.w;
+        c[half] = 2.0f * fmaf(s.x, s.x, fmaf(s.y, s.y, fmaf(s.z, s.z, s.w * s.w)));
+        c[2 + half] = __uint_as_float(code);
       }
       __syncwarp();
       if (!live) continue;
-      float sw = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, sc = 0.f, se = 0.f;
-      for (int t = 0; t < count; ++t) {
-        const float4 y = tq[w][t];
-        const float mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
-        const float dm2 = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
-        if (dm2 > cut2) continue;
-        const float2 m = tm[w][t];
-        const uint32_t code = __float_as_uint(m.y);
-        if ((code & ~kIdentityBit) == i) {
-          if (code == i && dm2 < best) {
-            best = dm2;
-            if (TRACK) best_at = (int)(base + t);
-          }
-          continue;
+      float2 sw = splat(0.f), sx = splat(0.f), sy = splat(0.f), sz = splat(0.f), sc = splat(0.f), se = splat(0.f);
+      const int pairs = (count + 1) >> 1;
+      for (int u = 0; u < pairs; ++u) {
+        const float4 A = T.wx[u], B = T.yz[u];
+        const float2 mw = fma2(make_float2(A.x, A.y), splat(-1.0f), xw);
+        const float2 mx = fma2(make_float2(A.z, A.w), splat(-1.0f), xx);
+        const float2 my = fma2(make_float2(B.x, B.y), splat(-1.0f), xy);
+        const float2 mz = fma2(make_float2(B.z, B.w), splat(-1.0f), xz);
+        const float2 dm2 = fma2(mw, mw, fma2(mx, mx, fma2(my, my, mul2(mz, mz))));
+        if (dm2.x > cut2 && dm2.y > cut2) continue;
+        const float4 M = T.nc[u];
+        const uint32_t c0 = __float_as_uint(M.z), c1 = __float_as_uint(M.w);
+        const bool own0 = ((c0 ^ i) & ~kIdentityBit) == 0, own1 = ((c1 ^ i) & ~kIdentityBit) == 0;
+        const bool own = own0 || own1;
+        float n0 = dm2.x, n1 = dm2.y;
+        if (own) {  // the thread's own source: no force; its identity image is no neighbour
+          if (own0 && c0 != i) n0 = 4.0f;
+          if (own1 && c1 != i) n1 = 4.0f;
         }
         if (TRACK) {
-          if (dm2 < best) {
-            best = dm2;
-            best_at = (int)(base + t);
+          if (n0 < best) {
+            best = n0;
+            best_at = (int)(base + 2 * u);
+          }
+          if (n1 < best) {
+            best = n1;
+            best_at = (int)(base + 2 * u + 1);
           }
         } else {
-          best = fminf(best, dm2);
+          best = fminf(best, fminf(n0, n1));
         }
-        float c, cv, e;
-        near_pair32<SHORT>(dm2, nx2 + m.x - dm2, cz, cw, c, cv, e);
-        sw = fmaf(c, mw, sw);
-        sx = fmaf(c, mx, sx);
-        sy = fmaf(c, my, sy);
-        sz = fmaf(c, mz, sz);
-        sc += cv;
-        se += e;
+        const float2 dp2 = fma2(dm2, splat(-1.0f), add2(xn, make_float2(M.x, M.y)));
+        Pair2 pr = near_pair32x2<SHORT>(dm2, dp2, cw, czw);
+        if (own) {
+          const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
+          pr.coef = mul2(pr.coef, keep);
+          pr.curv = mul2(pr.curv, keep);
+          pr.energy = mul2(pr.energy, keep);
+        }
+        sw = fma2(pr.coef, mw, sw);
+        sx = fma2(pr.coef, mx, sx);
+        sy = fma2(pr.coef, my, sy);
+        sz = fma2(pr.coef, mz, sz);
+        sc = add2(sc, pr.curv);
+        se = add2(se, pr.energy);
       }
-      yw += sw;
-      yx += sx;
-      yy += sy;
-      yz += sz;
-      fc += sc;
-      fe += se;
+      sums[0][threadIdx.x] += (double)sw.x + (double)sw.y;
+      sums[1][threadIdx.x] += (double)sx.x + (double)sx.y;
+      sums[2][threadIdx.x] += (double)sy.x + (double)sy.y;
+      sums[3][threadIdx.x] += (double)sz.x + (double)sz.y;
+      sums[4][threadIdx.x] += (double)sc.x + (double)sc.y;
+      sums[5][threadIdx.x] += (double)se.x + (double)se.y;
     }
   }
   if (!live) return;
-  const double3 f = force_from_differences(to_d4(x), make_double4(yw, yx, yy, yz));
+  if (best > cut2) {  // no site within the cutoff
+    best = 4.0f;
+    best_at = -1;
+  }
+  const double3 f = force_from_differences(
+      to_d4(x), make_double4(sums[0][threadIdx.x], sums[1][threadIdx.x], sums[2][threadIdx.x], sums[3][threadIdx.x]));
   const size_t at = (size_t)slice * stride + p;
-  out.force[at] = make_double4(f.x, f.y, f.z, fc);
-  out.energy[at] = fe;
+  out.force[at] = make_double4(f.x, f.y, f.z, sums[4][threadIdx.x]);
+  out.energy[at] = sums[5][threadIdx.x];
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;
 }

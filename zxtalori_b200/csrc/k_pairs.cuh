@@ -200,79 +200,124 @@ __device__ __forceinline__ PairTile pair_tile(int tile, int jtiles, int n) {
 // FP32 rows (the relaxation's force pass, quey_partial semantics, shaders/pairs.wgsl:266-308):
 // force and energy over every image of every other source; nearest over every image
 // but the identity self pair. TRACK keeps the first image index of the nearest chord.
-template <bool TRACK, bool CHECK>
-__device__ __forceinline__ void pairs32_tile(const float4 x, const float4* tile, int count, int i, int j0, int k, int n,
-                                             float& sw, float& sx, float& sy, float& sz, float& sc, float& se,
-                                             float& best, int& best_at) {
+//
+// A block holds 128 sources, one per thread, and walks tiles of 128 images of one operator
+// built in shared memory; each thread evaluates two images per iteration with packed FP32
+// arithmetic. The tile stores the images as pairs, component by component (w, w', x, x')
+// and (y, y', z, z'), plus 2|y|^2 of each, so one broadcast load gives a component of both.
+// The near twin of an image is chosen by the sign of x . y; its difference d = x - y~
+// gives the near chord |d|^2 directly and the far chord by the parallelogram law
+// (2|x|^2 + 2|y|^2 - |d|^2 >= 2, no cancellation), and the force sum is
+// sum coef (x - y~), turned into the tangent force once per source.
+struct PairSlots {
+  float4 wx[kPairBlock / 2];
+  float4 yz[kPairBlock / 2];
+  float2 n2[kPairBlock / 2];
+};
+
+// MASKED: the tile holds the thread's own source or ends in half a slot.
+template <bool TRACK, bool MASKED>
+__device__ __forceinline__ void pairs32_tile(const float4 x, float nx2, const PairSlots& S, int count, int i, int j0,
+                                             int k, int n, float2& sw, float2& sx, float2& sy, float2& sz, float2& sc,
+                                             float2& se, float& best, int& best_at) {
+  const float2 xw = splat(x.x), xx = splat(x.y), xy = splat(x.z), xz = splat(x.w), xn = splat(nx2);
+  const int slots = (count + 1) >> 1;
 #pragma unroll 2
-  for (int t = 0; t < count; ++t) {
-    const float4 y = tile[t];
-    const float mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
-    const float pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
-    const float dm2 = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
-    const float dp2 = fmaf(pw, pw, fmaf(px, px, fmaf(py, py, pz * pz)));
-    const float c = fminf(dm2, dp2);
-    const bool own = CHECK && (j0 + t == i);
-    if (!(own && k == 0)) {
-      if (TRACK) {
-        if (c < best) {
-          best = c;
-          best_at = k * n + j0 + t;
-        }
-      } else {
-        best = fminf(best, c);
-      }
+  for (int u = 0; u < slots; ++u) {
+    const float4 A = S.wx[u], B = S.yz[u];
+    const float2 yw = make_float2(A.x, A.y), yx = make_float2(A.z, A.w);
+    const float2 yy = make_float2(B.x, B.y), yz = make_float2(B.z, B.w);
+    const float2 dot = fma2(xw, yw, fma2(xx, yx, fma2(xy, yy, mul2(xz, yz))));
+    const float2 ms = make_float2(dot.x >= 0.f ? -1.f : 1.f, dot.y >= 0.f ? -1.f : 1.f);
+    const float2 dw = fma2(ms, yw, xw), dx = fma2(ms, yx, xx), dy = fma2(ms, yy, xy), dz = fma2(ms, yz, xz);
+    const float2 nearv = fma2(dw, dw, fma2(dx, dx, fma2(dy, dy, mul2(dz, dz))));
+    const float2 farv = fma2(nearv, splat(-1.0f), add2(xn, S.n2[u]));
+    float2 keep = splat(1.0f);  // force and energy weight of each pair
+    float n0 = nearv.x, n1 = nearv.y;
+    if (MASKED) {
+      const int j = j0 + 2 * u;
+      const bool own0 = j == i, own1 = j + 1 == i, pad1 = 2 * u + 1 >= count;
+      if (own0 && k == 0) n0 = 4.0f;
+      if ((own1 && k == 0) || pad1) n1 = 4.0f;
+      keep = make_float2(own0 ? 0.f : 1.f, (own1 || pad1) ? 0.f : 1.f);
     }
-    if (own) continue;
-    const PairF p = quey_pair32(dm2, dp2);
-    // dir(y) = -dir(x - y) = dir(x + y): accumulate the near twin's short difference,
-    // c (x - y) or -c (x + y), turned into -dir(sum) per source (force_from_differences).
-    const bool minus = dm2 <= dp2;
-    const float cs = minus ? p.coef : -p.coef;
-    sw = fmaf(cs, minus ? mw : pw, sw);
-    sx = fmaf(cs, minus ? mx : px, sx);
-    sy = fmaf(cs, minus ? my : py, sy);
-    sz = fmaf(cs, minus ? mz : pz, sz);
-    sc += p.curv;
-    se += p.energy;
+    if (TRACK) {
+      if (n0 < best) {
+        best = n0;
+        best_at = k * n + j0 + 2 * u;
+      }
+      if (n1 < best) {
+        best = n1;
+        best_at = k * n + j0 + 2 * u + 1;
+      }
+    } else {
+      best = fminf(best, fminf(n0, n1));
+    }
+    Pair2 p = quey_pair32x2(max2(nearv, 1e-30f), farv);
+    if (MASKED) {
+      p.coef = mul2(p.coef, keep);
+      p.curv = mul2(p.curv, keep);
+      p.energy = mul2(p.energy, keep);
+    }
+    sw = fma2(p.coef, dw, sw);
+    sx = fma2(p.coef, dx, sx);
+    sy = fma2(p.coef, dy, sy);
+    sz = fma2(p.coef, dz, sz);
+    sc = add2(sc, p.curv);
+    se = add2(se, p.energy);
   }
 }
 
 template <bool TRACK>
-__global__ void __launch_bounds__(kPairBlock) k_pairs32(const float4* __restrict__ q, int n, int op_off, int jtiles,
-                                                        int total_tiles, int tiles_per_chunk, Rows out, int stride) {
-  __shared__ float4 tile[kPairBlock];
+__global__ void __launch_bounds__(kPairBlock, 8) k_pairs32(const float4* __restrict__ q, int n, int op_off, int jtiles,
+                                                           int total_tiles, int tiles_per_chunk, Rows out, int stride) {
+  __shared__ PairSlots S;
+  __shared__ double sums[6][kPairBlock];  // FP64 row sums (shared: registers go to the pairs)
   const int i0 = blockIdx.x * kPairBlock;
   const int i = i0 + threadIdx.x;
   const bool live = i < n;
   const float4 x = live ? q[i] : make_float4(1.f, 0.f, 0.f, 0.f);
-  double yw = 0, yx = 0, yy = 0, yz = 0, fc = 0, fe = 0;
+  const float nx2 = 2.0f * fmaf(x.x, x.x, fmaf(x.y, x.y, fmaf(x.z, x.z, x.w * x.w)));
+  for (int k = 0; k < 6; ++k) sums[k][threadIdx.x] = 0.0;
   float best = 4.0f;
   int best_at = -1;
   const int t0 = blockIdx.y * tiles_per_chunk, t1 = min(total_tiles, t0 + tiles_per_chunk);
+  const int slot = threadIdx.x >> 1, half = threadIdx.x & 1;
   for (int tid = t0; tid < t1; ++tid) {
     const PairTile pt = pair_tile(tid, jtiles, n);
     __syncthreads();
-    if ((int)threadIdx.x < pt.count) tile[threadIdx.x] = image32(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0);
+    {
+      const float4 y = (int)threadIdx.x < pt.count ? image32(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0)
+                                                   : make_float4(1.f, 0.f, 0.f, 0.f);
+      float* wx = reinterpret_cast<float*>(&S.wx[slot]);
+      float* yz = reinterpret_cast<float*>(&S.yz[slot]);
+      wx[half] = y.x;
+      wx[2 + half] = y.y;
+      yz[half] = y.z;
+      yz[2 + half] = y.w;
+      reinterpret_cast<float*>(&S.n2[slot])[half] = 2.0f * fmaf(y.x, y.x, fmaf(y.y, y.y, fmaf(y.z, y.z, y.w * y.w)));
+    }
     __syncthreads();
     if (!live) continue;
-    float sw = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, sc = 0.f, se = 0.f;
-    if (pt.j0 < i0 + kPairBlock && i0 < pt.j0 + pt.count)
-      pairs32_tile<TRACK, true>(x, tile, pt.count, i, pt.j0, pt.k, n, sw, sx, sy, sz, sc, se, best, best_at);
+    float2 sw = splat(0.f), sx = splat(0.f), sy = splat(0.f), sz = splat(0.f), sc = splat(0.f), se = splat(0.f);
+    const bool masked = (pt.j0 < i0 + kPairBlock && i0 < pt.j0 + pt.count) || (pt.count & 1);
+    if (masked)
+      pairs32_tile<TRACK, true>(x, nx2, S, pt.count, i, pt.j0, pt.k, n, sw, sx, sy, sz, sc, se, best, best_at);
     else
-      pairs32_tile<TRACK, false>(x, tile, pt.count, i, pt.j0, pt.k, n, sw, sx, sy, sz, sc, se, best, best_at);
-    yw += sw;
-    yx += sx;
-    yy += sy;
-    yz += sz;
-    fc += sc;
-    fe += se;
+      pairs32_tile<TRACK, false>(x, nx2, S, pt.count, i, pt.j0, pt.k, n, sw, sx, sy, sz, sc, se, best, best_at);
+    sums[0][threadIdx.x] += (double)sw.x + (double)sw.y;
+    sums[1][threadIdx.x] += (double)sx.x + (double)sx.y;
+    sums[2][threadIdx.x] += (double)sy.x + (double)sy.y;
+    sums[3][threadIdx.x] += (double)sz.x + (double)sz.y;
+    sums[4][threadIdx.x] += (double)sc.x + (double)sc.y;
+    sums[5][threadIdx.x] += (double)se.x + (double)se.y;
   }
   if (!live) return;
   const size_t at = (size_t)blockIdx.y * stride + i;
-  const double3 f = force_from_differences(to_d4(x), make_double4(yw, yx, yy, yz));
-  out.force[at] = make_double4(f.x, f.y, f.z, fc);
-  out.energy[at] = fe;
+  const double3 f = force_from_differences(
+      to_d4(x), make_double4(sums[0][threadIdx.x], sums[1][threadIdx.x], sums[2][threadIdx.x], sums[3][threadIdx.x]));
+  out.force[at] = make_double4(f.x, f.y, f.z, sums[4][threadIdx.x]);
+  out.energy[at] = sums[5][threadIdx.x];
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;
 }

@@ -64,41 +64,54 @@ cudaError_t launch_refine_nearest(const float4* q32, int n, int gid, Rows rows, 
 
 // FP32 FMA throughput probe: 8 independent FMA chains per thread (latency hidden by ILP and
 // occupancy), the result stored so nothing is eliminated. 16 flops per thread per iteration.
+// PACKED: the chains are float2 pairs advanced by one f32x2 FMA each (32 flops per thread
+// per iteration), to see whether packed FMAs raise the FP32 rate or only save issue slots.
+template <bool PACKED>
 __global__ void __launch_bounds__(256) k_fma_probe(float* out, int iterations, float seed) {
-  float a[8];
+  float2 a[8];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) a[c] = seed + (float)(threadIdx.x + c);
+  for (int c = 0; c < 8; ++c) a[c] = make_float2(seed + (float)(threadIdx.x + c), seed - (float)c);
   const float m = 0.999999f, b = 1e-7f;
   for (int it = 0; it < iterations; ++it) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) a[c] = fmaf(a[c], m, b);
+    for (int c = 0; c < 8; ++c) {
+      if (PACKED) a[c] = fma2(a[c], splat(m), splat(b));
+      else a[c].x = fmaf(a[c].x, m, b);
+    }
   }
   float s = 0.f;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) s += a[c];
+  for (int c = 0; c < 8; ++c) s += a[c].x + (PACKED ? a[c].y : 0.f);
   if (s == 12345.678f) out[blockIdx.x] = s;
 }
 
-cudaError_t measure_fp32_peak(int sms, double* tflops) {
-  float* out = nullptr;
-  cudaError_t e = cudaMalloc(&out, sizeof(float) * sms * 64);
-  if (e) return e;
+template <bool PACKED>
+static cudaError_t time_fma_probe(int sms, float* out, double* tflops) {
   const int blocks = sms * 8, iterations = 1 << 16;
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
-  k_fma_probe<<<blocks, 256>>>(out, 1024, 1.0f);
+  k_fma_probe<PACKED><<<blocks, 256>>>(out, 1024, 1.0f);
   cudaEventRecord(a);
-  for (int r = 0; r < 4; ++r) k_fma_probe<<<blocks, 256>>>(out, iterations, 1.0f + r);
+  for (int r = 0; r < 4; ++r) k_fma_probe<PACKED><<<blocks, 256>>>(out, iterations, 1.0f + r);
   cudaEventRecord(b);
   cudaEventSynchronize(b);
   float ms = 0;
   cudaEventElapsedTime(&ms, a, b);
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  cudaFree(out);
-  *tflops = 4.0 * blocks * 256.0 * iterations * 16.0 / (ms * 1e-3) / 1e12;
+  *tflops = 4.0 * blocks * 256.0 * iterations * (PACKED ? 32.0 : 16.0) / (ms * 1e-3) / 1e12;
   return cudaGetLastError();
+}
+
+cudaError_t measure_fp32_peak(int sms, double* tflops, double* packed_tflops) {
+  float* out = nullptr;
+  cudaError_t e = cudaMalloc(&out, sizeof(float) * sms * 64);
+  if (e) return e;
+  e = time_fma_probe<false>(sms, out, tflops);
+  if (!e && packed_tflops) e = time_fma_probe<true>(sms, out, packed_tflops);
+  cudaFree(out);
+  return e;
 }
 
 cudaError_t launch_neighbour_index(Rows rows, int n, bool near_sites, const uint32_t* scode, int* neighbour,

@@ -89,7 +89,7 @@ cudaError_t launch_neighbour_index(Rows rows, int n, bool near_sites, const uint
                                    cudaStream_t s);
 
 // Measured FP32 FMA throughput of the current device (TFLOP/s, 2 flops per FMA).
-cudaError_t measure_fp32_peak(int sms, double* tflops);
+cudaError_t measure_fp32_peak(int sms, double* tflops, double* packed_tflops);
 
 // Blocks used by the row-summary and stats reductions for n rows.
 inline int reduce_blocks(int n) { return (n + 255) / 256; }

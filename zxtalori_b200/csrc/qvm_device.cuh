@@ -135,6 +135,100 @@ __device__ __forceinline__ PairF quey_pair32(float dm2, float dp2) {
   return p;
 }
 
+// ------------------------------------------------------------------ packed FP32 (two pairs)
+// sm_100 f32x2 arithmetic: one instruction does the same add, multiply or fused
+// multiply-add on two lanes of a float2, each rounded exactly as its scalar counterpart.
+// The hot loops evaluate two pairs per thread this way, halving their issue slots.
+__device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
+__device__ __forceinline__ float2 sqrt2(float2 a) { return make_float2(sqrt_approx(a.x), sqrt_approx(a.y)); }
+__device__ __forceinline__ float2 max2(float2 a, float b) { return make_float2(fmaxf(a.x, b), fmaxf(a.y, b)); }
+
+__device__ __forceinline__ float2 two_atan_unit2(float2 t, float2 t2) {
+  float2 p = splat(0x1.758a10p-8f);
+  p = fma2(p, t2, splat(-0x1.07448cp-5f));
+  p = fma2(p, t2, splat(0x1.5dba7cp-4f));
+  p = fma2(p, t2, splat(-0x1.336030p-3f));
+  p = fma2(p, t2, splat(0x1.b3da44p-3f));
+  p = fma2(p, t2, splat(-0x1.22e400p-2f));
+  p = fma2(p, t2, splat(0x1.9972e8p-2f));
+  p = fma2(p, t2, splat(-0x1.5554a6p-1f));
+  p = fma2(p, t2, splat(2.0f));
+  return mul2(t, p);
+}
+__device__ __forceinline__ float2 two_atan_short2(float2 t, float2 t2) {
+  float2 p = splat(-0x1.117a86p-2f);
+  p = fma2(p, t2, splat(0x1.991528p-2f));
+  p = fma2(p, t2, splat(-0x1.5554c2p-1f));
+  p = fma2(p, t2, splat(2.0f));
+  return mul2(t, p);
+}
+
+// Two Quey pairs given near = |x - y~|^2 (clamped to >= 1e-30) and far = |x + y~|^2 of
+// each, y~ the near twin: the coefficient of (x - y~) in the force sum (minus the force
+// magnitude over sin a; sign included), curvature and energy. The arithmetic of
+// quey_pair32 lane by lane.
+struct Pair2 {
+  float2 coef, curv, energy;
+};
+__device__ __forceinline__ Pair2 quey_pair32x2(float2 nearv, float2 farv) {
+  const float2 t2 = mul2(nearv, rcp2(farv));
+  const float2 t = sqrt2(t2);
+  const float2 a = max2(two_atan_unit2(t, t2), 1e-12f);
+  const float2 b = fma2(a, splat(-1.0f), splat(kPiF));
+  const float2 aa = mul2(a, a), bb = mul2(b, b);
+  const float2 a2 = add2(aa, splat(1e-9f)), b2 = add2(bb, splat(1e-9f));
+  const float2 a3 = fma2(aa, a, splat(1e-9f)), b3 = fma2(bb, b, splat(1e-9f));
+  const float2 onept2 = add2(t2, splat(1.0f));
+  const float2 sp = fma2(splat(1e-9f), onept2, add2(t, t));  // (sine + 1e-9) (1 + t^2)
+  const float2 a2b2 = mul2(a2, b2);
+  const float2 r1 = rcp2(mul2(a2b2, sp));
+  const float2 ab = mul2(a, b);
+  const float2 a3b3 = mul2(a3, b3);
+  const float2 r2 = rcp2(mul2(a3b3, ab));
+  Pair2 p;
+  p.coef = mul2(mul2(fma2(b2, splat(-1.0f), a2), onept2), r1);  // -(b2 - a2)(1 + t^2) / (a2 b2 sp)
+  p.curv = mul2(mul2(add2(a3, b3), ab), r2);
+  p.energy = mul2(mul2(splat(kPiF), a3b3), r2);
+  return p;
+}
+
+// near_pair32 (below) on two sites at once: dm2 and dp2 of each, the window's start cz and
+// inverse width cw, and czw = cz * cw. Beyond the cutoff the window is exactly zero, so
+// such a site contributes nothing (coefficient, curvature and energy all 0).
+template <bool SHORT>
+__device__ __forceinline__ Pair2 near_pair32x2(float2 dm2, float2 dp2, float cw, float czw) {
+  const float2 t2 = mul2(max2(dm2, 1e-30f), rcp2(dp2));
+  const float2 t = sqrt2(t2);
+  const float2 a = max2(SHORT ? two_atan_short2(t, t2) : two_atan_unit2(t, t2), 1e-12f);
+  const float2 b = fma2(a, splat(-1.0f), splat(kPiF));
+  const float2 aa = mul2(a, a), bb = mul2(b, b);
+  const float2 a2 = add2(aa, splat(1e-9f)), b2 = add2(bb, splat(1e-9f));
+  const float2 a3 = fma2(aa, a, splat(1e-9f)), b3 = fma2(bb, b, splat(1e-9f));
+  const float2 onept2 = add2(t2, splat(1.0f));
+  const float2 sp = fma2(splat(1e-9f), onept2, add2(t, t));
+  const float2 a2b2 = mul2(a2, b2);
+  const float2 r1 = rcp2(mul2(a2b2, sp));
+  const float2 ab = mul2(a, b);
+  const float2 a3b3 = mul2(a3, b3);
+  const float2 r2 = rcp2(mul2(a3b3, ab));
+  const float2 e = mul2(mul2(splat(kPiF), a3b3), r2);
+  const float2 sr = fma2(a, splat(cw), splat(-czw));
+  const float2 s = make_float2(__saturatef(sr.x), __saturatef(sr.y));
+  const float2 w = fma2(mul2(s, s), fma2(s, splat(2.0f), splat(-3.0f)), splat(1.0f));  // 1 - s^2 (3 - 2s)
+  const float2 slope = mul2(mul2(s, fma2(s, splat(-1.0f), splat(1.0f))), splat(-6.0f * cw));
+  const float2 nalong = mul2(mul2(fma2(b2, splat(-1.0f), a2), onept2), r1);  // -along
+  const float2 inv_sine = mul2(mul2(onept2, a2b2), r1);
+  Pair2 p;
+  p.coef = fma2(w, nalong, mul2(mul2(e, slope), inv_sine));
+  p.curv = mul2(mul2(mul2(add2(a3, b3), ab), r2), w);
+  p.energy = mul2(e, w);
+  return p;
+}
+
 // Windowed near-field pair, FP32, for a site that is the near twin (dm2 <= cut < 2 <= dp2,
 // so the sign is +1, near = dm2 and far = dp2): the coefficient c of the pair's direction
 // (force contribution c * dir), its windowed curvature and energy. Same arithmetic as
