@@ -144,6 +144,8 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   // Warp tasks (32 sources x one slice of their cell rows): several waves of resident warps.
   const int warps = (n + 31) / 32;
   slices_ = std::max(1, std::min(64, (sms * 48 + warps - 1) / warps));
+  const int warps32 = (n + kNearGroup - 1) / kNearGroup;
+  slices32_ = std::max(1, std::min(slices_, (sms * 48 + warps32 - 1) / warps32));
   partial_.ensure((size_t)slices_ * n);
   ZO_CUDA(cudaStreamSynchronize(s));
   ready_ = true;
@@ -165,6 +167,7 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
   L.capacity = capacity_;
   L.sdim_max = sdim_max_;
   L.slices = slices_;
+  L.slices32 = slices32_;
   L.track = track;
   L.short_atan = radius_ <= 0.4;
   L.s_margin = s_margin_;

@@ -8,11 +8,12 @@
 //      counted, scanned and written in (source, image) order - deterministic sites;
 //   2. the sites' stereographic chart box, a grid of sdim^3 cells, a counting sort of the
 //      sites into row-major cells with each cell ordered by site index;
-//   3. sources counting-sorted along a Hilbert curve of a 64^3 grid (then by index), so 32
+//   3. sources counting-sorted along a Hilbert curve of a 64^3 grid (then by index), so
 //      consecutive sources are close together;
-//   4. one warp per 32 sources and slice: the warp's chart box, the cell rows within the
-//      chart reach of the cutoff chord, each row's x-run trimmed; runs stream through shared
-//      memory 32 sites at a time and every lane tests its source against each site;
+//   4. one warp per kNearGroup sources (FP32; 32 in FP64) and slice: the warp's chart box,
+//      the cell rows within the chart reach of the cutoff chord, each row's x-run trimmed;
+//      runs stream through shared memory 32 sites at a time and the lanes test their
+//      sources against each site;
 //   5. the slices' partial rows summed in slice order into each source's row.
 // Nothing is read back between passes: grid parameters live in device memory.
 #pragma once
@@ -149,7 +150,8 @@ __global__ void __launch_bounds__(256) k_shell_write(const float4* __restrict__ 
 // ------------------------------------------------------------------ 2. grid and site sort
 // Chart grid from the box (near.zig:124-137): a 5% margin, width 1.1x the largest extent,
 // sdim = clamp(round(cbrt(sites/kSitesPerCell)), 1, sdim_max). The reference aims at 8 sites
-// per cell; 3 trims the candidate runs closer to the cutoff ball (rows are cheap on B200).
+// per cell; fewer trims the candidate runs closer to the cutoff ball (the FP32 gather
+// concatenates runs, so short rows cost nothing extra).
 // The box is reset for the next pass.
 __global__ void k_grid_setup(NearGrid* g, const uint32_t* __restrict__ total, int capacity, int sdim_max,
                              int* __restrict__ cells) {
@@ -290,7 +292,16 @@ __global__ void k_source_count(const float4* __restrict__ q32, const double4* __
 // ------------------------------------------------------------------ 4. the gather
 struct NearCut {
   double cut2, chord, cut_z, cut_w;
+  // Squared chord at angle 1.25 r, where the window is exactly zero: the packed gather
+  // evaluates an out-of-cutoff site with its chord clamped to this (finite terms, zero
+  // contribution) when the other site of its pair is within the cutoff.
+  double cut_hi;
 };
+inline NearCut near_cut(double cut2, double chord, double cut_z, double cut_w) {
+  const double r = cut_z + 1.0 / cut_w;
+  const double s = 2.0 * std::sin(0.5 * std::min(1.25 * r, 1.5));
+  return NearCut{cut2, chord, cut_z, cut_w, s * s};
+}
 
 constexpr int kNearWarps = 4;
 
@@ -358,12 +369,40 @@ __device__ __forceinline__ bool row_run(const WarpBox& b, const NearGrid& g, con
   return start < end;
 }
 
+// The gather (pairs.wgsl:363-416). A warp holds kNearGroup sources (consecutive along the
+// Hilbert order), each on kNearSub = 32 / kNearGroup lanes that split its sites between
+// them. The warp walks the cell rows within reach of its sources' chart box 32 rows at a
+// time, one lane per row finding the row's run of sorted sites; the runs are concatenated
+// and streamed through shared memory in tiles of kNearTile sites, and every lane evaluates
+// its source against kNearTile / kNearSub sites of each tile, two per instruction with
+// packed FP32 arithmetic. For a site within the cutoff chord the windowed pair runs with
+// dp2 = 2(|x|^2+|y|^2) - dm2 (parallelogram law; the site is the near twin); sites beyond it
+// contribute exactly zero through the window, and the nearest chord is taken over every
+// site and reset to 4 when it exceeds the cutoff (no site within it), which is the same as
+// testing each site. The force is kept as sum c (x - y), turned into a force once per
+// source. Lane sums are FP32 over 32 sites, then FP64; the lanes of a source are added in
+// lane order at the end.
+constexpr int kNearSub = 32 / kNearGroup;          // lanes per source
+constexpr int kNearTile = 128;                      // sites per tile
+constexpr int kNearSlots = kNearTile / (2 * kNearSub);  // site pairs per lane and tile
+constexpr int kNearMerge = 16 / kNearSlots;          // tiles between FP64 merges (16 pairs)
+
+// One tile. Slot u holds elements 2u and 2u + 1; lane (source s, sub-lane j) evaluates
+// slots j + kNearSub m, m < kNearSlots.
+struct NearTile {
+  float4 wx[kNearTile / 2];  // (w, w', x, x')
+  float4 yz[kNearTile / 2];  // (y, y', z, z')
+  float4 nc[kNearTile / 2];  // (2|y|^2, 2|y'|^2, code bits, code' bits)
+  uint32_t at[kNearTile];    // sorted-site index of each element
+};
+
 // Per-warp data of the row walk, kept in shared memory (it is warp-uniform) so the hot
 // loop's registers go to the pair arithmetic.
 struct NearWalk {
   WarpBox box;
   float lower[3], cells_per_unit;
   int sdim;
+  uint2 runs[32];  // a batch's nonempty row runs (start, length), compacted
 };
 
 // row_run from the warp's shared walk data.
@@ -387,40 +426,38 @@ __device__ __forceinline__ bool walk_row(const NearWalk& W, const uint32_t* cell
   return start < end;
 }
 
-// The gather (pairs.wgsl:363-416). Each lane holds one source; the warp streams its
-// cell-row runs through shared memory 32 sites at a time and every lane tests its source
-// against each site, two sites per iteration with packed FP32 arithmetic: the tile holds
-// the sites as pairs, component by component, with 2|y|^2 and the code of each. For a site
-// within the cutoff chord the windowed pair runs with dp2 = 2(|x|^2+|y|^2) - dm2
-// (parallelogram law; the site is the near twin); sites beyond it contribute exactly zero
-// through the window, and the nearest chord is taken over every site and reset to 4 when
-// it exceeds the cutoff (no site within it), which is the same as testing each site. The
-// force is kept as sum c (x - y), turned into a force once per source. Tile sums are FP32,
-// merged into FP64 per tile.
-struct NearSlots {
-  float4 wx[16];  // (w, w', x, x') of sites 2u and 2u+1
-  float4 yz[16];  // (y, y', z, z')
-  float4 nc[16];  // (2|y|^2, 2|y'|^2, code bits, code' bits)
-};
+// Adds a lane's FP32 sums into its FP64 sums in shared memory and clears them.
+__device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], float2& sw, float2& sx, float2& sy,
+                                           float2& sz, float2& sc, float2& se) {
+  sums[0][threadIdx.x] += (double)sw.x + (double)sw.y;
+  sums[1][threadIdx.x] += (double)sx.x + (double)sx.y;
+  sums[2][threadIdx.x] += (double)sy.x + (double)sy.y;
+  sums[3][threadIdx.x] += (double)sz.x + (double)sz.y;
+  sums[4][threadIdx.x] += (double)sc.x + (double)sc.y;
+  sums[5][threadIdx.x] += (double)se.x + (double)se.y;
+  sw = sx = sy = sz = sc = se = splat(0.f);
+}
 
 template <bool TRACK, bool SHORT>
-__global__ void __launch_bounds__(kNearWarps * 32, 8) k_near32(const float4* __restrict__ q, int n,
+__global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __restrict__ q, int n,
                                                               const uint32_t* __restrict__ src_perm,
                                                               const float4* __restrict__ sq,
                                                               const uint32_t* __restrict__ scode,
                                                               const uint32_t* __restrict__ cell_off,
                                                               const NearGrid* __restrict__ gp, NearCut cut, int slices,
                                                               Rows out, int stride) {
-  __shared__ NearSlots tiles[kNearWarps];
+  __shared__ NearTile tiles[kNearWarps];
   __shared__ NearWalk walks[kNearWarps];
-  __shared__ double sums[6][kNearWarps * 32];  // FP64 row sums: force differences, curvature, energy
+  __shared__ double sums[6][kNearWarps * 32];  // FP64 lane sums: force differences, curvature, energy
+  const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  NearSlots& T = tiles[w];
+  NearTile& T = tiles[w];
   NearWalk& W = walks[w];
   const int warp = blockIdx.x * kNearWarps + w;
   const int slice = blockIdx.y;
-  if (warp * 32 >= n) return;
-  const int p = warp * 32 + lane;
+  if (warp * kNearGroup >= n) return;
+  const int sub = lane % kNearSub;
+  const int p = warp * kNearGroup + lane / kNearSub;
   const bool live = p < n;
   const uint32_t i = live ? src_perm[p] : 0u;
   const float4 x = q[i];
@@ -437,105 +474,183 @@ __global__ void __launch_bounds__(kNearWarps * 32, 8) k_near32(const float4* __r
   }
   for (int k = 0; k < 6; ++k) sums[k][threadIdx.x] = 0.0;
   __syncwarp();
-  const float cut2 = (float)cut.cut2, cw = (float)cut.cut_w, czw = (float)(cut.cut_z * cut.cut_w);
+  const float cut2 = (float)cut.cut2, cut_hi = (float)cut.cut_hi, cw = (float)cut.cut_w,
+              czw = (float)(cut.cut_z * cut.cut_w);
   const float nx2 = 2.0f * fmaf(x.x, x.x, fmaf(x.y, x.y, fmaf(x.z, x.z, x.w * x.w)));
   const float2 xw = splat(x.x), xx = splat(x.y), xy = splat(x.z), xz = splat(x.w), xn = splat(nx2);
   float best = 4.0f;
   int best_at = -1;
+  float2 sw = splat(0.f), sx = splat(0.f), sy = splat(0.f), sz = splat(0.f), sc = splat(0.f), se = splat(0.f);
+  int since = 0;  // tiles since the last FP64 merge
   const int rows = (W.box.chi[1] - W.box.clo[1] + 1) * (W.box.chi[2] - W.box.clo[2] + 1);
-  const int slot = lane >> 1, half = lane & 1;
-  for (int r = slice; r < rows; r += slices) {
-    uint32_t start, end;
-    if (!walk_row(W, cell_off, r, start, end)) continue;
-    for (uint32_t base = start; base < end; base += 32) {
-      const int count = (int)min(32u, end - base);
+  const int mine = rows > slice ? (rows - slice + slices - 1) / slices : 0;  // rows slice, slice+slices, ...
+  for (int rb = 0; rb < mine; rb += 32) {
+    uint32_t start = 0, len = 0;
+    if (rb + lane < mine) {
+      uint32_t a, b;
+      if (walk_row(W, cell_off, slice + (rb + lane) * slices, a, b)) {
+        start = a;
+        len = b - a;
+      }
+    }
+    // Compact the nonempty runs to the first lanes (in row order), so every row boundary
+    // the tiles cross is a real one.
+    const unsigned nonempty = __ballot_sync(full, len > 0);
+    __syncwarp();
+    if (len > 0) W.runs[__popc(nonempty & ((1u << lane) - 1u))] = make_uint2(start, len);
+    __syncwarp();
+    const int nr = __popc(nonempty);
+    start = 0;
+    len = 0;
+    if (lane < nr) {
+      const uint2 run = W.runs[lane];
+      start = run.x;
+      len = run.y;
+    }
+    uint32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(full, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(full, incl, 31);
+    const uint32_t shift = start - (incl - len);  // element e of run k is site shift_k + e
+    int k = 0;  // the run of this lane's next element: the first lane with incl > e
+    for (uint32_t tb = 0; tb < total; tb += kNearTile) {
+      const int count = (int)min((uint32_t)kNearTile, total - tb);
       __syncwarp();
-      {
-        // A lane past the run's end writes a blank site: at the origin, dm2 = |x|^2 ~ 1 lies
-        // beyond every cutoff of the chart-grid path (r < 0.5 rad, cut2 < 0.25), and its
-        // code matches no source.
-        float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
-        uint32_t code = 0xffffffffu;
-        if (lane < count) {
-          s = sq[base + lane];
-          code = scode[base + lane];
+#pragma unroll
+      for (int h = 0; h < kNearTile / 64; ++h) {
+        // Lane l loads elements 64h + 2l and 64h + 2l + 1 (slot 32h + l) and writes the slot
+        // whole. An element past the batch's end is a blank site: at the origin,
+        // dm2 = |x|^2 ~ 1 lies beyond every cutoff of the chart-grid path (r < 0.5 rad,
+        // cut2 < 0.25), and its code matches no source.
+        const int el = 64 * h + 2 * lane;
+        const uint32_t e = tb + el;
+        uint32_t kin;
+        // Warp-uniform advance; it ends: each pass moves some lane's k, and k stops at 31.
+        for (;;) {
+          kin = __shfl_sync(full, incl, k);
+          const bool advance = k < 31 && kin <= e;
+          if (!__any_sync(full, advance)) break;
+          if (advance) ++k;
         }
-        float* a = reinterpret_cast<float*>(&T.wx[slot]);
-        float* b = reinterpret_cast<float*>(&T.yz[slot]);
-        float* c = reinterpret_cast<float*>(&T.nc[slot]);
-        a[half] = s.x;
-        a[2 + half] = s.y;
-        b[half] = s.z;
-        b[2 + half] = s.w;
-        c[half] = 2.0f * fmaf(s.x, s.x, fmaf(s.y, s.y, fmaf(s.z, s.z, s.w * s.w)));
-        c[2 + half] = __uint_as_float(code);
+        // Element e + 1 is in run k, or starts run k + 1 (runs are nonempty).
+        const int k1 = (e + 1 >= kin && k < 31) ? k + 1 : k;
+        uint32_t site[2];
+        site[0] = __shfl_sync(full, shift, k) + e;
+        site[1] = __shfl_sync(full, shift, k1) + e + 1;
+        float4 y[2];
+        uint32_t code[2];
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+          y[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+          code[b] = 0xffffffffu;
+          if (el + b < count) {
+            y[b] = sq[site[b]];
+            code[b] = scode[site[b]];
+          }
+        }
+        const int slot = 32 * h + lane;
+        T.wx[slot] = make_float4(y[0].x, y[1].x, y[0].y, y[1].y);
+        T.yz[slot] = make_float4(y[0].z, y[1].z, y[0].w, y[1].w);
+        T.nc[slot] = make_float4(2.0f * fmaf(y[0].x, y[0].x, fmaf(y[0].y, y[0].y, fmaf(y[0].z, y[0].z, y[0].w * y[0].w))),
+                                 2.0f * fmaf(y[1].x, y[1].x, fmaf(y[1].y, y[1].y, fmaf(y[1].z, y[1].z, y[1].w * y[1].w))),
+                                 __uint_as_float(code[0]), __uint_as_float(code[1]));
+        if (TRACK) reinterpret_cast<uint2*>(T.at)[slot] = make_uint2(site[0], site[1]);
       }
       __syncwarp();
-      if (!live) continue;
-      float2 sw = splat(0.f), sx = splat(0.f), sy = splat(0.f), sz = splat(0.f), sc = splat(0.f), se = splat(0.f);
-      const int pairs = (count + 1) >> 1;
-      for (int u = 0; u < pairs; ++u) {
-        const float4 A = T.wx[u], B = T.yz[u];
-        const float2 mw = fma2(make_float2(A.x, A.y), splat(-1.0f), xw);
-        const float2 mx = fma2(make_float2(A.z, A.w), splat(-1.0f), xx);
-        const float2 my = fma2(make_float2(B.x, B.y), splat(-1.0f), xy);
-        const float2 mz = fma2(make_float2(B.z, B.w), splat(-1.0f), xz);
-        const float2 dm2 = fma2(mw, mw, fma2(mx, mx, fma2(my, my, mul2(mz, mz))));
-        if (dm2.x > cut2 && dm2.y > cut2) continue;
-        const float4 M = T.nc[u];
-        const uint32_t c0 = __float_as_uint(M.z), c1 = __float_as_uint(M.w);
-        const bool own0 = ((c0 ^ i) & ~kIdentityBit) == 0, own1 = ((c1 ^ i) & ~kIdentityBit) == 0;
-        const bool own = own0 || own1;
-        float n0 = dm2.x, n1 = dm2.y;
-        if (own) {  // the thread's own source: no force; its identity image is no neighbour
-          if (own0 && c0 != i) n0 = 4.0f;
-          if (own1 && c1 != i) n1 = 4.0f;
-        }
-        if (TRACK) {
-          if (n0 < best) {
-            best = n0;
-            best_at = (int)(base + 2 * u);
+      if (live) {
+#pragma unroll
+        for (int m = 0; m < kNearSlots; ++m) {
+          const int u = sub + kNearSub * m;  // elements 2u and 2u + 1
+          const int first = 2 * u;
+          if (first >= count) break;
+          const float4 A = T.wx[u], B = T.yz[u];
+          const float2 mw = fma2(make_float2(A.x, A.y), splat(-1.0f), xw);
+          const float2 mx = fma2(make_float2(A.z, A.w), splat(-1.0f), xx);
+          const float2 my = fma2(make_float2(B.x, B.y), splat(-1.0f), xy);
+          const float2 mz = fma2(make_float2(B.z, B.w), splat(-1.0f), xz);
+          const float2 dm2 = fma2(mw, mw, fma2(mx, mx, fma2(my, my, mul2(mz, mz))));
+          if (dm2.x > cut2 && dm2.y > cut2) continue;
+          const float4 M = T.nc[u];
+          const uint32_t c0 = __float_as_uint(M.z), c1 = __float_as_uint(M.w);
+          const bool own0 = ((c0 ^ i) & ~kIdentityBit) == 0, own1 = ((c1 ^ i) & ~kIdentityBit) == 0;
+          const bool own = own0 || own1;
+          float n0 = dm2.x, n1 = dm2.y;
+          if (own) {  // the thread's own source: no force; its identity image is no neighbour
+            if (own0 && c0 != i) n0 = 4.0f;
+            if (own1 && c1 != i) n1 = 4.0f;
           }
-          if (n1 < best) {
-            best = n1;
-            best_at = (int)(base + 2 * u + 1);
+          if (TRACK) {
+            if (n0 < best) {
+              best = n0;
+              best_at = (int)T.at[first];
+            }
+            if (n1 < best) {
+              best = n1;
+              best_at = (int)T.at[first + 1];
+            }
+          } else {
+            best = fminf(best, fminf(n0, n1));
           }
-        } else {
-          best = fminf(best, fminf(n0, n1));
+          // A site beyond the cutoff takes the chord at 1.25 r: its terms stay finite (a site
+          // nearer the antipode, dm2 > 2, would drive the half-angle out of range) and the
+          // window makes them exactly zero.
+          const float2 dmc = make_float2(fminf(dm2.x, cut_hi), fminf(dm2.y, cut_hi));
+          const float2 dp2 = fma2(dmc, splat(-1.0f), add2(xn, make_float2(M.x, M.y)));
+          Pair2 pr = near_pair32x2<SHORT>(dmc, dp2, cw, czw);
+          if (own) {
+            const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
+            pr.coef = mul2(pr.coef, keep);
+            pr.curv = mul2(pr.curv, keep);
+            pr.energy = mul2(pr.energy, keep);
+          }
+          sw = fma2(pr.coef, mw, sw);
+          sx = fma2(pr.coef, mx, sx);
+          sy = fma2(pr.coef, my, sy);
+          sz = fma2(pr.coef, mz, sz);
+          sc = add2(sc, pr.curv);
+          se = add2(se, pr.energy);
         }
-        const float2 dp2 = fma2(dm2, splat(-1.0f), add2(xn, make_float2(M.x, M.y)));
-        Pair2 pr = near_pair32x2<SHORT>(dm2, dp2, cw, czw);
-        if (own) {
-          const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
-          pr.coef = mul2(pr.coef, keep);
-          pr.curv = mul2(pr.curv, keep);
-          pr.energy = mul2(pr.energy, keep);
-        }
-        sw = fma2(pr.coef, mw, sw);
-        sx = fma2(pr.coef, mx, sx);
-        sy = fma2(pr.coef, my, sy);
-        sz = fma2(pr.coef, mz, sz);
-        sc = add2(sc, pr.curv);
-        se = add2(se, pr.energy);
       }
-      sums[0][threadIdx.x] += (double)sw.x + (double)sw.y;
-      sums[1][threadIdx.x] += (double)sx.x + (double)sx.y;
-      sums[2][threadIdx.x] += (double)sy.x + (double)sy.y;
-      sums[3][threadIdx.x] += (double)sz.x + (double)sz.y;
-      sums[4][threadIdx.x] += (double)sc.x + (double)sc.y;
-      sums[5][threadIdx.x] += (double)se.x + (double)se.y;
+      if (++since == kNearMerge) {
+        merge_sums(sums, sw, sx, sy, sz, sc, se);
+        since = 0;
+      }
     }
   }
-  if (!live) return;
+  merge_sums(sums, sw, sx, sy, sz, sc, se);
+  // The nearest over the source's lanes: smallest chord, then smallest sorted-site index
+  // (the first such site in the walk's order).
+#pragma unroll
+  for (int o = kNearSub / 2; o > 0; o >>= 1) {
+    const float ob = __shfl_xor_sync(full, best, o);
+    if (TRACK) {
+      const int oa = __shfl_xor_sync(full, best_at, o);
+      if (ob < best || (ob == best && (unsigned)oa < (unsigned)best_at)) {
+        best = ob;
+        best_at = oa;
+      }
+    } else {
+      best = fminf(best, ob);
+    }
+  }
+  __syncwarp();
+  if (!live || sub != 0) return;
   if (best > cut2) {  // no site within the cutoff
     best = 4.0f;
     best_at = -1;
   }
-  const double3 f = force_from_differences(
-      to_d4(x), make_double4(sums[0][threadIdx.x], sums[1][threadIdx.x], sums[2][threadIdx.x], sums[3][threadIdx.x]));
+  double t[6];
+  for (int c = 0; c < 6; ++c) {
+    t[c] = 0.0;
+    for (int l = 0; l < kNearSub; ++l) t[c] += sums[c][threadIdx.x + l];
+  }
+  const double3 f = force_from_differences(to_d4(x), make_double4(t[0], t[1], t[2], t[3]));
   const size_t at = (size_t)slice * stride + p;
-  out.force[at] = make_double4(f.x, f.y, f.z, sums[4][threadIdx.x]);
-  out.energy[at] = sums[5][threadIdx.x];
+  out.force[at] = make_double4(f.x, f.y, f.z, t[4]);
+  out.energy[at] = t[5];
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;
 }
@@ -768,7 +883,7 @@ cudaError_t launch_dense_near(int prec, bool track, bool short_atan, const float
   const dim3 grid(pl.jtiles, pl.chunks);
   const bool direct = pl.chunks == 1;
   const Rows dst = direct ? out : partial;
-  const NearCut cut{cut2, chord, cut_z, cut_w};
+  const NearCut cut = near_cut(cut2, chord, cut_z, cut_w);
   probe_mark(s);
   if (prec == kFP64) {
     if (track) k_dense64<true><<<grid, kPairBlock, 0, s>>>(q64, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, cut, dst, n);
@@ -834,9 +949,10 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   k_scatter<<<(n + tb - 1) / tb, tb, 0, s>>>(L.src_key, L.src_rank, L.moff, n, nullptr, L.src_perm);
   k_bucket_sort<<<(mcells + tb - 1) / tb, tb, 0, s>>>(L.moff, mcells, nullptr, L.src_perm);
   // 4. gather, 5. slices summed into rows
-  const int warps = (n + 31) / 32;
-  const dim3 grid((warps + kNearWarps - 1) / kNearWarps, L.slices);
-  NearCut cut{L.cut2, L.chord, L.cut_z, L.cut_w};
+  const int warps = fp64 ? (n + 31) / 32 : (n + kNearGroup - 1) / kNearGroup;
+  const int slices = fp64 ? L.slices : L.slices32;
+  const dim3 grid((warps + kNearWarps - 1) / kNearWarps, slices);
+  const NearCut cut = near_cut(L.cut2, L.chord, L.cut_z, L.cut_w);
   const Rows dst = L.partial;
   probe_mark(s);
   if (fp64) {
@@ -845,11 +961,11 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   } else {
     auto kernel = L.track ? (L.short_atan ? k_near32<true, true> : k_near32<true, false>)
                           : (L.short_atan ? k_near32<false, true> : k_near32<false, false>);
-    kernel<<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, L.slices,
+    kernel<<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, slices,
                                             dst, n);
   }
   probe_mark(s);
-  k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(L.partial, n, L.slices, n, (const int*)L.src_perm, L.out, L.track ? 1 : 0);
+  k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(L.partial, n, slices, n, (const int*)L.src_perm, L.out, L.track ? 1 : 0);
   // shell count, shell write, grid, cell count, scatter, bucket sort, site gather, source
   // count, scatter, bucket sort, gather, reduce (scans counted by launch_scan; memsets aside)
   probe_count(12);

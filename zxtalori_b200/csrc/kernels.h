@@ -44,6 +44,7 @@ cudaError_t launch_full(int prec, const float4* q32, const double4* q64, int n, 
 // One near-field pass; every pointer is device memory sized by the host (Near workspace).
 struct NearLaunch {
   int prec, gid, n, capacity, sdim_max, slices;
+  int slices32;  // slices of the FP32 gather (kNearGroup sources per warp); <= slices
   bool track;
   bool short_atan;  // cutoff r <= 0.4 rad: the short-range arctangent applies
   double s_margin, cut2, chord, cut_z, cut_w;

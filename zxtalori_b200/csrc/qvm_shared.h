@@ -13,7 +13,10 @@ constexpr int kMaxCellDim = 128;        // chart grid side (src/near.zig:135)
 constexpr int kOrderBits = 6;
 constexpr int kOrderDim = 1 << kOrderBits;
 // Target sites per cell of the chart grid (the reference uses 8, src/near.zig:135).
-constexpr double kSitesPerCell = 3.0;
+constexpr double kSitesPerCell = 2.0;
+// FP32 near-field gather: sources per warp (each source's sites split over 32 / kNearGroup
+// lanes). Small groups keep the union of the sources' neighbourhoods close to each one's.
+constexpr int kNearGroup = 4;
 
 // Precision of one sample's arithmetic.
 //  kFP32: FP32 pair arithmetic (approximate SFU reciprocals, own atan), FP64 row sums,
