@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-extras", action="store_true",
                    help="skip the all-pairs, spacing, batched and served sections")
+    p.add_argument("--cpu-budget", type=float, default=None,
+                   help="seconds of CPU work per reference-arm step (default: a few minutes in all)")
     p.add_argument("--large", action="store_true",
                    help="also time the default measures of group I at N=1M (all pairs, about a minute)")
     return p.parse_args()
@@ -178,7 +180,7 @@ def run_reference(args, dist):
         return 0
     from oracle import cref
 
-    budget = max(2.0, min(15.0, 150.0 / max(1, args.steps + args.warmup)))
+    budget = args.cpu_budget or max(2.0, min(15.0, 150.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
         cpu_sample(budget_s=budget / 4)
     times, rates = [], []
