@@ -98,6 +98,7 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   }
   counts_.ensure((size_t)(n + 1) * 4);
   offsets_.ensure((size_t)(n + 1) * 4);
+  shell_mask_.ensure((size_t)n * sizeof(uint4));
   scan_tmp_.ensure(4096 * 4);
   ZO_CUDA(launch_shell_count(prec, q32, q64, n, gid_, s_margin_, counts_.as<uint32_t>(), offsets_.as<uint32_t>(),
                              scan_tmp_.as<uint32_t>(), s));
@@ -180,6 +181,7 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
   L.counts = counts_.as<uint32_t>();
   L.offsets = offsets_.as<uint32_t>();
   L.scan_tmp = scan_tmp_.as<uint32_t>();
+  L.shell_mask = shell_mask_.as<uint4>();
   L.site_q32 = prec == kFP64 ? nullptr : site_q_.as<float4>();
   L.site_q64 = prec == kFP64 ? site_q_.as<double4>() : nullptr;
   L.site_code = site_code_.as<uint32_t>();

@@ -44,47 +44,98 @@ __device__ __forceinline__ double4 source_d(const float4* q32, const double4* q6
   return fp64 ? q64[j] : to_d4(q32[j]);
 }
 
-// Classification image of (source, operator k, sign): normalize(orig * normalize(g_k)), negated.
-__device__ __forceinline__ double4 shell_image(double4 orig, int op_row, bool neg, bool fp64) {
-  const double4 g = normalize4(fp64 ? c_ops64[op_row] : c_ops32[op_row]);
+// Classification image of (source, operator k, sign): normalize(orig * normalize(g_k)),
+// negated; g is the normalised operator.
+__device__ __forceinline__ double4 shell_image(double4 orig, double4 g, bool neg) {
   double4 c = normalize4(qmul(orig, g));
   return neg ? neg4(c) : c;
 }
 
-__global__ void k_shell_count(const float4* __restrict__ q32, const double4* __restrict__ q64, int n, int gid, int fp64i,
-                              double s_margin, uint32_t* __restrict__ counts) {
+// The group's operators, normalised once per block into shared memory.
+__device__ __forceinline__ void unit_operators(double4* g, int off, int order, bool fp64) {
+  for (int k = threadIdx.x; k < order; k += blockDim.x) g[k] = normalize4(fp64 ? c_ops64[off + k] : c_ops32[off + k]);
+  __syncthreads();
+}
+
+// Counts each source's sites and records which images are sites (bit img of a 128-bit
+// mask, img = 2 operator + sign; the identity image always), so the write pass needs no
+// second classification. FP64 mode classifies in FP64 (shell.wgsl:19-22 restated); FP32
+// mode in FP32 with the float32 planes: rounding moves a decision only within ~1e-7 of the
+// widened plane, while the margin, sin(r + 1e-4) + 2e-6, leaves 1e-4 rad between it and
+// any site a zone source can reach within r.
+template <bool FP64>
+__global__ void __launch_bounds__(256) k_shell_count(const float4* __restrict__ q32, const double4* __restrict__ q64,
+                                                     int n, int gid, double s_margin, uint32_t* __restrict__ counts,
+                                                     uint4* __restrict__ masks) {
+  __shared__ double4 g64[FP64 ? 60 : 1];
+  __shared__ float4 g32[60];
+  const int off = c_group_offset[gid], order = c_group_order[gid];
+  for (int k = threadIdx.x; k < order; k += blockDim.x) {
+    if (FP64) g64[k] = normalize4(c_ops64[off + k]);
+    else g32[k] = to_f4(normalize4(c_ops32[off + k]));
+  }
+  __syncthreads();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
-  const bool fp64 = fp64i != 0;
-  const int off = c_group_offset[gid], order = c_group_order[gid];
   const int poff = c_plane_offset[gid], planes = 2 * order - 1;
-  const double4 orig = normalize4(source_d(q32, q64, j, fp64));
-  uint32_t c = 1;  // the identity image (a core site)
-  if (on_rim(orig, poff, planes, fp64, s_margin + 2e-6)) {
-    for (int img = 1; img < 2 * order; ++img) {
-      const double4 y = shell_image(orig, off + img / 2, img & 1, fp64);
-      if (y.x > -0.9999999 && inside_planes(y, poff, planes, fp64, s_margin + 2e-6)) ++c;
+  uint32_t w[4] = {1u, 0u, 0u, 0u};  // the identity image is always a (core) site
+  if (FP64) {
+    const double margin = s_margin + 2e-6;
+    const double4 orig = normalize4(q64[j]);
+    if (on_rim(orig, poff, planes, true, margin)) {
+      for (int img = 1; img < 2 * order; ++img) {
+        const double4 y = shell_image(orig, g64[img / 2], img & 1);
+        if (y.x > -0.9999999 && inside_planes(y, poff, planes, true, margin)) w[img >> 5] |= 1u << (img & 31);
+      }
+    }
+  } else {
+    const float margin = (float)(s_margin + 2e-6);
+    const float4 orig = to_f4(normalize4(to_d4(q32[j])));
+    bool rim = false;
+    for (int k = 0; k < planes && !rim; ++k) {
+      const float4 h = c_planes32[poff + k];
+      rim = fmaf(orig.x, h.x, fmaf(orig.y, h.y, fmaf(orig.z, h.z, orig.w * h.w))) <= margin;
+    }
+    if (rim) {
+      for (int img = 1; img < 2 * order; ++img) {
+        const float4 a = orig, b = g32[img / 2];
+        float4 y = make_float4(a.x * b.x - a.y * b.y - a.z * b.z - a.w * b.w,
+                               a.x * b.y + a.y * b.x + a.z * b.w - a.w * b.z,
+                               a.x * b.z - a.y * b.w + a.z * b.x + a.w * b.y,
+                               a.x * b.w + a.y * b.z - a.z * b.y + a.w * b.x);
+        if (img & 1) y = make_float4(-y.x, -y.y, -y.z, -y.w);
+        if (!(y.x > -0.9999999f)) continue;
+        bool inside = true;
+        for (int k = 0; k < planes && inside; ++k) {
+          const float4 h = c_planes32[poff + k];
+          inside = fmaf(y.x, h.x, fmaf(y.y, h.y, fmaf(y.z, h.z, y.w * h.w))) >= -margin;
+        }
+        if (inside) w[img >> 5] |= 1u << (img & 31);
+      }
     }
   }
-  counts[j] = c;
+  counts[j] = (uint32_t)(__popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]));
+  if (masks) masks[j] = make_uint4(w[0], w[1], w[2], w[3]);
 }
 
 // Writes the sites of each source at its scanned offset: the rebuilt image quaternion
 // (pairs.wgsl:181 / near.wgsl:263-269), its code (source, high bit for the identity
 // image), its image number 2*operator+sign, and its chart position; plus the chart box.
+// The images are those k_shell_count recorded in the source's mask.
 template <bool FP64>
 __global__ void __launch_bounds__(256) k_shell_write(const float4* __restrict__ q32, const double4* __restrict__ q64,
-                                                     int n, int gid, double s_margin,
+                                                     int n, int gid, const uint4* __restrict__ masks,
                                                      const uint32_t* __restrict__ offsets, int capacity,
                                                      float4* __restrict__ site_q32, double4* __restrict__ site_q64,
                                                      uint32_t* __restrict__ site_code, uint32_t* __restrict__ site_img,
                                                      float4* __restrict__ site_pos, NearGrid* grid) {
+  __shared__ double4 g[60];
+  const int off = c_group_offset[gid], order = c_group_order[gid];
+  unit_operators(g, off, order, FP64);
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
   bool overflow = false;
   if (j < n) {
-    const int off = c_group_offset[gid], order = c_group_order[gid];
-    const int poff = c_plane_offset[gid], planes = 2 * order - 1;
     const double4 src = source_d(q32, q64, j, FP64);
     const double4 orig = normalize4(src);
     uint32_t at = offsets[j];
@@ -114,11 +165,15 @@ __global__ void __launch_bounds__(256) k_shell_write(const float4* __restrict__ 
       hi[2] = fmaxf(hi[2], p.z);
       ++at;
     };
+    const uint4 m = masks[j];
+    const uint32_t words[4] = {m.x, m.y, m.z, m.w};
     emit(orig, 0, true);
-    if (on_rim(orig, poff, planes, FP64, s_margin + 2e-6)) {
-      for (int img = 1; img < 2 * order; ++img) {
-        const double4 y = shell_image(orig, off + img / 2, img & 1, FP64);
-        if (y.x > -0.9999999 && inside_planes(y, poff, planes, FP64, s_margin + 2e-6)) emit(y, img, false);
+    for (int w = 0; w < 4; ++w) {
+      uint32_t b = words[w] & (w == 0 ? ~1u : ~0u);
+      while (b) {
+        const int img = 32 * w + __ffs(b) - 1;
+        b &= b - 1;
+        emit(shell_image(orig, g[img / 2], img & 1), img, false);
       }
     }
   }
@@ -903,7 +958,8 @@ cudaError_t launch_dense_near(int prec, bool track, bool short_atan, const float
 // Site count of a shell pass (offsets[n] after the scan), for sizing the workspace.
 cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, int n, int gid, double s_margin,
                                uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, cudaStream_t s) {
-  k_shell_count<<<(n + 255) / 256, 256, 0, s>>>(q32, q64, n, gid, prec == kFP64, s_margin, counts);
+  if (prec == kFP64) k_shell_count<true><<<(n + 255) / 256, 256, 0, s>>>(q32, q64, n, gid, s_margin, counts, nullptr);
+  else k_shell_count<false><<<(n + 255) / 256, 256, 0, s>>>(q32, q64, n, gid, s_margin, counts, nullptr);
   return launch_scan(counts, offsets, n, nullptr, scan_tmp, s);
 }
 
@@ -912,15 +968,16 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   const bool fp64 = L.prec == kFP64;
   const int tb = 256;
   // 1. shell
-  k_shell_count<<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, fp64, L.s_margin, L.counts);
+  if (fp64) k_shell_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.s_margin, L.counts, L.shell_mask);
+  else k_shell_count<false><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.s_margin, L.counts, L.shell_mask);
   cudaError_t e = launch_scan(L.counts, L.offsets, n, nullptr, L.scan_tmp, s);
   if (e) return e;
   if (fp64)
-    k_shell_write<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.s_margin, L.offsets, L.capacity,
+    k_shell_write<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.shell_mask, L.offsets, L.capacity,
                                                          L.site_q32, L.site_q64, L.site_code, L.site_img, L.site_pos,
                                                          L.grid);
   else
-    k_shell_write<false><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.s_margin, L.offsets, L.capacity,
+    k_shell_write<false><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.shell_mask, L.offsets, L.capacity,
                                                           L.site_q32, L.site_q64, L.site_code, L.site_img, L.site_pos,
                                                           L.grid);
   // 2. grid and the site sort

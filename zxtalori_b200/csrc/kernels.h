@@ -51,6 +51,7 @@ struct NearLaunch {
   const float4* q32;
   const double4* q64;
   uint32_t *counts, *offsets, *scan_tmp;
+  uint4* shell_mask;  // per source: which images are sites (bit 2 operator + sign)
   float4* site_q32;
   double4* site_q64;
   uint32_t *site_code, *site_img, *site_cell, *site_rank;
