@@ -452,32 +452,46 @@ struct NearTile {
 };
 
 // Per-warp data of the row walk, kept in shared memory (it is warp-uniform) so the hot
-// loop's registers go to the pair arithmetic.
+// loop's registers go to the pair arithmetic. Stereographic projection maps spheres to
+// spheres: the sites within the cutoff of source x (x . y >= k, k = 1 - cut2/2) are the
+// chart points within rho = sqrt(1 - k^2) / (x_w + k) of c = x_v / (x_w + k) (exactly, for
+// a unit x and k > -x_w). The walk covers the union of its sources' balls.
 struct NearWalk {
-  WarpBox box;
+  float cen[kNearGroup][3];
+  float rad[kNearGroup];  // < 0: no source in this place
+  int clo[3], chi[3];     // cells of the balls' bounding box
   float lower[3], cells_per_unit;
   int sdim;
   uint2 runs[32];  // a batch's nonempty row runs (start, length), compacted
 };
 
-// row_run from the warp's shared walk data.
+// Row r of the walk's (y, z) cell rows: the run of sorted sites of the x cells that some
+// source's ball reaches in this row.
 __device__ __forceinline__ bool walk_row(const NearWalk& W, const uint32_t* cell_off, int r, uint32_t& start,
                                          uint32_t& end) {
-  const WarpBox& b = W.box;
-  const int ny = b.chi[1] - b.clo[1] + 1;
-  const int y = b.clo[1] + r % ny, z = b.clo[2] + r / ny;
+  const int ny = W.chi[1] - W.clo[1] + 1;
+  const int y = W.clo[1] + r % ny, z = W.clo[2] + r / ny;
   const float width = 1.0f / W.cells_per_unit;
   const float cy = W.lower[1] + (float)y * width, cz = W.lower[2] + (float)z * width;
-  const float gy = fmaxf(0.f, fmaxf(cy - b.hi[1], b.lo[1] - (cy + width)));
-  const float gz = fmaxf(0.f, fmaxf(cz - b.hi[2], b.lo[2] - (cz + width)));
-  const float rest = b.d * b.d - gy * gy - gz * gz;
-  if (rest < 0.f) return false;
-  const float span = sqrtf(rest);
-  const int x0 = cell_axis(b.lo[0] - span, W.lower[0], W.cells_per_unit, W.sdim);
-  const int x1 = cell_axis(b.hi[0] + span, W.lower[0], W.cells_per_unit, W.sdim);
+  float x0 = 3e38f, x1 = -3e38f;
+#pragma unroll
+  for (int s = 0; s < kNearGroup; ++s) {
+    const float rho = W.rad[s];
+    if (rho < 0.f) continue;
+    const float gy = fmaxf(0.f, fmaxf(cy - W.cen[s][1], W.cen[s][1] - (cy + width)));
+    const float gz = fmaxf(0.f, fmaxf(cz - W.cen[s][2], W.cen[s][2] - (cz + width)));
+    const float rest = rho * rho - gy * gy - gz * gz;
+    if (rest < 0.f) continue;
+    const float span = sqrtf(rest);
+    x0 = fminf(x0, W.cen[s][0] - span);
+    x1 = fmaxf(x1, W.cen[s][0] + span);
+  }
+  if (!(x0 <= x1)) return false;
+  const int c0 = cell_axis(x0, W.lower[0], W.cells_per_unit, W.sdim);
+  const int c1 = cell_axis(x1, W.lower[0], W.cells_per_unit, W.sdim);
   const int row = W.sdim * (y + W.sdim * z);
-  start = cell_off[row + x0];
-  end = cell_off[row + x1 + 1];
+  start = cell_off[row + c0];
+  end = cell_off[row + c1 + 1];
   return start < end;
 }
 
@@ -517,12 +531,29 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
   const uint32_t i = live ? src_perm[p] : 0u;
   const float4 x = q[i];
   {
+    // This source's chart ball, 0.1% wider (plus 1e-6) for the FP32 rounding of the chart.
     const NearGrid g = *gp;
-    WarpBox box;
-    if (!warp_box(chart(x), live, g, (float)cut.chord, box)) return;
+    const double kappa = 1.0 - 0.5 * cut.cut2;
+    const double den = 1.0 / ((double)x.x + kappa);
+    const float c[3] = {(float)(x.y * den), (float)(x.z * den), (float)(x.w * den)};
+    const float rho = (float)(sqrt(1.0 - kappa * kappa) * den) * 1.001f + 1e-6f;
+    float lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = warp_min(live ? c[a] - rho : 3e38f);
+      hi[a] = warp_max(live ? c[a] + rho : -3e38f);
+    }
+    if (!(lo[0] <= hi[0])) return;  // no live source in this warp
+    if (sub == 0) {
+      const int s = lane / kNearSub;
+      for (int a = 0; a < 3; ++a) W.cen[s][a] = c[a];
+      W.rad[s] = live ? rho : -1.0f;
+    }
     if (lane == 0) {
-      W.box = box;
-      for (int a = 0; a < 3; ++a) W.lower[a] = g.lower[a];
+      for (int a = 0; a < 3; ++a) {
+        W.clo[a] = cell_axis(lo[a], g.lower[a], g.cells_per_unit, g.sdim);
+        W.chi[a] = cell_axis(hi[a], g.lower[a], g.cells_per_unit, g.sdim);
+        W.lower[a] = g.lower[a];
+      }
       W.cells_per_unit = g.cells_per_unit;
       W.sdim = g.sdim;
     }
@@ -537,7 +568,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
   int best_at = -1;
   float2 sw = splat(0.f), sx = splat(0.f), sy = splat(0.f), sz = splat(0.f), sc = splat(0.f), se = splat(0.f);
   int since = 0;  // tiles since the last FP64 merge
-  const int rows = (W.box.chi[1] - W.box.clo[1] + 1) * (W.box.chi[2] - W.box.clo[2] + 1);
+  const int rows = (W.chi[1] - W.clo[1] + 1) * (W.chi[2] - W.clo[2] + 1);
   const int mine = rows > slice ? (rows - slice + slices - 1) / slices : 0;  // rows slice, slice+slices, ...
   for (int rb = 0; rb < mine; rb += 32) {
     uint32_t start = 0, len = 0;

@@ -174,34 +174,42 @@ __global__ void __launch_bounds__(256) k_median_round(Rows rows, int n, int roun
 __global__ void k_move_fold(float4* __restrict__ q32, double4* __restrict__ q64, int n, int gid, int prec, Rows rows,
                             double4* __restrict__ prev_f, double4* __restrict__ prev_d, RelaxDev* st, int fixed,
                             double radius, double step_scale) {
+  if (st->flags != 0u) return;  // the step stopped (uniform across the grid)
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || st->flags != 0u) return;
   const bool fp64 = prec == kFP64;
-  if (i == fixed) {
+  double moved_by = 0.0;  // this source's step length (>= 0)
+  if (i < n && i == fixed) {
     prev_f[i] = make_double4(0, 0, 0, 0);
     prev_d[i] = make_double4(0, 0, 0, 0);
     q32[i] = make_float4(1.f, 0.f, 0.f, 0.f);
     if (fp64) q64[i] = make_double4(1, 0, 0, 0);
-    return;
+  } else if (i < n) {
+    const double alpha = st->alpha, median = st->median;
+    const double4 f = rows.force[i];
+    const double scale = alpha * step_scale / fmax(1e-6, f.w / median + 1e-2);
+    const double size = sqrt(f.x * f.x + f.y * f.y + f.z * f.z) * scale;
+    const double clip = fmin(1.0, 0.5 * radius / fmax(size, 1e-12));
+    const double k = scale * clip;
+    const double dx = f.x * k, dy = f.y * k, dz = f.z * k;
+    prev_f[i] = make_double4(f.x, f.y, f.z, 0.0);
+    prev_d[i] = make_double4(dx, dy, dz, 0.0);
+    moved_by = size * clip;
+    const double angle = sqrt(dx * dx + dy * dy + dz * dz);
+    const double sinc = angle > 1e-4 ? sin(angle) / angle : 1.0 - angle * angle / 6.0;
+    const double4 rot = make_double4(cos(angle), dx * sinc, dy * sinc, dz * sinc);
+    const double4 qi = fp64 ? q64[i] : to_d4(q32[i]);
+    double4 moved = normalize4(qmul(rot, qi));
+    moved = fold64(moved, gid, !fp64);
+    q32[i] = to_f4(moved);
+    if (fp64) q64[i] = moved;
   }
-  const double alpha = st->alpha, median = st->median;
-  const double4 f = rows.force[i];
-  const double scale = alpha * step_scale / fmax(1e-6, f.w / median + 1e-2);
-  const double size = sqrt(f.x * f.x + f.y * f.y + f.z * f.z) * scale;
-  const double clip = fmin(1.0, 0.5 * radius / fmax(size, 1e-12));
-  const double k = scale * clip;
-  const double dx = f.x * k, dy = f.y * k, dz = f.z * k;
-  prev_f[i] = make_double4(f.x, f.y, f.z, 0.0);
-  prev_d[i] = make_double4(dx, dy, dz, 0.0);
-  atomicMax(&st->step_bits, (unsigned long long)__double_as_longlong(size * clip));
-  const double angle = sqrt(dx * dx + dy * dy + dz * dz);
-  const double sinc = angle > 1e-4 ? sin(angle) / angle : 1.0 - angle * angle / 6.0;
-  const double4 rot = make_double4(cos(angle), dx * sinc, dy * sinc, dz * sinc);
-  const double4 qi = fp64 ? q64[i] : to_d4(q32[i]);
-  double4 moved = normalize4(qmul(rot, qi));
-  moved = fold64(moved, gid, !fp64);
-  q32[i] = to_f4(moved);
-  if (fp64) q64[i] = moved;
+  // The largest step: non-negative doubles order as their bit patterns; one atomic per warp.
+  unsigned long long bits = (unsigned long long)__double_as_longlong(moved_by);
+  for (int o = 16; o; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+    bits = other > bits ? other : bits;
+  }
+  if ((threadIdx.x & 31) == 0 && bits) atomicMax(&st->step_bits, bits);
 }
 
 // Quick measures of a force pass (src/pairs.zig:130-140, 182-199): energy sum, force^2 sum
