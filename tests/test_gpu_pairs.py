@@ -172,3 +172,37 @@ def test_chunked_sums_match(engine, group, count):
     for key in ("quey_energy", "riesz_1", "riesz_2", "riesz_3", "green_ratio", "log_ratio", "separation_deg"):
         assert chunked[key] == pytest.approx(whole[key], rel=2e-5, abs=2e-6), key
     assert np.max(np.abs(moved_chunked - moved_whole)) < 2e-5
+
+
+def _turn(q, axis, h):
+    """Left rotation by angle h about a coordinate axis (tests/test_pair_kernels.py:151-153)."""
+    d = np.zeros(4)
+    d[0], d[axis + 1] = math.cos(h), math.sin(h)
+    return qvm.qmul(d, q)
+
+
+@pytest.mark.parametrize("precision,rtol", [("fp64", 2e-6), ("fp32", 1e-5)])
+def test_force_is_half_energy_gradient(engine, golden, precision, rtol):
+    """Force sign, left-tangent frame and factor of two against finite differences
+    (tests/test_pair_kernels.py:147-159): turning source 0 by +-h (h = 1e-6) about each axis,
+    d(sum E)/d(theta) = -2 F_0. The engine's force is taken at its own positions; the energy
+    sums come from the FP64 oracle at the same positions turned (a float32 import would round
+    away the 1e-6 turn)."""
+    base = golden["rows_q"][:9].astype(np.float64)
+    base /= np.linalg.norm(base, axis=-1, keepdims=True)
+    ops = golden["ops_C2"].astype(np.float64) if precision == "fp64" else \
+        golden["ops_C2"].astype(np.float32).astype(np.float64)
+    with engine.from_quaternions(base.astype(np.float32), "C2", precision=precision) as grid:
+        q = grid.quaternions.astype(np.float64)
+        force = grid.debug_rows(0)[:, :3]
+    if precision == "fp64":  # the engine's FP64 state: the FP64 fold of the float32 input
+        q = qvm.fold(base.astype(np.float32), GROUPS.index("C2"), ops, f32=False)
+    h = 1e-6
+    for axis in range(3):
+        energy = []
+        for sign in (1, -1):
+            moved = q.copy()
+            moved[0] = _turn(q[0], axis, sign * h)
+            energy.append(qvm.pair_rows(moved, ops)["energy"].sum())
+        derivative = (energy[0] - energy[1]) / (2 * h)
+        assert abs(derivative + 2 * force[0, axis]) <= rtol * max(1.0, abs(derivative)), (axis, derivative, force[0])

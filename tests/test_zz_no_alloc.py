@@ -66,3 +66,32 @@ def test_no_alloc_rejects_sizes_beyond_its_scratch(engine):
     assert rc == -2 and "65536" in msg
     rc, msg = run(fn, 11, q_dev, 4, out)
     assert rc == -1 and "group" in msg
+
+
+def test_no_alloc_rows_do_not_depend_on_representative_signs(engine):
+    """Antipodal invariance of the all-pairs kernel on unfolded input (this entry point takes
+    positions as given, with no zone fold): negating every other quaternion leaves force,
+    curvature, energy and nearest chord unchanged (tests/test_pair_kernels.py:131-135); each
+    pair picks its near twin by the sign of x.y either way, so only rounding may differ."""
+    import torch
+
+    fn = bind(engine)
+    with engine.haar("D3", 2000, 5) as grid:
+        q = grid.quaternions
+    signed = q.copy()
+    signed[::2] *= -1
+    rows = []
+    for values in (q, signed):
+        out = torch.zeros((6 * len(q),), dtype=torch.float64, device="cuda")
+        rc, msg = run(fn, engine.GROUPS.index("D3"), torch.from_numpy(values).cuda(), len(q), out)
+        assert rc == 0, msg
+        torch.cuda.synchronize()
+        rows.append(out.cpu().numpy())
+    n = len(q)
+    a, b = rows
+    fa, fb = a[:4 * n].reshape(n, 4), b[:4 * n].reshape(n, 4)
+    # The left-tangent force vec(y x*) is unchanged by x -> -x (the near twin flips with it).
+    assert np.abs(fa[:, :3] - fb[:, :3]).max() < 1e-5 * np.abs(fa[:, :3]).max()
+    np.testing.assert_allclose(fa[:, 3], fb[:, 3], rtol=1e-5)
+    np.testing.assert_allclose(a[4 * n:5 * n], b[4 * n:5 * n], rtol=1e-5)
+    np.testing.assert_allclose(a[5 * n:], b[5 * n:], rtol=1e-5)

@@ -180,19 +180,16 @@ __device__ __forceinline__ Pair2 quey_pair32x2(float2 nearv, float2 farv) {
   const float2 a = max2(two_atan_unit2(t, t2), 1e-12f);
   const float2 b = fma2(a, splat(-1.0f), splat(kPiF));
   const float2 aa = mul2(a, a), bb = mul2(b, b);
-  const float2 a2 = add2(aa, splat(1e-9f)), b2 = add2(bb, splat(1e-9f));
+  // b >= pi/2 (a is the near twin's angle), so b^2 + 1e-9 rounds to b^2: b2 = bb.
+  const float2 a2 = add2(aa, splat(1e-9f));
   const float2 a3 = fma2(aa, a, splat(1e-9f)), b3 = fma2(bb, b, splat(1e-9f));
   const float2 onept2 = add2(t2, splat(1.0f));
   const float2 sp = fma2(splat(1e-9f), onept2, add2(t, t));  // (sine + 1e-9) (1 + t^2)
-  const float2 a2b2 = mul2(a2, b2);
-  const float2 r1 = rcp2(mul2(a2b2, sp));
-  const float2 ab = mul2(a, b);
-  const float2 a3b3 = mul2(a3, b3);
-  const float2 r2 = rcp2(mul2(a3b3, ab));
+  const float2 r1 = rcp2(mul2(mul2(a2, bb), sp));
   Pair2 p;
-  p.coef = mul2(mul2(fma2(b2, splat(-1.0f), a2), onept2), r1);  // -(b2 - a2)(1 + t^2) / (a2 b2 sp)
-  p.curv = mul2(mul2(add2(a3, b3), ab), r2);
-  p.energy = mul2(mul2(splat(kPiF), a3b3), r2);
+  p.coef = mul2(mul2(fma2(bb, splat(-1.0f), a2), onept2), r1);  // -(b2 - a2)(1 + t^2) / (a2 b2 sp)
+  p.curv = mul2(add2(a3, b3), rcp2(mul2(a3, b3)));              // 1/a3 + 1/b3
+  p.energy = mul2(splat(kPiF), rcp2(mul2(a, b)));               // pi / (a b)
   return p;
 }
 
@@ -206,25 +203,23 @@ __device__ __forceinline__ Pair2 near_pair32x2(float2 dm2, float2 dp2, float cw,
   const float2 a = max2(SHORT ? two_atan_short2(t, t2) : two_atan_unit2(t, t2), 1e-12f);
   const float2 b = fma2(a, splat(-1.0f), splat(kPiF));
   const float2 aa = mul2(a, a), bb = mul2(b, b);
-  const float2 a2 = add2(aa, splat(1e-9f)), b2 = add2(bb, splat(1e-9f));
+  // b >= pi/2 (the site is the near twin), so b^2 + 1e-9 rounds to b^2: b2 = bb.
+  const float2 a2 = add2(aa, splat(1e-9f));
   const float2 a3 = fma2(aa, a, splat(1e-9f)), b3 = fma2(bb, b, splat(1e-9f));
   const float2 onept2 = add2(t2, splat(1.0f));
   const float2 sp = fma2(splat(1e-9f), onept2, add2(t, t));
-  const float2 a2b2 = mul2(a2, b2);
+  const float2 a2b2 = mul2(a2, bb);
   const float2 r1 = rcp2(mul2(a2b2, sp));
-  const float2 ab = mul2(a, b);
-  const float2 a3b3 = mul2(a3, b3);
-  const float2 r2 = rcp2(mul2(a3b3, ab));
-  const float2 e = mul2(mul2(splat(kPiF), a3b3), r2);
+  const float2 e = mul2(splat(kPiF), rcp2(mul2(a, b)));  // pi / (a b)
   const float2 sr = fma2(a, splat(cw), splat(-czw));
   const float2 s = make_float2(__saturatef(sr.x), __saturatef(sr.y));
   const float2 w = fma2(mul2(s, s), fma2(s, splat(2.0f), splat(-3.0f)), splat(1.0f));  // 1 - s^2 (3 - 2s)
   const float2 slope = mul2(mul2(s, fma2(s, splat(-1.0f), splat(1.0f))), splat(-6.0f * cw));
-  const float2 nalong = mul2(mul2(fma2(b2, splat(-1.0f), a2), onept2), r1);  // -along
-  const float2 inv_sine = mul2(mul2(onept2, a2b2), r1);
+  const float2 u = mul2(onept2, r1);
+  const float2 nalong = mul2(fma2(bb, splat(-1.0f), a2), u);  // -along
   Pair2 p;
-  p.coef = fma2(w, nalong, mul2(mul2(e, slope), inv_sine));
-  p.curv = mul2(mul2(mul2(add2(a3, b3), ab), r2), w);
+  p.coef = fma2(w, nalong, mul2(mul2(e, slope), mul2(a2b2, u)));  // a2 b2 u = 1 / sine
+  p.curv = mul2(mul2(add2(a3, b3), rcp2(mul2(a3, b3))), w);       // (1/a3 + 1/b3) w
   p.energy = mul2(e, w);
   return p;
 }
