@@ -54,8 +54,8 @@ def test_near_rows_large_against_c_oracle(engine, ops32, ops64, precision):
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 @pytest.mark.parametrize("group,count", [("C2", 120000), ("D3", 60000), ("T", 40000), ("I", 20000)])
 def test_chart_grid_path_across_groups(engine, ops32, ops64, group, count, precision):
-    """Cutoffs below 0.5 rad take the shell and chart-grid path; above, the dense path
-    (the small-N cases above). Each group's grid path against the C oracle."""
+    """Cutoffs below 0.5 rad take the shell and chart-grid path in both modes; the small-N
+    cases above take the dense path. Each group's grid path against the C oracle."""
     gid = GROUPS.index(group)
     ops = ops32[group] if precision == "fp32" else ops64[group]
     with engine.haar(group, count, 31, precision=precision) as grid:
@@ -65,6 +65,22 @@ def test_chart_grid_path_across_groups(engine, ops32, ops64, group, count, preci
                                                                                      f32=False)
     assert qvm.near_radius(count, len(ops), 20)[0] < 0.5
     compare(rows, cref.near_rows(q, ops, 20), precision)
+
+
+@pytest.mark.parametrize("group,count", [("C2", 20000), ("O", 4000), ("D6", 3300), ("I", 1800)])
+def test_grid_path_wide_cutoffs(engine, ops32, group, count):
+    """FP32 mode keeps the chart grid for cutoffs of 0.5 to 0.9 rad when the sample has
+    more than 1e8 image pairs (its gather walks exact chart balls); these samples take it,
+    checked against the C oracle."""
+    gid = GROUPS.index(group)
+    ops = ops32[group]
+    r = qvm.near_radius(count, len(ops), 20)[0]
+    assert 0.5 <= r < 0.9 and count * count * len(ops) > 1e8
+    with engine.haar(group, count, 41) as grid:
+        grid.relax(0, neighbourhood=20)
+        rows = grid.debug_rows(0)
+        q = grid.quaternions.astype(np.float64)
+    compare(rows, cref.near_rows(q, ops, 20), "fp32")
 
 
 @pytest.mark.parametrize("group,count", [("O", 1000), ("D6", 1000), ("C2", 800)])

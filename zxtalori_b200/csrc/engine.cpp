@@ -17,7 +17,13 @@ constexpr uint32_t kMaxCount = 10000000;          // hopf.max_count (src/hopf.zi
 constexpr double kFullMeasurePairs = 5e10;        // src/engine.zig:1123
 constexpr uint32_t kSpacingAllPairs = 20000;      // src/engine.zig:1126
 constexpr double kSpacingDelta = 4;               // src/engine.zig:1127
-constexpr double kDenseRadius = 0.5;              // cutoffs from here on use the dense near field
+// Near field over every image ("dense") or over the chart grid. FP64 mode: dense from a
+// 0.5 rad cutoff on. FP32 mode (the gather walks exact chart balls): dense from 0.9 rad on,
+// or from 0.5 rad for samples of at most 1e8 image pairs, where the grid's fixed cost and
+// few warps lose to testing every image (measured on B200 over C2..I, r = 0.57..0.98).
+constexpr double kDenseRadius = 0.5;
+constexpr double kDenseRadius32 = 0.9;
+constexpr double kDenseSmallPairs = 1e8;
 constexpr const char* kVersion = "0.3.0";
 
 std::mutex g_tables_mutex;
@@ -89,7 +95,9 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   chord_ = 2.0 * std::sin(radius_ / 2.0);
   // Wide cutoffs: every image is tested (the shell holds most images anyway, and images
   // near the chart's far pole spread the chart box until the grid degenerates).
-  dense_ = radius_ >= kDenseRadius;
+  const double image_pairs = (double)n * n * host_group_order(gid_);
+  dense_ = prec == kFP64 ? radius_ >= kDenseRadius
+                         : radius_ >= kDenseRadius32 || (radius_ >= kDenseRadius && image_pairs <= kDenseSmallPairs);
   if (dense_) {
     plan_ = plan_pairs(n, host_group_order(gid_), 1.0, sms);
     if (plan_.chunks > 1) partial_.ensure((size_t)plan_.chunks * n);

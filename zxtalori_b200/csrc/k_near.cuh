@@ -609,8 +609,8 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
       for (int h = 0; h < kNearTile / 64; ++h) {
         // Lane l loads elements 64h + 2l and 64h + 2l + 1 (slot 32h + l) and writes the slot
         // whole. An element past the batch's end is a blank site: at the origin,
-        // dm2 = |x|^2 ~ 1 lies beyond every cutoff of the chart-grid path (r < 0.5 rad,
-        // cut2 < 0.25), and its code matches no source.
+        // dm2 = |x|^2 ~ 1 lies beyond every cutoff of the chart-grid path (r < 0.9 rad,
+        // cut2 < 0.76), and its code matches no source.
         const int el = 64 * h + 2 * lane;
         const uint32_t e = tb + el;
         uint32_t kin;
