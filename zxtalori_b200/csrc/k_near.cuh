@@ -649,25 +649,22 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
       if (live) {
 #pragma unroll
         for (int m = 0; m < kNearSlots; ++m) {
+          // No branches in the slot: sites past the batch's end are blank and sites beyond the
+          // cutoff contribute zero, so every slot runs the same arithmetic and the compiler
+          // can overlap consecutive slots.
           const int u = sub + kNearSub * m;  // elements 2u and 2u + 1
           const int first = 2 * u;
-          if (first >= count) break;
           const float4 A = T.wx[u], B = T.yz[u];
           const float2 mw = fma2(make_float2(A.x, A.y), splat(-1.0f), xw);
           const float2 mx = fma2(make_float2(A.z, A.w), splat(-1.0f), xx);
           const float2 my = fma2(make_float2(B.x, B.y), splat(-1.0f), xy);
           const float2 mz = fma2(make_float2(B.z, B.w), splat(-1.0f), xz);
           const float2 dm2 = fma2(mw, mw, fma2(mx, mx, fma2(my, my, mul2(mz, mz))));
-          if (dm2.x > cut2 && dm2.y > cut2) continue;
           const float4 M = T.nc[u];
           const uint32_t c0 = __float_as_uint(M.z), c1 = __float_as_uint(M.w);
+          // The thread's own source: no force; its identity image is no neighbour.
           const bool own0 = ((c0 ^ i) & ~kIdentityBit) == 0, own1 = ((c1 ^ i) & ~kIdentityBit) == 0;
-          const bool own = own0 || own1;
-          float n0 = dm2.x, n1 = dm2.y;
-          if (own) {  // the thread's own source: no force; its identity image is no neighbour
-            if (own0 && c0 != i) n0 = 4.0f;
-            if (own1 && c1 != i) n1 = 4.0f;
-          }
+          const float n0 = (own0 && c0 != i) ? 4.0f : dm2.x, n1 = (own1 && c1 != i) ? 4.0f : dm2.y;
           if (TRACK) {
             if (n0 < best) {
               best = n0;
@@ -686,7 +683,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
           const float2 dmc = make_float2(fminf(dm2.x, cut_hi), fminf(dm2.y, cut_hi));
           const float2 dp2 = fma2(dmc, splat(-1.0f), add2(xn, make_float2(M.x, M.y)));
           Pair2 pr = near_pair32x2<SHORT>(dmc, dp2, cw, czw);
-          if (own) {
+          {
             const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
             pr.coef = mul2(pr.coef, keep);
             pr.curv = mul2(pr.curv, keep);
@@ -821,85 +818,126 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near64(const double4* __res
 }
 
 // ------------------------------------------------------------------ dense near field
-// Wide cutoffs (r >= 0.5 rad: few images, or low-order groups at small N, where the chart
-// grid degenerates because images near the far pole spread the chart box) are summed over
-// every image like all pairs, with the same near-field semantics: the near twin of each
-// image (y or -y) counts when its chord is within the cutoff, the windowed pair applies, the
-// own orbit is excluded from forces and its non-identity images bound the nearest.
-template <bool TRACK, bool CHECK, bool SHORT>
-__device__ __forceinline__ void dense32_tile(const float4 x, const float4* tile, int count, int i, int j0, int k, int n,
-                                             float cut2, float cz, float cw, float& sw, float& sx, float& sy, float& sz,
-                                             float& sc, float& se, float& best, int& best_at) {
-  for (int t = 0; t < count; ++t) {
-    const float4 y = tile[t];
-    const float mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
-    const float pw = x.x + y.x, px = x.y + y.y, py = x.z + y.z, pz = x.w + y.w;
-    const float dm2 = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
-    const float dp2 = fmaf(pw, pw, fmaf(px, px, fmaf(py, py, pz * pz)));
-    const bool minus = dm2 <= dp2;
-    const float nearv = minus ? dm2 : dp2;
-    if (nearv > cut2) continue;
-    if (CHECK && j0 + t == i) {
-      if (k != 0 && nearv < best) {
-        best = nearv;
-        if (TRACK) best_at = k * n + j0 + t;
+// Wide cutoffs on small samples (and FP64 mode from r = 0.5 rad on) are summed over every
+// image like all pairs, with the same near-field semantics: the near twin of each image
+// (y or -y) counts when its chord is within the cutoff, the windowed pair applies, the own
+// orbit is excluded from forces and its non-identity images bound the nearest. FP32 mode
+// uses the all-pairs tile (pairs of images, packed f32x2 arithmetic, near twin by the sign
+// of x . y): a site beyond the cutoff is evaluated at the 1.25 r chord, where the window is
+// exactly zero, and the nearest chord is reset to 4 when no site is within the cutoff.
+template <bool TRACK, bool MASKED, bool SHORT>
+__device__ __forceinline__ void dense32_tile(const float4 x, float nx2, const PairSlots& S, int count, int i, int j0,
+                                             int k, int n, float cut_hi, float cw, float czw, float2& sw, float2& sx,
+                                             float2& sy, float2& sz, float2& sc, float2& se, float& best,
+                                             int& best_at) {
+  const float2 xw = splat(x.x), xx = splat(x.y), xy = splat(x.z), xz = splat(x.w), xn = splat(nx2);
+  const int slots = (count + 1) >> 1;
+#pragma unroll 2
+  for (int u = 0; u < slots; ++u) {
+    const float4 A = S.wx[u], B = S.yz[u];
+    const float2 yw = make_float2(A.x, A.y), yx = make_float2(A.z, A.w);
+    const float2 yy = make_float2(B.x, B.y), yz = make_float2(B.z, B.w);
+    const float2 dot = fma2(xw, yw, fma2(xx, yx, fma2(xy, yy, mul2(xz, yz))));
+    const float2 ms = make_float2(dot.x >= 0.f ? -1.f : 1.f, dot.y >= 0.f ? -1.f : 1.f);
+    const float2 dw = fma2(ms, yw, xw), dx = fma2(ms, yx, xx), dy = fma2(ms, yy, xy), dz = fma2(ms, yz, xz);
+    const float2 nearv = fma2(dw, dw, fma2(dx, dx, fma2(dy, dy, mul2(dz, dz))));
+    float n0 = nearv.x, n1 = nearv.y;
+    float2 keep = splat(1.0f);
+    if (MASKED) {
+      const int j = j0 + 2 * u;
+      const bool own0 = j == i, own1 = j + 1 == i, pad1 = 2 * u + 1 >= count;
+      if (own0 && k == 0) n0 = 4.0f;
+      if ((own1 && k == 0) || pad1) n1 = 4.0f;
+      keep = make_float2(own0 ? 0.f : 1.f, (own1 || pad1) ? 0.f : 1.f);
+    }
+    if (TRACK) {
+      if (n0 < best) {
+        best = n0;
+        best_at = k * n + j0 + 2 * u;
       }
-      continue;
+      if (n1 < best) {
+        best = n1;
+        best_at = k * n + j0 + 2 * u + 1;
+      }
+    } else {
+      best = fminf(best, fminf(n0, n1));
     }
-    if (nearv < best) {
-      best = nearv;
-      if (TRACK) best_at = k * n + j0 + t;
+    const float2 dmc = make_float2(fminf(nearv.x, cut_hi), fminf(nearv.y, cut_hi));
+    const float2 farv = fma2(dmc, splat(-1.0f), add2(xn, S.n2[u]));
+    Pair2 p = near_pair32x2<SHORT>(dmc, farv, cw, czw);
+    if (MASKED) {
+      p.coef = mul2(p.coef, keep);
+      p.curv = mul2(p.curv, keep);
+      p.energy = mul2(p.energy, keep);
     }
-    float c, cv, e;
-    near_pair32<SHORT>(nearv, minus ? dp2 : dm2, cz, cw, c, cv, e);
-    sw = fmaf(c, minus ? mw : pw, sw);
-    sx = fmaf(c, minus ? mx : px, sx);
-    sy = fmaf(c, minus ? my : py, sy);
-    sz = fmaf(c, minus ? mz : pz, sz);
-    sc += cv;
-    se += e;
+    sw = fma2(p.coef, dw, sw);
+    sx = fma2(p.coef, dx, sx);
+    sy = fma2(p.coef, dy, sy);
+    sz = fma2(p.coef, dz, sz);
+    sc = add2(sc, p.curv);
+    se = add2(se, p.energy);
   }
 }
 
 template <bool TRACK, bool SHORT>
-__global__ void __launch_bounds__(kPairBlock) k_dense32(const float4* __restrict__ q, int n, int op_off, int jtiles,
-                                                        int total_tiles, int tiles_per_chunk, NearCut cut, Rows out,
-                                                        int stride) {
-  __shared__ float4 tile[kPairBlock];
+__global__ void __launch_bounds__(kPairBlock, 8) k_dense32(const float4* __restrict__ q, int n, int op_off, int jtiles,
+                                                           int total_tiles, int tiles_per_chunk, NearCut cut, Rows out,
+                                                           int stride) {
+  __shared__ PairSlots S;
+  __shared__ double sums[6][kPairBlock];  // FP64 row sums (shared: registers go to the pairs)
   const int i0 = blockIdx.x * kPairBlock;
   const int i = i0 + threadIdx.x;
   const bool live = i < n;
   const float4 x = live ? q[i] : make_float4(1.f, 0.f, 0.f, 0.f);
-  const float cut2 = (float)cut.cut2, cz = (float)cut.cut_z, cw = (float)cut.cut_w;
-  double yw = 0, yx = 0, yy = 0, yz = 0, fc = 0, fe = 0;
+  const float nx2 = 2.0f * fmaf(x.x, x.x, fmaf(x.y, x.y, fmaf(x.z, x.z, x.w * x.w)));
+  const float cut2 = (float)cut.cut2, cut_hi = (float)cut.cut_hi, cw = (float)cut.cut_w,
+              czw = (float)(cut.cut_z * cut.cut_w);
+  for (int c = 0; c < 6; ++c) sums[c][threadIdx.x] = 0.0;
   float best = 4.0f;
   int best_at = -1;
   const int t0 = blockIdx.y * tiles_per_chunk, t1 = min(total_tiles, t0 + tiles_per_chunk);
+  const int slot = threadIdx.x >> 1, half = threadIdx.x & 1;
   for (int tid = t0; tid < t1; ++tid) {
     const PairTile pt = pair_tile(tid, jtiles, n);
     __syncthreads();
-    if ((int)threadIdx.x < pt.count) tile[threadIdx.x] = image32(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0);
+    {
+      const float4 y = (int)threadIdx.x < pt.count ? image32(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0)
+                                                   : make_float4(1.f, 0.f, 0.f, 0.f);
+      float* wx = reinterpret_cast<float*>(&S.wx[slot]);
+      float* yz = reinterpret_cast<float*>(&S.yz[slot]);
+      wx[half] = y.x;
+      wx[2 + half] = y.y;
+      yz[half] = y.z;
+      yz[2 + half] = y.w;
+      reinterpret_cast<float*>(&S.n2[slot])[half] = 2.0f * fmaf(y.x, y.x, fmaf(y.y, y.y, fmaf(y.z, y.z, y.w * y.w)));
+    }
     __syncthreads();
     if (!live) continue;
-    float sw = 0.f, sx = 0.f, sy = 0.f, sz = 0.f, sc = 0.f, se = 0.f;
-    if (pt.j0 < i0 + kPairBlock && i0 < pt.j0 + pt.count)
-      dense32_tile<TRACK, true, SHORT>(x, tile, pt.count, i, pt.j0, pt.k, n, cut2, cz, cw, sw, sx, sy, sz, sc, se, best,
-                                       best_at);
+    float2 sw = splat(0.f), sx = splat(0.f), sy = splat(0.f), sz = splat(0.f), sc = splat(0.f), se = splat(0.f);
+    const bool masked = (pt.j0 < i0 + kPairBlock && i0 < pt.j0 + pt.count) || (pt.count & 1);
+    if (masked)
+      dense32_tile<TRACK, true, SHORT>(x, nx2, S, pt.count, i, pt.j0, pt.k, n, cut_hi, cw, czw, sw, sx, sy, sz, sc, se,
+                                       best, best_at);
     else
-      dense32_tile<TRACK, false, SHORT>(x, tile, pt.count, i, pt.j0, pt.k, n, cut2, cz, cw, sw, sx, sy, sz, sc, se,
-                                        best, best_at);
-    yw += sw;
-    yx += sx;
-    yy += sy;
-    yz += sz;
-    fc += sc;
-    fe += se;
+      dense32_tile<TRACK, false, SHORT>(x, nx2, S, pt.count, i, pt.j0, pt.k, n, cut_hi, cw, czw, sw, sx, sy, sz, sc,
+                                        se, best, best_at);
+    sums[0][threadIdx.x] += (double)sw.x + (double)sw.y;
+    sums[1][threadIdx.x] += (double)sx.x + (double)sx.y;
+    sums[2][threadIdx.x] += (double)sy.x + (double)sy.y;
+    sums[3][threadIdx.x] += (double)sz.x + (double)sz.y;
+    sums[4][threadIdx.x] += (double)sc.x + (double)sc.y;
+    sums[5][threadIdx.x] += (double)se.x + (double)se.y;
   }
   if (!live) return;
+  if (best > cut2) {  // no image within the cutoff
+    best = 4.0f;
+    best_at = -1;
+  }
   const size_t at = (size_t)blockIdx.y * stride + i;
-  const double3 f = force_from_differences(to_d4(x), make_double4(yw, yx, yy, yz));
-  out.force[at] = make_double4(f.x, f.y, f.z, fc);
-  out.energy[at] = fe;
+  const double3 f = force_from_differences(
+      to_d4(x), make_double4(sums[0][threadIdx.x], sums[1][threadIdx.x], sums[2][threadIdx.x], sums[3][threadIdx.x]));
+  out.force[at] = make_double4(f.x, f.y, f.z, sums[4][threadIdx.x]);
+  out.energy[at] = sums[5][threadIdx.x];
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;
 }
