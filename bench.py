@@ -407,7 +407,7 @@ def run_ours(args, dist):
     t64 = dist.reduce(out64[0], "max")
     fp64_value = dist.reduce(k64 * EVALS_PER_PASS, "sum") / (t64 / 1e3)
     # End to end through the public API.
-    e2e_value, lat, _ = e2e_requests(zo, seed, requests=2)
+    e2e_value, lat, _ = e2e_requests(zo, seed, requests=4)
     e2e_value = dist.reduce(e2e_value, "sum")
     if dist.rank != 0:
         return 0

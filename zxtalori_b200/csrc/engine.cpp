@@ -107,9 +107,13 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   counts_.ensure((size_t)(n + 1) * 4);
   offsets_.ensure((size_t)(n + 1) * 4);
   shell_mask_.ensure((size_t)n * sizeof(uint4));
+  rim_list_.ensure((size_t)n * sizeof(uint32_t));
+  rim_q_.ensure((size_t)n * sizeof(float4));
+  rim_count_.ensure(sizeof(uint32_t));
   scan_tmp_.ensure(4096 * 4);
   ZO_CUDA(launch_shell_count(prec, q32, q64, n, gid_, s_margin_, counts_.as<uint32_t>(), offsets_.as<uint32_t>(),
-                             scan_tmp_.as<uint32_t>(), s));
+                             scan_tmp_.as<uint32_t>(), shell_mask_.as<uint4>(), rim_list_.as<uint32_t>(),
+                             rim_q_.as<float4>(), rim_count_.as<uint32_t>(), s));
   uint32_t total = 0;
   ZO_CUDA(cudaMemcpyAsync(&total, offsets_.as<uint32_t>() + n, 4, cudaMemcpyDeviceToHost, s));
   ZO_CUDA(cudaStreamSynchronize(s));
@@ -190,6 +194,9 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
   L.offsets = offsets_.as<uint32_t>();
   L.scan_tmp = scan_tmp_.as<uint32_t>();
   L.shell_mask = shell_mask_.as<uint4>();
+  L.rim_list = rim_list_.as<uint32_t>();
+  L.rim_q = rim_q_.as<float4>();
+  L.rim_count = rim_count_.as<uint32_t>();
   L.site_q32 = prec == kFP64 ? nullptr : site_q_.as<float4>();
   L.site_q64 = prec == kFP64 ? site_q_.as<double4>() : nullptr;
   L.site_code = site_code_.as<uint32_t>();

@@ -17,6 +17,8 @@
 //   5. the slices' partial rows summed in slice order into each source's row.
 // Nothing is read back between passes: grid parameters live in device memory.
 #pragma once
+#include <algorithm>
+
 #include "k_common.cuh"
 #include "kernels.h"
 
@@ -57,65 +59,151 @@ __device__ __forceinline__ void unit_operators(double4* g, int off, int order, b
   __syncthreads();
 }
 
-// Counts each source's sites and records which images are sites (bit img of a 128-bit
-// mask, img = 2 operator + sign; the identity image always), so the write pass needs no
-// second classification. FP64 mode classifies in FP64 (shell.wgsl:19-22 restated); FP32
-// mode in FP32 with the float32 planes: rounding moves a decision only within ~1e-7 of the
-// widened plane, while the margin, sin(r + 1e-4) + 2e-6, leaves 1e-4 rad between it and
-// any site a zone source can reach within r.
-template <bool FP64>
-__global__ void __launch_bounds__(256) k_shell_count(const float4* __restrict__ q32, const double4* __restrict__ q64,
-                                                     int n, int gid, double s_margin, uint32_t* __restrict__ counts,
-                                                     uint4* __restrict__ masks) {
-  __shared__ double4 g64[FP64 ? 60 : 1];
-  __shared__ float4 g32[60];
+// Which images of each source are sites: bit img of a 128-bit mask (img = 2 operator +
+// sign; the identity image always), so the write pass needs no second classification, and
+// the source's site count.
+//
+// FP64 mode: one thread per source, FP64 classification (shell.wgsl:19-22 restated).
+__global__ void __launch_bounds__(256) k_shell_count64(const double4* __restrict__ q64, int n, int gid, double s_margin,
+                                                       uint32_t* __restrict__ counts, uint4* __restrict__ masks) {
+  __shared__ double4 g64[60];
   const int off = c_group_offset[gid], order = c_group_order[gid];
-  for (int k = threadIdx.x; k < order; k += blockDim.x) {
-    if (FP64) g64[k] = normalize4(c_ops64[off + k]);
-    else g32[k] = to_f4(normalize4(c_ops32[off + k]));
-  }
+  for (int k = threadIdx.x; k < order; k += blockDim.x) g64[k] = normalize4(c_ops64[off + k]);
   __syncthreads();
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const int poff = c_plane_offset[gid], planes = 2 * order - 1;
   uint32_t w[4] = {1u, 0u, 0u, 0u};  // the identity image is always a (core) site
-  if (FP64) {
-    const double margin = s_margin + 2e-6;
-    const double4 orig = normalize4(q64[j]);
-    if (on_rim(orig, poff, planes, true, margin)) {
-      for (int img = 1; img < 2 * order; ++img) {
-        const double4 y = shell_image(orig, g64[img / 2], img & 1);
-        if (y.x > -0.9999999 && inside_planes(y, poff, planes, true, margin)) w[img >> 5] |= 1u << (img & 31);
-      }
+  const double margin = s_margin + 2e-6;
+  const double4 orig = normalize4(q64[j]);
+  if (on_rim(orig, poff, planes, true, margin)) {
+    for (int img = 1; img < 2 * order; ++img) {
+      const double4 y = shell_image(orig, g64[img / 2], img & 1);
+      // Plane img - 1 (the bisector of the identity and the image's own operator) rejects
+      // almost every image far from the zone: test it first.
+      if (y.x > -0.9999999 && dot4(y, c_planes64[poff + img - 1]) >= -margin &&
+          inside_planes(y, poff, planes, true, margin))
+        w[img >> 5] |= 1u << (img & 31);
     }
-  } else {
-    const float margin = (float)(s_margin + 2e-6);
-    const float4 orig = to_f4(normalize4(to_d4(q32[j])));
-    bool rim = false;
+  }
+  counts[j] = (uint32_t)(__popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]));
+  masks[j] = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// FP32 mode, in FP32 with the float32 planes: rounding moves a decision only within ~1e-7
+// of the widened plane, while the margin, sin(r + 1e-4) + 2e-6, leaves 1e-4 rad between it
+// and any site a zone source can reach within r. Three steps, so that the few rim sources'
+// images spread over whole warps: (1) the rim test per source, listing the rim sources and
+// their positions; (2) a warp per rim source, its lanes over the images, setting the mask
+// bit of each site; (3) the counts.
+__global__ void __launch_bounds__(256) k_shell_rim32(const float4* __restrict__ q32, int n, int gid, float margin,
+                                                     uint4* __restrict__ masks, uint32_t* __restrict__ rim_list,
+                                                     float4* __restrict__ rim_q, uint32_t* __restrict__ rim_count) {
+  const unsigned full = 0xffffffffu;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  bool rim = false;
+  float4 orig = make_float4(1.f, 0.f, 0.f, 0.f);
+  if (j < n) {
+    const int poff = c_plane_offset[gid], planes = 2 * c_group_order[gid] - 1;
+    orig = q32[j];  // unit to 1e-7 (folded in FP64), far inside the margin's slack
     for (int k = 0; k < planes && !rim; ++k) {
       const float4 h = c_planes32[poff + k];
       rim = fmaf(orig.x, h.x, fmaf(orig.y, h.y, fmaf(orig.z, h.z, orig.w * h.w))) <= margin;
     }
+    masks[j] = make_uint4(1u, 0u, 0u, 0u);  // the identity image is always a (core) site
+  }
+  const unsigned m = __ballot_sync(full, rim);  // one atomic per warp for its rim sources
+  if (m) {
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(rim_count, (uint32_t)__popc(m));
+    base = __shfl_sync(full, base, leader);
     if (rim) {
-      for (int img = 1; img < 2 * order; ++img) {
-        const float4 a = orig, b = g32[img / 2];
-        float4 y = make_float4(a.x * b.x - a.y * b.y - a.z * b.z - a.w * b.w,
-                               a.x * b.y + a.y * b.x + a.z * b.w - a.w * b.z,
-                               a.x * b.z - a.y * b.w + a.z * b.x + a.w * b.y,
-                               a.x * b.w + a.y * b.z - a.z * b.y + a.w * b.x);
+      const uint32_t at = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+      rim_list[at] = (uint32_t)j;
+      rim_q[at] = orig;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_shell_classify32(int gid, float margin, const uint32_t* __restrict__ rim_list,
+                                                          const float4* __restrict__ rim_q,
+                                                          const uint32_t* __restrict__ rim_count, uint4* masks) {
+  // The group's operators and planes in shared memory: lanes read different ones at once,
+  // which constant memory would serialise.
+  __shared__ float4 g32[60];
+  __shared__ float4 h32[119];
+  const int off = c_group_offset[gid], order = c_group_order[gid];
+  const int poff = c_plane_offset[gid], planes = 2 * order - 1;
+  for (int k = threadIdx.x; k < order; k += blockDim.x) g32[k] = to_f4(normalize4(c_ops32[off + k]));
+  for (int k = threadIdx.x; k < planes; k += blockDim.x) h32[k] = c_planes32[poff + k];
+  __syncthreads();
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const uint32_t rims = *rim_count;
+  auto plane_dot = [&](const float4& y, int k) {
+    const float4 h = h32[k];
+    return fmaf(y.x, h.x, fmaf(y.y, h.y, fmaf(y.z, h.z, y.w * h.w)));
+  };
+  // One warp per rim source (grid-stride), its lanes over the images 1 .. 2|K|-1, 32 at a
+  // time. Image img = 2j + sign of x is y = +-x g_j, and plane img - 1 is the bisector of the
+  // identity and +-g_j: its dot with y is proportional to y_w - x_w, negative unless y lies
+  // near the zone. Each lane tests that plane alone; the few images that pass are checked
+  // against every plane by the whole warp together.
+  for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rims; r += (gridDim.x * blockDim.x) >> 5) {
+    const float4 a = rim_q[r];
+    uint32_t* word = reinterpret_cast<uint32_t*>(&masks[rim_list[r]]);
+    for (int base = 1; base < 2 * order; base += 32) {
+      const int img = base + lane;
+      float4 y = make_float4(0.f, 0.f, 0.f, 0.f);
+      bool alive = false;
+      if (img < 2 * order) {
+        const float4 b = g32[img / 2];
+        y = make_float4(a.x * b.x - a.y * b.y - a.z * b.z - a.w * b.w, a.x * b.y + a.y * b.x + a.z * b.w - a.w * b.z,
+                        a.x * b.z - a.y * b.w + a.z * b.x + a.w * b.y, a.x * b.w + a.y * b.z - a.z * b.y + a.w * b.x);
         if (img & 1) y = make_float4(-y.x, -y.y, -y.z, -y.w);
-        if (!(y.x > -0.9999999f)) continue;
-        bool inside = true;
-        for (int k = 0; k < planes && inside; ++k) {
-          const float4 h = c_planes32[poff + k];
-          inside = fmaf(y.x, h.x, fmaf(y.y, h.y, fmaf(y.z, h.z, y.w * h.w))) >= -margin;
-        }
-        if (inside) w[img >> 5] |= 1u << (img & 31);
+        alive = y.x > -0.9999999f && plane_dot(y, img - 1) >= -margin;
+      }
+      unsigned survivors = __ballot_sync(full, alive);
+      while (survivors) {
+        const int src = __ffs(survivors) - 1;
+        survivors &= survivors - 1;
+        const float4 z = make_float4(__shfl_sync(full, y.x, src), __shfl_sync(full, y.y, src),
+                                     __shfl_sync(full, y.z, src), __shfl_sync(full, y.w, src));
+        bool out = false;
+        for (int k = lane; k < planes; k += 32) out |= plane_dot(z, k) < -margin;
+        if (!__any_sync(full, out) && lane == src) atomicOr(word + (img >> 5), 1u << (img & 31));
       }
     }
   }
-  counts[j] = (uint32_t)(__popc(w[0]) + __popc(w[1]) + __popc(w[2]) + __popc(w[3]));
-  if (masks) masks[j] = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+__global__ void k_shell_popc(const uint4* __restrict__ masks, int n, uint32_t* __restrict__ counts) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint4 w = masks[j];
+  counts[j] = (uint32_t)(__popc(w.x) + __popc(w.y) + __popc(w.z) + __popc(w.w));
+}
+
+// The shell's masks and counts (all three FP32 steps, or the FP64 kernel); returns the
+// number of kernels launched through `launches`.
+inline cudaError_t launch_shell_masks(int prec, const float4* q32, const double4* q64, int n, int gid,
+                                      double s_margin, uint32_t* counts, uint4* masks, uint32_t* rim_list,
+                                      float4* rim_q, uint32_t* rim_count, cudaStream_t s, int* launches) {
+  if (prec == kFP64) {
+    k_shell_count64<<<(n + 255) / 256, 256, 0, s>>>(q64, n, gid, s_margin, counts, masks);
+    *launches = 1;
+    return cudaGetLastError();
+  }
+  const float margin = (float)(s_margin + 2e-6);
+  cudaError_t e = cudaMemsetAsync(rim_count, 0, sizeof(uint32_t), s);
+  if (e) return e;
+  k_shell_rim32<<<(n + 255) / 256, 256, 0, s>>>(q32, n, gid, margin, masks, rim_list, rim_q, rim_count);
+  const int blocks = std::min((n + 7) / 8, 4096);  // a warp per rim source, at most n of them
+  k_shell_classify32<<<blocks, 256, 0, s>>>(gid, margin, rim_list, rim_q, rim_count, masks);
+  k_shell_popc<<<(n + 255) / 256, 256, 0, s>>>(masks, n, counts);
+  *launches = 3;
+  return cudaGetLastError();
 }
 
 // Writes the sites of each source at its scanned offset: the rebuilt image quaternion
@@ -1026,9 +1114,12 @@ cudaError_t launch_dense_near(int prec, bool track, bool short_atan, const float
 // ------------------------------------------------------------------ the pass
 // Site count of a shell pass (offsets[n] after the scan), for sizing the workspace.
 cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, int n, int gid, double s_margin,
-                               uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, cudaStream_t s) {
-  if (prec == kFP64) k_shell_count<true><<<(n + 255) / 256, 256, 0, s>>>(q32, q64, n, gid, s_margin, counts, nullptr);
-  else k_shell_count<false><<<(n + 255) / 256, 256, 0, s>>>(q32, q64, n, gid, s_margin, counts, nullptr);
+                               uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, uint4* masks,
+                               uint32_t* rim_list, float4* rim_q, uint32_t* rim_count, cudaStream_t s) {
+  int launches = 0;
+  cudaError_t e = launch_shell_masks(prec, q32, q64, n, gid, s_margin, counts, masks, rim_list, rim_q, rim_count, s,
+                                     &launches);
+  if (e) return e;
   return launch_scan(counts, offsets, n, nullptr, scan_tmp, s);
 }
 
@@ -1037,9 +1128,11 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   const bool fp64 = L.prec == kFP64;
   const int tb = 256;
   // 1. shell
-  if (fp64) k_shell_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.s_margin, L.counts, L.shell_mask);
-  else k_shell_count<false><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.s_margin, L.counts, L.shell_mask);
-  cudaError_t e = launch_scan(L.counts, L.offsets, n, nullptr, L.scan_tmp, s);
+  int shell_launches = 0;
+  cudaError_t e = launch_shell_masks(L.prec, L.q32, L.q64, n, L.gid, L.s_margin, L.counts, L.shell_mask, L.rim_list,
+                                     L.rim_q, L.rim_count, s, &shell_launches);
+  if (e) return e;
+  e = launch_scan(L.counts, L.offsets, n, nullptr, L.scan_tmp, s);
   if (e) return e;
   if (fp64)
     k_shell_write<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.shell_mask, L.offsets, L.capacity,
@@ -1092,9 +1185,10 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   }
   probe_mark(s);
   k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(L.partial, n, slices, n, (const int*)L.src_perm, L.out, L.track ? 1 : 0);
-  // shell count, shell write, grid, cell count, scatter, bucket sort, site gather, source
-  // count, scatter, bucket sort, gather, reduce (scans counted by launch_scan; memsets aside)
-  probe_count(12);
+  // shell masks (1 or 3), shell write, grid, cell count, scatter, bucket sort, site gather,
+  // source count, scatter, bucket sort, gather, reduce (scans counted by launch_scan;
+  // memsets aside)
+  probe_count(11 + shell_launches);
   return cudaGetLastError();
 }
 

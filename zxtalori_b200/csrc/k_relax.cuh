@@ -259,13 +259,37 @@ __global__ void __launch_bounds__(kRelaxBlock) k_row_summary(Rows rows, int n, d
   if (!last_block(&out->ticket)) return;
   double s[2];
   sum_partials<2>(partials, gridDim.x, s);
+  // The blocks' minima, reduced by the whole block: smallest chord, then lowest row (rows
+  // grow with the block index, so this is the first block holding the minimum).
+  double b = 4.0;
+  int a = -1;
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+    const double v = near_partials[k];
+    const int r = near_rows[k];
+    if (v < b || (v == b && r >= 0 && (a < 0 || r < a))) {
+      b = v;
+      a = r;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    const double b2 = __shfl_xor_sync(0xffffffffu, b, o);
+    const int a2 = __shfl_xor_sync(0xffffffffu, a, o);
+    if (b2 < b || (b2 == b && a2 >= 0 && (a < 0 || a2 < a))) {
+      b = b2;
+      a = a2;
+    }
+  }
+  __syncthreads();  // wb / wa reused
+  if ((threadIdx.x & 31) == 0) {
+    wb[threadIdx.x >> 5] = b;
+    wa[threadIdx.x >> 5] = a;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    double b = 4.0;
-    int a = -1;
-    for (int k = 0; k < (int)gridDim.x; ++k)
-      if (near_partials[k] < b) {
-        b = near_partials[k];
-        a = near_rows[k];
+    for (int k = 1; k < kRelaxBlock / 32; ++k)
+      if (wb[k] < b || (wb[k] == b && wa[k] >= 0 && (a < 0 || wa[k] < a))) {
+        b = wb[k];
+        a = wa[k];
       }
     out->energy = s[0];
     out->force2 = s[1];

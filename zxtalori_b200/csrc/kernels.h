@@ -52,6 +52,9 @@ struct NearLaunch {
   const double4* q64;
   uint32_t *counts, *offsets, *scan_tmp;
   uint4* shell_mask;  // per source: which images are sites (bit 2 operator + sign)
+  uint32_t* rim_list;  // FP32 shell: rim sources, their normalised positions, their count
+  float4* rim_q;
+  uint32_t* rim_count;
   float4* site_q32;
   double4* site_q64;
   uint32_t *site_code, *site_img, *site_cell, *site_rank;
@@ -73,7 +76,8 @@ cudaError_t launch_dense_near(int prec, bool track, bool short_atan, const float
                               int gid, const PairsPlan& pl, double cut2, double chord, double cut_z, double cut_w,
                               Rows partial, Rows out, cudaStream_t s);
 cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, int n, int gid, double s_margin,
-                               uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, cudaStream_t s);
+                               uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, uint4* masks,
+                               uint32_t* rim_list, float4* rim_q, uint32_t* rim_count, cudaStream_t s);
 
 // Relaxation step pieces.
 cudaError_t launch_relax_stats(Rows rows, const double4* prev_f, const double4* prev_d, int n, int fixed,
