@@ -528,7 +528,7 @@ __device__ __forceinline__ bool row_run(const WarpBox& b, const NearGrid& g, con
 constexpr int kNearSub = 32 / kNearGroup;          // lanes per source
 constexpr int kNearTile = 128;                      // sites per tile
 constexpr int kNearSlots = kNearTile / (2 * kNearSub);  // site pairs per lane and tile
-constexpr int kNearMerge = 16 / kNearSlots;          // tiles between FP64 merges (16 pairs)
+constexpr int kNearMerge = kNearSlots >= 16 ? 1 : 16 / kNearSlots;  // tiles between FP64 merges
 
 // One tile. Slot u holds elements 2u and 2u + 1; lane (source s, sub-lane j) evaluates
 // slots j + kNearSub m, m < kNearSlots.
