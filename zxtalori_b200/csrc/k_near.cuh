@@ -547,6 +547,7 @@ struct NearTile {
 struct NearWalk {
   float cen[kNearGroup][3];
   float rad[kNearGroup];  // < 0: no source in this place
+  uint32_t src[kNearGroup];  // the sources' indices (codes' low bits); 0xfffffffe when absent
   int clo[3], chi[3];     // cells of the balls' bounding box
   float lower[3], cells_per_unit;
   int sdim;
@@ -595,6 +596,70 @@ __device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], floa
   sw = sx = sy = sz = sc = se = splat(0.f);
 }
 
+// The slots of one tile for one lane of k_near32: slot u = sub + kNearSub m holds elements
+// 2u and 2u + 1. No branches in the slot: sites past the batch's end are blank and sites
+// beyond the cutoff contribute zero, so every slot runs the same arithmetic and the compiler
+// can overlap consecutive slots. OWN: the tile may hold images of the warp's sources, so
+// each site's source is tested (the thread's own source gets no force from its images, and
+// its identity image is no neighbour); without it that test is left out.
+template <bool TRACK, bool SHORT, bool OWN>
+__device__ __forceinline__ void near_slots(const NearTile& T, int sub, uint32_t i, float2 xw, float2 xx, float2 xy,
+                                           float2 xz, float2 xn, float cut_hi, float cw, float czw, float2& sw,
+                                           float2& sx, float2& sy, float2& sz, float2& sc, float2& se, float& best,
+                                           int& best_at) {
+#pragma unroll
+  for (int m = 0; m < kNearSlots; ++m) {
+    const int u = sub + kNearSub * m;
+    const int first = 2 * u;
+    const float4 A = T.wx[u], B = T.yz[u];
+    const float2 mw = fma2(make_float2(A.x, A.y), splat(-1.0f), xw);
+    const float2 mx = fma2(make_float2(A.z, A.w), splat(-1.0f), xx);
+    const float2 my = fma2(make_float2(B.x, B.y), splat(-1.0f), xy);
+    const float2 mz = fma2(make_float2(B.z, B.w), splat(-1.0f), xz);
+    const float2 dm2 = fma2(mw, mw, fma2(mx, mx, fma2(my, my, mul2(mz, mz))));
+    const float4 M = T.nc[u];
+    bool own0 = false, own1 = false;
+    float n0 = dm2.x, n1 = dm2.y;
+    if (OWN) {
+      const uint32_t c0 = __float_as_uint(M.z), c1 = __float_as_uint(M.w);
+      own0 = ((c0 ^ i) & ~kIdentityBit) == 0;
+      own1 = ((c1 ^ i) & ~kIdentityBit) == 0;
+      if (own0 && c0 != i) n0 = 4.0f;
+      if (own1 && c1 != i) n1 = 4.0f;
+    }
+    if (TRACK) {
+      if (n0 < best) {
+        best = n0;
+        best_at = (int)T.at[first];
+      }
+      if (n1 < best) {
+        best = n1;
+        best_at = (int)T.at[first + 1];
+      }
+    } else {
+      best = fminf(best, fminf(n0, n1));
+    }
+    // A site beyond the cutoff takes the chord at 1.25 r: its terms stay finite (a site
+    // nearer the antipode, dm2 > 2, would drive the half-angle out of range) and the
+    // window makes them exactly zero.
+    const float2 dmc = make_float2(fminf(dm2.x, cut_hi), fminf(dm2.y, cut_hi));
+    const float2 dp2 = fma2(dmc, splat(-1.0f), add2(xn, make_float2(M.x, M.y)));
+    Pair2 pr = near_pair32x2<SHORT>(dmc, dp2, cw, czw);
+    if (OWN) {
+      const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
+      pr.coef = mul2(pr.coef, keep);
+      pr.curv = mul2(pr.curv, keep);
+      pr.energy = mul2(pr.energy, keep);
+    }
+    sw = fma2(pr.coef, mw, sw);
+    sx = fma2(pr.coef, mx, sx);
+    sy = fma2(pr.coef, my, sy);
+    sz = fma2(pr.coef, mz, sz);
+    sc = add2(sc, pr.curv);
+    se = add2(se, pr.energy);
+  }
+}
+
 template <bool TRACK, bool SHORT>
 __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __restrict__ q, int n,
                                                               const uint32_t* __restrict__ src_perm,
@@ -635,6 +700,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
       const int s = lane / kNearSub;
       for (int a = 0; a < 3; ++a) W.cen[s][a] = c[a];
       W.rad[s] = live ? rho : -1.0f;
+      W.src[s] = live ? i : 0xfffffffeu;
     }
     if (lane == 0) {
       for (int a = 0; a < 3; ++a) {
@@ -692,6 +758,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
     int k = 0;  // the run of this lane's next element: the first lane with incl > e
     for (uint32_t tb = 0; tb < total; tb += kNearTile) {
       const int count = (int)min((uint32_t)kNearTile, total - tb);
+      bool mine = false;  // this lane loaded an image of one of the warp's sources
       __syncwarp();
 #pragma unroll
       for (int h = 0; h < kNearTile / 64; ++h) {
@@ -732,58 +799,21 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
                                  2.0f * fmaf(y[1].x, y[1].x, fmaf(y[1].y, y[1].y, fmaf(y[1].z, y[1].z, y[1].w * y[1].w))),
                                  __uint_as_float(code[0]), __uint_as_float(code[1]));
         if (TRACK) reinterpret_cast<uint2*>(T.at)[slot] = make_uint2(site[0], site[1]);
+#pragma unroll
+        for (int s2 = 0; s2 < kNearGroup; ++s2)
+          mine |= ((code[0] & ~kIdentityBit) == W.src[s2]) | ((code[1] & ~kIdentityBit) == W.src[s2]);
       }
+      // Whether the tile holds an image of one of the warp's sources (rare): only then does
+      // the slot loop test each site's source.
+      const bool tile_own = __any_sync(full, mine);
       __syncwarp();
       if (live) {
-#pragma unroll
-        for (int m = 0; m < kNearSlots; ++m) {
-          // No branches in the slot: sites past the batch's end are blank and sites beyond the
-          // cutoff contribute zero, so every slot runs the same arithmetic and the compiler
-          // can overlap consecutive slots.
-          const int u = sub + kNearSub * m;  // elements 2u and 2u + 1
-          const int first = 2 * u;
-          const float4 A = T.wx[u], B = T.yz[u];
-          const float2 mw = fma2(make_float2(A.x, A.y), splat(-1.0f), xw);
-          const float2 mx = fma2(make_float2(A.z, A.w), splat(-1.0f), xx);
-          const float2 my = fma2(make_float2(B.x, B.y), splat(-1.0f), xy);
-          const float2 mz = fma2(make_float2(B.z, B.w), splat(-1.0f), xz);
-          const float2 dm2 = fma2(mw, mw, fma2(mx, mx, fma2(my, my, mul2(mz, mz))));
-          const float4 M = T.nc[u];
-          const uint32_t c0 = __float_as_uint(M.z), c1 = __float_as_uint(M.w);
-          // The thread's own source: no force; its identity image is no neighbour.
-          const bool own0 = ((c0 ^ i) & ~kIdentityBit) == 0, own1 = ((c1 ^ i) & ~kIdentityBit) == 0;
-          const float n0 = (own0 && c0 != i) ? 4.0f : dm2.x, n1 = (own1 && c1 != i) ? 4.0f : dm2.y;
-          if (TRACK) {
-            if (n0 < best) {
-              best = n0;
-              best_at = (int)T.at[first];
-            }
-            if (n1 < best) {
-              best = n1;
-              best_at = (int)T.at[first + 1];
-            }
-          } else {
-            best = fminf(best, fminf(n0, n1));
-          }
-          // A site beyond the cutoff takes the chord at 1.25 r: its terms stay finite (a site
-          // nearer the antipode, dm2 > 2, would drive the half-angle out of range) and the
-          // window makes them exactly zero.
-          const float2 dmc = make_float2(fminf(dm2.x, cut_hi), fminf(dm2.y, cut_hi));
-          const float2 dp2 = fma2(dmc, splat(-1.0f), add2(xn, make_float2(M.x, M.y)));
-          Pair2 pr = near_pair32x2<SHORT>(dmc, dp2, cw, czw);
-          {
-            const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
-            pr.coef = mul2(pr.coef, keep);
-            pr.curv = mul2(pr.curv, keep);
-            pr.energy = mul2(pr.energy, keep);
-          }
-          sw = fma2(pr.coef, mw, sw);
-          sx = fma2(pr.coef, mx, sx);
-          sy = fma2(pr.coef, my, sy);
-          sz = fma2(pr.coef, mz, sz);
-          sc = add2(sc, pr.curv);
-          se = add2(se, pr.energy);
-        }
+        if (tile_own)
+          near_slots<TRACK, SHORT, true>(T, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, sw, sx, sy, sz, sc, se, best,
+                                         best_at);
+        else
+          near_slots<TRACK, SHORT, false>(T, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, sw, sx, sy, sz, sc, se, best,
+                                          best_at);
       }
       if (++since == kNearMerge) {
         merge_sums(sums, sw, sx, sy, sz, sc, se);
