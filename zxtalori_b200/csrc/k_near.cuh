@@ -535,8 +535,9 @@ constexpr int kNearMerge = kNearSlots >= 16 ? 1 : 16 / kNearSlots;  // tiles bet
 struct NearTile {
   float4 wx[kNearTile / 2];  // (w, w', x, x')
   float4 yz[kNearTile / 2];  // (y, y', z, z')
-  float4 nc[kNearTile / 2];  // (2|y|^2, 2|y'|^2, code bits, code' bits)
-  uint32_t at[kNearTile];    // sorted-site index of each element
+  float2 norm[kNearTile / 2];  // (2|y|^2, 2|y'|^2), for the arctangent form only
+  uint2 code[kNearTile / 2];   // (code, code')
+  uint32_t at[kNearTile];      // sorted-site index of each element
 };
 
 // Per-warp data of the row walk, kept in shared memory (it is warp-uniform) so the hot
@@ -601,12 +602,14 @@ __device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], floa
 // beyond the cutoff contribute zero, so every slot runs the same arithmetic and the compiler
 // can overlap consecutive slots. OWN: the tile may hold images of the warp's sources, so
 // each site's source is tested (the thread's own source gets no force from its images, and
-// its identity image is no neighbour); without it that test is left out.
+// its identity image is no neighbour); without it that test is left out. SHORT: cutoffs up
+// to 0.4 rad take the chord form (near_chord_pair32x2; se then sums energy / pi), wider ones
+// the arctangent of near over far.
 template <bool TRACK, bool SHORT, bool OWN>
 __device__ __forceinline__ void near_slots(const NearTile& T, int sub, uint32_t i, float2 xw, float2 xx, float2 xy,
-                                           float2 xz, float2 xn, float cut_hi, float cw, float czw, float2& sw,
-                                           float2& sx, float2& sy, float2& sz, float2& sc, float2& se, float& best,
-                                           int& best_at) {
+                                           float2 xz, float2 xn, float cut_hi, float cw, float czw, float pk,
+                                           float2& sw, float2& sx, float2& sy, float2& sz, float2& sc, float2& se,
+                                           float& best, int& best_at) {
 #pragma unroll
   for (int m = 0; m < kNearSlots; ++m) {
     const int u = sub + kNearSub * m;
@@ -617,15 +620,14 @@ __device__ __forceinline__ void near_slots(const NearTile& T, int sub, uint32_t 
     const float2 my = fma2(make_float2(B.x, B.y), splat(-1.0f), xy);
     const float2 mz = fma2(make_float2(B.z, B.w), splat(-1.0f), xz);
     const float2 dm2 = fma2(mw, mw, fma2(mx, mx, fma2(my, my, mul2(mz, mz))));
-    const float4 M = T.nc[u];
     bool own0 = false, own1 = false;
     float n0 = dm2.x, n1 = dm2.y;
     if (OWN) {
-      const uint32_t c0 = __float_as_uint(M.z), c1 = __float_as_uint(M.w);
-      own0 = ((c0 ^ i) & ~kIdentityBit) == 0;
-      own1 = ((c1 ^ i) & ~kIdentityBit) == 0;
-      if (own0 && c0 != i) n0 = 4.0f;
-      if (own1 && c1 != i) n1 = 4.0f;
+      const uint2 c = T.code[u];
+      own0 = ((c.x ^ i) & ~kIdentityBit) == 0;
+      own1 = ((c.y ^ i) & ~kIdentityBit) == 0;
+      if (own0 && c.x != i) n0 = 4.0f;
+      if (own1 && c.y != i) n1 = 4.0f;
     }
     if (TRACK) {
       if (n0 < best) {
@@ -643,20 +645,34 @@ __device__ __forceinline__ void near_slots(const NearTile& T, int sub, uint32_t 
     // nearer the antipode, dm2 > 2, would drive the half-angle out of range) and the
     // window makes them exactly zero.
     const float2 dmc = make_float2(fminf(dm2.x, cut_hi), fminf(dm2.y, cut_hi));
-    const float2 dp2 = fma2(dmc, splat(-1.0f), add2(xn, make_float2(M.x, M.y)));
-    Pair2 pr = near_pair32x2<SHORT>(dmc, dp2, cw, czw);
-    if (OWN) {
-      const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
-      pr.coef = mul2(pr.coef, keep);
-      pr.curv = mul2(pr.curv, keep);
-      pr.energy = mul2(pr.energy, keep);
+    float2 coef;
+    if (SHORT) {
+      ChordPair2 pr = near_chord_pair32x2(dmc, cw, czw, pk);
+      coef = pr.coef;
+      if (OWN) {
+        const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
+        coef = mul2(coef, keep);
+        pr.w = mul2(pr.w, keep);
+      }
+      sc = fma2(pr.q, pr.w, sc);
+      se = fma2(pr.rab, pr.w, se);
+    } else {
+      const float2 dp2 = fma2(dmc, splat(-1.0f), add2(xn, T.norm[u]));
+      Pair2 pr = near_pair32x2<false>(dmc, dp2, cw, czw);
+      if (OWN) {
+        const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
+        pr.coef = mul2(pr.coef, keep);
+        pr.curv = mul2(pr.curv, keep);
+        pr.energy = mul2(pr.energy, keep);
+      }
+      coef = pr.coef;
+      sc = add2(sc, pr.curv);
+      se = add2(se, pr.energy);
     }
-    sw = fma2(pr.coef, mw, sw);
-    sx = fma2(pr.coef, mx, sx);
-    sy = fma2(pr.coef, my, sy);
-    sz = fma2(pr.coef, mz, sz);
-    sc = add2(sc, pr.curv);
-    se = add2(se, pr.energy);
+    sw = fma2(coef, mw, sw);
+    sx = fma2(coef, mx, sx);
+    sy = fma2(coef, my, sy);
+    sz = fma2(coef, mz, sz);
   }
 }
 
@@ -715,7 +731,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
   for (int k = 0; k < 6; ++k) sums[k][threadIdx.x] = 0.0;
   __syncwarp();
   const float cut2 = (float)cut.cut2, cut_hi = (float)cut.cut_hi, cw = (float)cut.cut_w,
-              czw = (float)(cut.cut_z * cut.cut_w);
+              czw = (float)(cut.cut_z * cut.cut_w), pk = (float)(-6.0 * kPi * cut.cut_w);
   const float nx2 = 2.0f * fmaf(x.x, x.x, fmaf(x.y, x.y, fmaf(x.z, x.z, x.w * x.w)));
   const float2 xw = splat(x.x), xx = splat(x.y), xy = splat(x.z), xz = splat(x.w), xn = splat(nx2);
   float best = 4.0f;
@@ -795,9 +811,10 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
         const int slot = 32 * h + lane;
         T.wx[slot] = make_float4(y[0].x, y[1].x, y[0].y, y[1].y);
         T.yz[slot] = make_float4(y[0].z, y[1].z, y[0].w, y[1].w);
-        T.nc[slot] = make_float4(2.0f * fmaf(y[0].x, y[0].x, fmaf(y[0].y, y[0].y, fmaf(y[0].z, y[0].z, y[0].w * y[0].w))),
-                                 2.0f * fmaf(y[1].x, y[1].x, fmaf(y[1].y, y[1].y, fmaf(y[1].z, y[1].z, y[1].w * y[1].w))),
-                                 __uint_as_float(code[0]), __uint_as_float(code[1]));
+        T.code[slot] = make_uint2(code[0], code[1]);
+        if (!SHORT)
+          T.norm[slot] = make_float2(2.0f * fmaf(y[0].x, y[0].x, fmaf(y[0].y, y[0].y, fmaf(y[0].z, y[0].z, y[0].w * y[0].w))),
+                                     2.0f * fmaf(y[1].x, y[1].x, fmaf(y[1].y, y[1].y, fmaf(y[1].z, y[1].z, y[1].w * y[1].w))));
         if (TRACK) reinterpret_cast<uint2*>(T.at)[slot] = make_uint2(site[0], site[1]);
 #pragma unroll
         for (int s2 = 0; s2 < kNearGroup; ++s2)
@@ -809,11 +826,11 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
       __syncwarp();
       if (live) {
         if (tile_own)
-          near_slots<TRACK, SHORT, true>(T, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, sw, sx, sy, sz, sc, se, best,
-                                         best_at);
+          near_slots<TRACK, SHORT, true>(T, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy, sz, sc, se,
+                                         best, best_at);
         else
-          near_slots<TRACK, SHORT, false>(T, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, sw, sx, sy, sz, sc, se, best,
-                                          best_at);
+          near_slots<TRACK, SHORT, false>(T, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy, sz, sc, se,
+                                          best, best_at);
       }
       if (++since == kNearMerge) {
         merge_sums(sums, sw, sx, sy, sz, sc, se);
@@ -851,7 +868,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
   const double3 f = force_from_differences(to_d4(x), make_double4(t[0], t[1], t[2], t[3]));
   const size_t at = (size_t)slice * stride + p;
   out.force[at] = make_double4(f.x, f.y, f.z, t[4]);
-  out.energy[at] = t[5];
+  out.energy[at] = SHORT ? kPi * t[5] : t[5];
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;
 }

@@ -224,6 +224,46 @@ __device__ __forceinline__ Pair2 near_pair32x2(float2 dm2, float2 dp2, float cw,
   return p;
 }
 
+// The terms of two windowed near-field pairs from their squared chords d alone, for cutoffs
+// r <= 0.4 rad (d <= 0.25 after the clamp at 1.25 r). For unit quaternions the angle
+// a = 2 atan(sqrt(near/far)) of quey_pair is also 2 asin(c/2), c = sqrt(d) the chord, and
+// sin a = c sqrt(1 - d/4): a = c (1 + d Pa(d)) and sin a = c (1 + d Ps(d)) with Pa, Ps the
+// quadratic fits of fit_atan.py (relative error below 1e-8 on [0, 0.25]). Neither the far
+// chord nor its reciprocal is needed. The same terms as near_pair32x2, regrouped:
+//   coefficient = [w (a2 - b2) + pi slope a2 b2 / (a b)] / (a2 b2 (sin a + 1e-9)),
+//   curvature = q w with q = (a3 + b3) / (a3 b3), energy = pi w / (a b) = pi * (rab w),
+// so the caller accumulates q w and rab w with one FMA each and multiplies the energy sum
+// by pi once. pk = -6 pi cw (the window's slope factor times pi).
+struct ChordPair2 {
+  float2 coef, q, w, rab;
+};
+__device__ __forceinline__ ChordPair2 near_chord_pair32x2(float2 d, float cw, float czw, float pk) {
+  const float2 c = sqrt2(d);
+  const float2 cd = mul2(c, d);
+  const float2 pa = fma2(fma2(splat(0x1.8d9f56p-11f), d, splat(0x1.329be0p-8f)), d, splat(0x1.555620p-5f));
+  const float2 ps = fma2(fma2(splat(-0x1.147feap-10f), d, splat(-0x1.ff3d12p-8f)), d, splat(-0x1.000042p-3f));
+  const float2 a = max2(fma2(cd, pa, c), 1e-12f);
+  const float2 sn = fma2(cd, ps, add2(c, splat(1e-9f)));  // sin a + 1e-9
+  const float2 b = fma2(a, splat(-1.0f), splat(kPiF));
+  const float2 aa = mul2(a, a), bb = mul2(b, b);
+  // b >= pi/2 (the site is the near twin), so b^2 + 1e-9 rounds to b^2: b2 = bb.
+  const float2 a2 = add2(aa, splat(1e-9f));
+  const float2 a3 = fma2(aa, a, splat(1e-9f)), b3 = fma2(bb, b, splat(1e-9f));
+  const float2 a2b2 = mul2(a2, bb);
+  const float2 r1 = rcp2(mul2(a2b2, sn));  // 1 / (a2 b2 (sin a + 1e-9))
+  ChordPair2 p;
+  p.rab = rcp2(mul2(a, b));
+  const float2 sr = fma2(a, splat(cw), splat(-czw));
+  const float2 s = make_float2(__saturatef(sr.x), __saturatef(sr.y));
+  const float2 ss = mul2(s, s);
+  p.w = fma2(ss, fma2(s, splat(2.0f), splat(-3.0f)), splat(1.0f));  // 1 - s^2 (3 - 2s)
+  const float2 slope = fma2(ss, splat(-pk), mul2(s, splat(pk)));   // pi * (-6 cw) s (1 - s)
+  const float2 g = mul2(mul2(p.rab, slope), a2b2);
+  p.coef = mul2(fma2(p.w, fma2(bb, splat(-1.0f), a2), g), r1);
+  p.q = mul2(add2(a3, b3), rcp2(mul2(a3, b3)));
+  return p;
+}
+
 // Windowed near-field pair, FP32, for a site that is the near twin (dm2 <= cut < 2 <= dp2,
 // so the sign is +1, near = dm2 and far = dp2): the coefficient c of the pair's direction
 // (force contribution c * dir), its windowed curvature and energy. Same arithmetic as
