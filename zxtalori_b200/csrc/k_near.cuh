@@ -603,8 +603,8 @@ __device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], floa
 // can overlap consecutive slots. OWN: the tile may hold images of the warp's sources, so
 // each site's source is tested (the thread's own source gets no force from its images, and
 // its identity image is no neighbour); without it that test is left out. SHORT: cutoffs up
-// to 0.4 rad take the chord form (near_chord_pair32x2; se then sums energy / pi), wider ones
-// the arctangent of near over far.
+// to 0.4 rad take the chord form (near_chord_pair32x2), wider ones the arctangent of near
+// over far. se sums energy / pi.
 template <bool TRACK, bool SHORT, bool OWN>
 __device__ __forceinline__ void near_slots(const NearTile& T, int sub, uint32_t i, float2 xw, float2 xx, float2 xy,
                                            float2 xz, float2 xn, float cut_hi, float cw, float czw, float pk,
@@ -645,30 +645,19 @@ __device__ __forceinline__ void near_slots(const NearTile& T, int sub, uint32_t 
     // nearer the antipode, dm2 > 2, would drive the half-angle out of range) and the
     // window makes them exactly zero.
     const float2 dmc = make_float2(fminf(dm2.x, cut_hi), fminf(dm2.y, cut_hi));
-    float2 coef;
-    if (SHORT) {
-      ChordPair2 pr = near_chord_pair32x2(dmc, cw, czw, pk);
-      coef = pr.coef;
-      if (OWN) {
-        const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
-        coef = mul2(coef, keep);
-        pr.w = mul2(pr.w, keep);
-      }
-      sc = fma2(pr.q, pr.w, sc);
-      se = fma2(pr.rab, pr.w, se);
-    } else {
-      const float2 dp2 = fma2(dmc, splat(-1.0f), add2(xn, T.norm[u]));
-      Pair2 pr = near_pair32x2<false>(dmc, dp2, cw, czw);
-      if (OWN) {
-        const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
-        pr.coef = mul2(pr.coef, keep);
-        pr.curv = mul2(pr.curv, keep);
-        pr.energy = mul2(pr.energy, keep);
-      }
-      coef = pr.coef;
-      sc = add2(sc, pr.curv);
-      se = add2(se, pr.energy);
+    NearPair2 pr;
+    if (SHORT)
+      pr = near_chord_pair32x2(dmc, cw, czw, pk);
+    else
+      pr = near_pair32x2<false>(dmc, fma2(dmc, splat(-1.0f), add2(xn, T.norm[u])), cw, czw, pk);
+    float2 coef = pr.coef;
+    if (OWN) {
+      const float2 keep = make_float2(own0 ? 0.f : 1.f, own1 ? 0.f : 1.f);
+      coef = mul2(coef, keep);
+      pr.w = mul2(pr.w, keep);
     }
+    sc = fma2(pr.q, pr.w, sc);
+    se = fma2(pr.rab, pr.w, se);
     sw = fma2(coef, mw, sw);
     sx = fma2(coef, mx, sx);
     sy = fma2(coef, my, sy);
@@ -868,7 +857,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
   const double3 f = force_from_differences(to_d4(x), make_double4(t[0], t[1], t[2], t[3]));
   const size_t at = (size_t)slice * stride + p;
   out.force[at] = make_double4(f.x, f.y, f.z, t[4]);
-  out.energy[at] = SHORT ? kPi * t[5] : t[5];
+  out.energy[at] = kPi * t[5];
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;
 }
@@ -962,8 +951,8 @@ __global__ void __launch_bounds__(kNearWarps * 32) k_near64(const double4* __res
 // exactly zero, and the nearest chord is reset to 4 when no site is within the cutoff.
 template <bool TRACK, bool MASKED, bool SHORT>
 __device__ __forceinline__ void dense32_tile(const float4 x, float nx2, const PairSlots& S, int count, int i, int j0,
-                                             int k, int n, float cut_hi, float cw, float czw, float2& sw, float2& sx,
-                                             float2& sy, float2& sz, float2& sc, float2& se, float& best,
+                                             int k, int n, float cut_hi, float cw, float czw, float pk, float2& sw,
+                                             float2& sx, float2& sy, float2& sz, float2& sc, float2& se, float& best,
                                              int& best_at) {
   const float2 xw = splat(x.x), xx = splat(x.y), xy = splat(x.z), xz = splat(x.w), xn = splat(nx2);
   const int slots = (count + 1) >> 1;
@@ -999,18 +988,17 @@ __device__ __forceinline__ void dense32_tile(const float4 x, float nx2, const Pa
     }
     const float2 dmc = make_float2(fminf(nearv.x, cut_hi), fminf(nearv.y, cut_hi));
     const float2 farv = fma2(dmc, splat(-1.0f), add2(xn, S.n2[u]));
-    Pair2 p = near_pair32x2<SHORT>(dmc, farv, cw, czw);
+    NearPair2 p = near_pair32x2<SHORT>(dmc, farv, cw, czw, pk);
     if (MASKED) {
       p.coef = mul2(p.coef, keep);
-      p.curv = mul2(p.curv, keep);
-      p.energy = mul2(p.energy, keep);
+      p.w = mul2(p.w, keep);
     }
     sw = fma2(p.coef, dw, sw);
     sx = fma2(p.coef, dx, sx);
     sy = fma2(p.coef, dy, sy);
     sz = fma2(p.coef, dz, sz);
-    sc = add2(sc, p.curv);
-    se = add2(se, p.energy);
+    sc = fma2(p.q, p.w, sc);
+    se = fma2(p.rab, p.w, se);  // energy / pi
   }
 }
 
@@ -1026,7 +1014,7 @@ __global__ void __launch_bounds__(kPairBlock, 8) k_dense32(const float4* __restr
   const float4 x = live ? q[i] : make_float4(1.f, 0.f, 0.f, 0.f);
   const float nx2 = 2.0f * fmaf(x.x, x.x, fmaf(x.y, x.y, fmaf(x.z, x.z, x.w * x.w)));
   const float cut2 = (float)cut.cut2, cut_hi = (float)cut.cut_hi, cw = (float)cut.cut_w,
-              czw = (float)(cut.cut_z * cut.cut_w);
+              czw = (float)(cut.cut_z * cut.cut_w), pk = (float)(-6.0 * kPi * cut.cut_w);
   for (int c = 0; c < 6; ++c) sums[c][threadIdx.x] = 0.0;
   float best = 4.0f;
   int best_at = -1;
@@ -1051,11 +1039,11 @@ __global__ void __launch_bounds__(kPairBlock, 8) k_dense32(const float4* __restr
     float2 sw = splat(0.f), sx = splat(0.f), sy = splat(0.f), sz = splat(0.f), sc = splat(0.f), se = splat(0.f);
     const bool masked = (pt.j0 < i0 + kPairBlock && i0 < pt.j0 + pt.count) || (pt.count & 1);
     if (masked)
-      dense32_tile<TRACK, true, SHORT>(x, nx2, S, pt.count, i, pt.j0, pt.k, n, cut_hi, cw, czw, sw, sx, sy, sz, sc, se,
-                                       best, best_at);
+      dense32_tile<TRACK, true, SHORT>(x, nx2, S, pt.count, i, pt.j0, pt.k, n, cut_hi, cw, czw, pk, sw, sx, sy, sz, sc,
+                                       se, best, best_at);
     else
-      dense32_tile<TRACK, false, SHORT>(x, nx2, S, pt.count, i, pt.j0, pt.k, n, cut_hi, cw, czw, sw, sx, sy, sz, sc,
-                                        se, best, best_at);
+      dense32_tile<TRACK, false, SHORT>(x, nx2, S, pt.count, i, pt.j0, pt.k, n, cut_hi, cw, czw, pk, sw, sx, sy, sz,
+                                        sc, se, best, best_at);
     sums[0][threadIdx.x] += (double)sw.x + (double)sw.y;
     sums[1][threadIdx.x] += (double)sx.x + (double)sx.y;
     sums[2][threadIdx.x] += (double)sy.x + (double)sy.y;
@@ -1072,7 +1060,7 @@ __global__ void __launch_bounds__(kPairBlock, 8) k_dense32(const float4* __restr
   const double3 f = force_from_differences(
       to_d4(x), make_double4(sums[0][threadIdx.x], sums[1][threadIdx.x], sums[2][threadIdx.x], sums[3][threadIdx.x]));
   out.force[at] = make_double4(f.x, f.y, f.z, sums[4][threadIdx.x]);
-  out.energy[at] = sums[5][threadIdx.x];
+  out.energy[at] = kPi * sums[5][threadIdx.x];
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;
 }

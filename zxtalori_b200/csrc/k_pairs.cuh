@@ -253,18 +253,18 @@ __device__ __forceinline__ void pairs32_tile(const float4 x, float nx2, const Pa
     } else {
       best = fminf(best, fminf(n0, n1));
     }
-    Pair2 p = quey_pair32x2(max2(nearv, 1e-30f), farv);
+    QueyPair2 p = quey_pair32x2(max2(nearv, 1e-30f), farv);
     if (MASKED) {
       p.coef = mul2(p.coef, keep);
-      p.curv = mul2(p.curv, keep);
-      p.energy = mul2(p.energy, keep);
+      p.cr = mul2(p.cr, keep);
+      p.rab = mul2(p.rab, keep);
     }
     sw = fma2(p.coef, dw, sw);
     sx = fma2(p.coef, dx, sx);
     sy = fma2(p.coef, dy, sy);
     sz = fma2(p.coef, dz, sz);
-    sc = add2(sc, p.curv);
-    se = add2(se, p.energy);
+    sc = fma2(p.cs, p.cr, sc);
+    se = add2(se, p.rab);  // energy / pi
   }
 }
 
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(kPairBlock, 8) k_pairs32(const float4* __restr
   const double3 f = force_from_differences(
       to_d4(x), make_double4(sums[0][threadIdx.x], sums[1][threadIdx.x], sums[2][threadIdx.x], sums[3][threadIdx.x]));
   out.force[at] = make_double4(f.x, f.y, f.z, sums[4][threadIdx.x]);
-  out.energy[at] = sums[5][threadIdx.x];
+  out.energy[at] = kPi * sums[5][threadIdx.x];
   out.nearest[at] = best;
   if (TRACK) out.nearest_at[at] = best_at;
 }

@@ -169,12 +169,13 @@ __device__ __forceinline__ float2 two_atan_short2(float2 t, float2 t2) {
 
 // Two Quey pairs given near = |x - y~|^2 (clamped to >= 1e-30) and far = |x + y~|^2 of
 // each, y~ the near twin: the coefficient of (x - y~) in the force sum (minus the force
-// magnitude over sin a; sign included), curvature and energy. The arithmetic of
-// quey_pair32 lane by lane.
-struct Pair2 {
-  float2 coef, curv, energy;
+// magnitude over sin a; sign included), the curvature 1/a3 + 1/b3 = cs * cr and the energy
+// pi / (a b) = pi * rab, left as factors so the caller accumulates each with one FMA (and
+// multiplies the energy sum by pi once). The arithmetic of quey_pair32 lane by lane.
+struct QueyPair2 {
+  float2 coef, cs, cr, rab;
 };
-__device__ __forceinline__ Pair2 quey_pair32x2(float2 nearv, float2 farv) {
+__device__ __forceinline__ QueyPair2 quey_pair32x2(float2 nearv, float2 farv) {
   const float2 t2 = mul2(nearv, rcp2(farv));
   const float2 t = sqrt2(t2);
   const float2 a = max2(two_atan_unit2(t, t2), 1e-12f);
@@ -186,18 +187,26 @@ __device__ __forceinline__ Pair2 quey_pair32x2(float2 nearv, float2 farv) {
   const float2 onept2 = add2(t2, splat(1.0f));
   const float2 sp = fma2(splat(1e-9f), onept2, add2(t, t));  // (sine + 1e-9) (1 + t^2)
   const float2 r1 = rcp2(mul2(mul2(a2, bb), sp));
-  Pair2 p;
+  QueyPair2 p;
   p.coef = mul2(mul2(fma2(bb, splat(-1.0f), a2), onept2), r1);  // -(b2 - a2)(1 + t^2) / (a2 b2 sp)
-  p.curv = mul2(add2(a3, b3), rcp2(mul2(a3, b3)));              // 1/a3 + 1/b3
-  p.energy = mul2(splat(kPiF), rcp2(mul2(a, b)));               // pi / (a b)
+  p.cs = add2(a3, b3);
+  p.cr = rcp2(mul2(a3, b3));
+  p.rab = rcp2(mul2(a, b));
   return p;
 }
 
+// The terms of two windowed near-field pairs, left as factors for FMA accumulation: the
+// coefficient of (x - y~), the curvature q w and the energy pi (rab w), with the window w.
+struct NearPair2 {
+  float2 coef, q, w, rab;
+};
+
 // near_pair32 (below) on two sites at once: dm2 and dp2 of each, the window's start cz and
-// inverse width cw, and czw = cz * cw. Beyond the cutoff the window is exactly zero, so
-// such a site contributes nothing (coefficient, curvature and energy all 0).
+// inverse width cw, czw = cz * cw and pk = -6 pi cw (the window's slope factor times pi).
+// Regrouped as coefficient = (1 + t^2) [w (a2 - b2) + pi slope a2 b2 / (a b)] / (a2 b2 sp).
+// Beyond the cutoff the window is exactly zero, so such a site contributes nothing.
 template <bool SHORT>
-__device__ __forceinline__ Pair2 near_pair32x2(float2 dm2, float2 dp2, float cw, float czw) {
+__device__ __forceinline__ NearPair2 near_pair32x2(float2 dm2, float2 dp2, float cw, float czw, float pk) {
   const float2 t2 = mul2(max2(dm2, 1e-30f), rcp2(dp2));
   const float2 t = sqrt2(t2);
   const float2 a = max2(SHORT ? two_atan_short2(t, t2) : two_atan_unit2(t, t2), 1e-12f);
@@ -210,34 +219,27 @@ __device__ __forceinline__ Pair2 near_pair32x2(float2 dm2, float2 dp2, float cw,
   const float2 sp = fma2(splat(1e-9f), onept2, add2(t, t));
   const float2 a2b2 = mul2(a2, bb);
   const float2 r1 = rcp2(mul2(a2b2, sp));
-  const float2 e = mul2(splat(kPiF), rcp2(mul2(a, b)));  // pi / (a b)
+  NearPair2 p;
+  p.rab = rcp2(mul2(a, b));
   const float2 sr = fma2(a, splat(cw), splat(-czw));
   const float2 s = make_float2(__saturatef(sr.x), __saturatef(sr.y));
-  const float2 w = fma2(mul2(s, s), fma2(s, splat(2.0f), splat(-3.0f)), splat(1.0f));  // 1 - s^2 (3 - 2s)
-  const float2 slope = mul2(mul2(s, fma2(s, splat(-1.0f), splat(1.0f))), splat(-6.0f * cw));
-  const float2 u = mul2(onept2, r1);
-  const float2 nalong = mul2(fma2(bb, splat(-1.0f), a2), u);  // -along
-  Pair2 p;
-  p.coef = fma2(w, nalong, mul2(mul2(e, slope), mul2(a2b2, u)));  // a2 b2 u = 1 / sine
-  p.curv = mul2(mul2(add2(a3, b3), rcp2(mul2(a3, b3))), w);       // (1/a3 + 1/b3) w
-  p.energy = mul2(e, w);
+  const float2 ss = mul2(s, s);
+  p.w = fma2(ss, fma2(s, splat(2.0f), splat(-3.0f)), splat(1.0f));  // 1 - s^2 (3 - 2s)
+  const float2 slope = fma2(ss, splat(-pk), mul2(s, splat(pk)));   // pi * (-6 cw) s (1 - s)
+  const float2 g = mul2(mul2(p.rab, slope), a2b2);
+  p.coef = mul2(fma2(p.w, fma2(bb, splat(-1.0f), a2), g), mul2(onept2, r1));
+  p.q = mul2(add2(a3, b3), rcp2(mul2(a3, b3)));
   return p;
 }
 
-// The terms of two windowed near-field pairs from their squared chords d alone, for cutoffs
-// r <= 0.4 rad (d <= 0.25 after the clamp at 1.25 r). For unit quaternions the angle
-// a = 2 atan(sqrt(near/far)) of quey_pair is also 2 asin(c/2), c = sqrt(d) the chord, and
-// sin a = c sqrt(1 - d/4): a = c (1 + d Pa(d)) and sin a = c (1 + d Ps(d)) with Pa, Ps the
-// quadratic fits of fit_atan.py (relative error below 1e-8 on [0, 0.25]). Neither the far
-// chord nor its reciprocal is needed. The same terms as near_pair32x2, regrouped:
-//   coefficient = [w (a2 - b2) + pi slope a2 b2 / (a b)] / (a2 b2 (sin a + 1e-9)),
-//   curvature = q w with q = (a3 + b3) / (a3 b3), energy = pi w / (a b) = pi * (rab w),
-// so the caller accumulates q w and rab w with one FMA each and multiplies the energy sum
-// by pi once. pk = -6 pi cw (the window's slope factor times pi).
-struct ChordPair2 {
-  float2 coef, q, w, rab;
-};
-__device__ __forceinline__ ChordPair2 near_chord_pair32x2(float2 d, float cw, float czw, float pk) {
+// near_pair32x2 from the squared chords d alone, for cutoffs r <= 0.4 rad (d <= 0.25 after
+// the clamp at 1.25 r). For unit quaternions the angle a = 2 atan(sqrt(near/far)) of
+// quey_pair is also 2 asin(c/2), c = sqrt(d) the chord, and sin a = c sqrt(1 - d/4):
+// a = c (1 + d Pa(d)) and sin a = c (1 + d Ps(d)) with Pa, Ps the quadratic fits of
+// fit_atan.py (relative error below 1e-8 on [0, 0.25]). Neither the far chord nor its
+// reciprocal is needed: coefficient = [w (a2 - b2) + pi slope a2 b2 / (a b)] /
+// (a2 b2 (sin a + 1e-9)).
+__device__ __forceinline__ NearPair2 near_chord_pair32x2(float2 d, float cw, float czw, float pk) {
   const float2 c = sqrt2(d);
   const float2 cd = mul2(c, d);
   const float2 pa = fma2(fma2(splat(0x1.8d9f56p-11f), d, splat(0x1.329be0p-8f)), d, splat(0x1.555620p-5f));
@@ -251,7 +253,7 @@ __device__ __forceinline__ ChordPair2 near_chord_pair32x2(float2 d, float cw, fl
   const float2 a3 = fma2(aa, a, splat(1e-9f)), b3 = fma2(bb, b, splat(1e-9f));
   const float2 a2b2 = mul2(a2, bb);
   const float2 r1 = rcp2(mul2(a2b2, sn));  // 1 / (a2 b2 (sin a + 1e-9))
-  ChordPair2 p;
+  NearPair2 p;
   p.rab = rcp2(mul2(a, b));
   const float2 sr = fma2(a, splat(cw), splat(-czw));
   const float2 s = make_float2(__saturatef(sr.x), __saturatef(sr.y));
