@@ -606,12 +606,16 @@ __device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], floa
 // to 0.4 rad take the chord form (near_chord_pair32x2), wider ones the arctangent of near
 // over far. se sums energy / pi.
 template <bool TRACK, bool SHORT, bool OWN>
-__device__ __forceinline__ void near_slots(const NearTile& T, int sub, uint32_t i, float2 xw, float2 xx, float2 xy,
-                                           float2 xz, float2 xn, float cut_hi, float cw, float czw, float pk,
-                                           float2& sw, float2& sx, float2& sy, float2& sz, float2& sc, float2& se,
-                                           float& best, int& best_at) {
+__device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub, uint32_t i, float2 xw, float2 xx,
+                                           float2 xy, float2 xz, float2 xn, float cut_hi, float cw, float czw,
+                                           float pk, float2& sw, float2& sx, float2& sy, float2& sz, float2& sc,
+                                           float2& se, float& best, int& best_at) {
 #pragma unroll
   for (int m = 0; m < kNearSlots; ++m) {
+    // Slots m.. hold elements from 2 kNearSub m on; in a batch's last tile (count < 128)
+    // the warp stops at a 32-element boundary once they are all blank (count is
+    // warp-uniform, so the branch is too).
+    if (m > 0 && m % 2 == 0 && 2 * kNearSub * m >= count) break;
     const int u = sub + kNearSub * m;
     const int first = 2 * u;
     const float4 A = T.wx[u], B = T.yz[u];
@@ -815,11 +819,11 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
       __syncwarp();
       if (live) {
         if (tile_own)
-          near_slots<TRACK, SHORT, true>(T, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy, sz, sc, se,
-                                         best, best_at);
+          near_slots<TRACK, SHORT, true>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy, sz, sc,
+                                         se, best, best_at);
         else
-          near_slots<TRACK, SHORT, false>(T, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy, sz, sc, se,
-                                          best, best_at);
+          near_slots<TRACK, SHORT, false>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy, sz, sc,
+                                          se, best, best_at);
       }
       if (++since == kNearMerge) {
         merge_sums(sums, sw, sx, sy, sz, sc, se);
