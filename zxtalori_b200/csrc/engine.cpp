@@ -66,14 +66,24 @@ void* DeviceBuffer::ensure(size_t bytes) {
   if (bytes <= bytes_ && ptr_) return ptr_;
   release();
   const size_t want = std::max<size_t>(bytes, 256);
-  ZO_CUDA(cudaMalloc(&ptr_, want));
+  const cudaStream_t s = alloc_stream();
+  if (s) {
+    ptr_ = device_pool_alloc(want, s);
+    stream_ = s;
+  } else {
+    ZO_CUDA(cudaMalloc(&ptr_, want));
+  }
   bytes_ = want;
   return ptr_;
 }
 void DeviceBuffer::release() {
-  if (ptr_) cudaFree(ptr_);
+  if (ptr_) {
+    if (stream_) cudaFreeAsync(ptr_, stream_);
+    else cudaFree(ptr_);
+  }
   ptr_ = nullptr;
   bytes_ = 0;
+  stream_ = nullptr;
 }
 
 Rows RowBuffers::ensure(size_t n) {
@@ -388,14 +398,23 @@ Engine::Engine() {
   if (prop.major < 10) throw Failure("NeedsSm100");
   sms_ = prop.multiProcessorCount;
   ensure_tables(device_);
-  ZO_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  ZO_CUDA(cudaStreamCreateWithFlags(&owned_stream_.s, cudaStreamNonBlocking));
+  stream_ = owned_stream_.s;
 }
 
 Engine::~Engine() {
   cudaSetDevice(device_);
   if (stream_) cudaStreamSynchronize(stream_);
   drop_graph();
-  if (stream_) cudaStreamDestroy(stream_);
+  // The buffers are freed on stream_ as the members go; owned_stream_ then waits for those
+  // frees and destroys the stream.
+}
+
+Engine::OwnedStream::~OwnedStream() {
+  if (s) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
 }
 
 // ------------------------------------------------------------------ graph-captured steps
@@ -470,22 +489,27 @@ void Engine::relax_finish() {
   finish_collect();
 }
 
+// One pinned block holds every staging array (one cached allocation per engine).
 void Engine::Staging::ensure(size_t n) {
   if (n <= capacity && summary) return;
   release();
   const size_t cap = std::max<size_t>(n, 1);
-  ZO_CUDA(cudaMallocHost(&summary, sizeof(RowSummary)));
-  ZO_CUDA(cudaMallocHost(&state, sizeof(RelaxDev)));
-  ZO_CUDA(cudaMallocHost(&overflow, sizeof(unsigned int)));
-  ZO_CUDA(cudaMallocHost(&degrees, cap * sizeof(float)));
-  ZO_CUDA(cudaMallocHost(&neighbours, cap * sizeof(int)));
-  ZO_CUDA(cudaMallocHost(&positions, cap * 4 * sizeof(float)));
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t o_state = up(sizeof(RowSummary)), o_overflow = o_state + up(sizeof(RelaxDev)),
+               o_degrees = o_overflow + 256, o_neighbours = o_degrees + up(cap * sizeof(float)),
+               o_positions = o_neighbours + up(cap * sizeof(int)), total = o_positions + up(cap * 4 * sizeof(float));
+  char* base = static_cast<char*>(pinned_alloc(total));
+  summary = reinterpret_cast<RowSummary*>(base);
+  state = reinterpret_cast<RelaxDev*>(base + o_state);
+  overflow = reinterpret_cast<unsigned int*>(base + o_overflow);
+  degrees = reinterpret_cast<float*>(base + o_degrees);
+  neighbours = reinterpret_cast<int*>(base + o_neighbours);
+  positions = reinterpret_cast<float*>(base + o_positions);
   capacity = cap;
 }
 
 void Engine::Staging::release() {
-  for (void* p : {(void*)summary, (void*)state, (void*)overflow, (void*)degrees, (void*)neighbours, (void*)positions})
-    if (p) cudaFreeHost(p);
+  pinned_free(summary);
   summary = nullptr;
   state = nullptr;
   overflow = nullptr;

@@ -28,7 +28,30 @@ struct Failure : std::runtime_error {
 void check_cuda(cudaError_t e, const char* what);
 #define ZO_CUDA(expr) ::zo::check_cuda((expr), #expr)
 
-// Device allocation that only grows; contents are not preserved across growth.
+// Memory that outlives engines. Device buffers come from a per-device stream-ordered pool
+// (cudaMallocFromPoolAsync / cudaFreeAsync) that keeps freed blocks for the next engine:
+// creating and dropping samples costs no cudaMalloc/cudaFree, whose device-wide
+// synchronisation also stalls every other engine. Each block is allocated and freed on the
+// stream of the engine call that asked for it (AllocScope, set around every ABI call), so
+// it is reused only after the work queued on that stream before the free.
+cudaStream_t alloc_stream();
+void* device_pool_alloc(size_t bytes, cudaStream_t s);
+class AllocScope {
+ public:
+  explicit AllocScope(cudaStream_t s);
+  ~AllocScope();
+  AllocScope(const AllocScope&) = delete;
+  AllocScope& operator=(const AllocScope&) = delete;
+
+ private:
+  cudaStream_t prev_;
+};
+// Pinned host blocks, cached across engines by size (up to a bound; beyond it they are freed).
+void* pinned_alloc(size_t bytes);
+void pinned_free(void* p);
+
+// Device allocation that only grows; contents are not preserved across growth. Outside an
+// AllocScope it falls back to cudaMalloc/cudaFree.
 class DeviceBuffer {
  public:
   DeviceBuffer() = default;
@@ -44,6 +67,7 @@ class DeviceBuffer {
  private:
   void* ptr_ = nullptr;
   size_t bytes_ = 0;
+  cudaStream_t stream_ = nullptr;  // the stream it was allocated on; null: cudaMalloc
 };
 
 struct Measures {
@@ -218,6 +242,7 @@ class Engine {
   }
 
   int group() const { return group_; }
+  cudaStream_t stream() const { return stream_; }
   uint32_t count() const { return n_; }
   uint32_t order() const { return (uint32_t)host_group_order(group_); }
   const float* quaternions() const { return host_.data(); }
@@ -261,6 +286,13 @@ class Engine {
   double4* q64() { return prec_ == kFP64 ? q64_.as<double4>() : nullptr; }
 
   int device_ = 0, sms_ = 148;
+  // The engine's stream, declared before every device buffer so that it is destroyed after
+  // them (their frees are ordered on it); its destructor waits for the stream.
+  struct OwnedStream {
+    cudaStream_t s = nullptr;
+    ~OwnedStream();
+  };
+  OwnedStream owned_stream_;
   cudaStream_t stream_ = nullptr;
   int group_ = 9;
   int prec_ = kFP32;

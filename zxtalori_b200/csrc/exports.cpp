@@ -19,6 +19,7 @@ template <class F>
 int guarded(void* h, const char* prefix, F&& f) {
   Engine* e = static_cast<Engine*>(h);
   try {
+    zo::AllocScope scope(e->stream());  // the call's device buffers are ordered on its stream
     f(*e);
     return 0;
   } catch (const std::exception& x) {
