@@ -384,6 +384,22 @@ Measures RelaxState::measures_of(const RowSummary& sum, int n, int order) const 
 }
 
 // ------------------------------------------------------------------ engine
+namespace {
+// The device's name, queried once per process (cudaGetDeviceProperties takes milliseconds).
+std::string device_name(int device) {
+  static std::mutex mutex;
+  static std::vector<std::string> names;
+  std::lock_guard<std::mutex> lock(mutex);
+  if ((int)names.size() <= device) names.resize(device + 1);
+  if (names[device].empty()) {
+    cudaDeviceProp prop;
+    ZO_CUDA(cudaGetDeviceProperties(&prop, device));
+    names[device] = prop.name;
+  }
+  return names[device];
+}
+}  // namespace
+
 Engine::Engine() {
   const char* dev = std::getenv("ZXTALORI_DEVICE");
   int count = 0;
@@ -393,10 +409,11 @@ Engine::Engine() {
   else ZO_CUDA(cudaGetDevice(&device_));
   if (device_ < 0 || device_ >= count) throw Failure("InvalidDevice");
   ZO_CUDA(cudaSetDevice(device_));
-  cudaDeviceProp prop;
-  ZO_CUDA(cudaGetDeviceProperties(&prop, device_));
-  if (prop.major < 10) throw Failure("NeedsSm100");
-  sms_ = prop.multiProcessorCount;
+  int major = 0;
+  ZO_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device_));
+  if (major < 10) throw Failure("NeedsSm100");
+  ZO_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
+  adapter_ = device_name(device_);
   ensure_tables(device_);
   ZO_CUDA(cudaStreamCreateWithFlags(&owned_stream_.s, cudaStreamNonBlocking));
   stream_ = owned_stream_.s;
@@ -1157,8 +1174,7 @@ const char* Engine::stats() {
   j.num("step_deg", step_deg_);
   j.opt("force_rms", m ? finite(m->force_rms) : finite(force_rms_));
   j.str("arithmetic", prec_ == kFP64 ? "fp64" : "fp32-refined");
-  cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device_) == cudaSuccess) j.str("adapter", prop.name);
+  j.str("adapter", adapter_);
   j.s += "}";
   text_ = j.s;
   return text_.c_str();

@@ -286,6 +286,7 @@ class Engine {
   double4* q64() { return prec_ == kFP64 ? q64_.as<double4>() : nullptr; }
 
   int device_ = 0, sms_ = 148;
+  std::string adapter_;  // the device's name, for stats
   // The engine's stream, declared before every device buffer so that it is destroyed after
   // them (their frees are ordered on it); its destructor waits for the stream.
   struct OwnedStream {
