@@ -216,28 +216,65 @@ __global__ void __launch_bounds__(kPairBlock) k_full64(const double4* __restrict
   degen[at] = degenerate;
 }
 
-// Chunks summed in order: rows as k_rows_reduce, extras and degenerate flags alongside.
-__global__ void k_full_reduce(Rows part, const double* __restrict__ pextra, const int* __restrict__ pdegen, int parts,
-                              int n, Rows out, double* __restrict__ extra, int* __restrict__ degen) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// Chunks summed as k_rows_reduce does (warp w takes chunks w, w + kReduceWarps, ...; warp 0
+// adds the warps' sums in warp order), extras and degenerate flags alongside.
+__global__ void __launch_bounds__(32 * kReduceWarps) k_full_reduce(Rows part, const double* __restrict__ pextra,
+                                                                   const int* __restrict__ pdegen, int parts, int n,
+                                                                   Rows out, double* __restrict__ extra,
+                                                                   int* __restrict__ degen) {
+  __shared__ double sv[kReduceWarps][6][32];  // force xyzw, energy, nearest
+  __shared__ double sx[kReduceWarps][5][32];
+  __shared__ int sa[kReduceWarps][32], sc[kReduceWarps][32], sd[kReduceWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int i = blockIdx.x * 32 + lane;
   double4 f = make_double4(0, 0, 0, 0);
   double e = 0, best = 4.0, x[5] = {0, 0, 0, 0, 0};
-  int best_at = -1, dg = 0;
-  for (int c = 0; c < parts; ++c) {
-    const size_t at = (size_t)c * n + i;
-    const double4 g = part.force[at];
-    f.x += g.x;
-    f.y += g.y;
-    f.z += g.z;
-    f.w += g.w;
-    e += part.energy[at];
-    if (part.nearest[at] < best) {
-      best = part.nearest[at];
-      best_at = part.nearest_at[at];
+  int best_at = -1, best_c = parts, dg = 0;
+  if (i < n) {
+    for (int c = w; c < parts; c += kReduceWarps) {
+      const size_t at = (size_t)c * n + i;
+      const double4 g = part.force[at];
+      f.x += g.x;
+      f.y += g.y;
+      f.z += g.z;
+      f.w += g.w;
+      e += part.energy[at];
+      const double b = part.nearest[at];
+      if (b < best) {
+        best = b;
+        best_c = c;
+        best_at = part.nearest_at[at];
+      }
+      for (int r = 0; r < 5; ++r) x[r] += pextra[at * 5 + r];
+      dg |= pdegen[at];
     }
-    for (int r = 0; r < 5; ++r) x[r] += pextra[at * 5 + r];
-    dg |= pdegen[at];
+  }
+  sv[w][0][lane] = f.x;
+  sv[w][1][lane] = f.y;
+  sv[w][2][lane] = f.z;
+  sv[w][3][lane] = f.w;
+  sv[w][4][lane] = e;
+  sv[w][5][lane] = best;
+  for (int r = 0; r < 5; ++r) sx[w][r][lane] = x[r];
+  sa[w][lane] = best_at;
+  sc[w][lane] = best_c;
+  sd[w][lane] = dg;
+  __syncthreads();
+  if (w != 0 || i >= n) return;
+  for (int k = 1; k < kReduceWarps; ++k) {
+    f.x += sv[k][0][lane];
+    f.y += sv[k][1][lane];
+    f.z += sv[k][2][lane];
+    f.w += sv[k][3][lane];
+    e += sv[k][4][lane];
+    const double b = sv[k][5][lane];
+    if (b < best || (b == best && sc[k][lane] < best_c)) {
+      best = b;
+      best_c = sc[k][lane];
+      best_at = sa[k][lane];
+    }
+    for (int r = 0; r < 5; ++r) x[r] += sx[k][r][lane];
+    dg |= sd[k][lane];
   }
   out.force[i] = f;
   out.energy[i] = e;
@@ -259,7 +296,8 @@ cudaError_t launch_full(int prec, const float4* q32, const double4* q64, int n, 
     k_full64<<<grid, kPairBlock, 0, s>>>(q64, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, dx, dd, n);
   else
     k_full32<<<grid, kPairBlock, 0, s>>>(q32, n, op_off, pl.jtiles, pl.total_tiles, pl.tiles_per_chunk, dst, dx, dd, n);
-  if (!direct) k_full_reduce<<<(n + 255) / 256, 256, 0, s>>>(partial, pextra, pdegen, pl.chunks, n, out, extra, degen);
+  if (!direct)
+    k_full_reduce<<<(n + 31) / 32, 32 * kReduceWarps, 0, s>>>(partial, pextra, pdegen, pl.chunks, n, out, extra, degen);
   return cudaGetLastError();
 }
 

@@ -1146,7 +1146,8 @@ cudaError_t launch_dense_near(int prec, bool track, bool short_atan, const float
   }
   probe_mark(s);
   probe_count(direct ? 1 : 2);
-  if (!direct) k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(partial, n, pl.chunks, n, nullptr, out, track ? 1 : 0);
+  if (!direct)
+    k_rows_reduce<<<(n + 31) / 32, 32 * kReduceWarps, 0, s>>>(partial, n, pl.chunks, n, nullptr, out, track ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -1223,7 +1224,8 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
                                             dst, n);
   }
   probe_mark(s);
-  k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(L.partial, n, slices, n, (const int*)L.src_perm, L.out, L.track ? 1 : 0);
+  k_rows_reduce<<<(n + 31) / 32, 32 * kReduceWarps, 0, s>>>(L.partial, n, slices, n, (const int*)L.src_perm, L.out,
+                                                           L.track ? 1 : 0);
   // shell masks (1 or 3), shell write, grid, cell count, scatter, bucket sort, site gather,
   // source count, scatter, bucket sort, gather, reduce (scans counted by launch_scan;
   // memsets aside)

@@ -383,27 +383,58 @@ __global__ void __launch_bounds__(kPairBlock) k_pairs64(const double4* __restric
   if (TRACK) out.nearest_at[at] = best_at;
 }
 
-// Partial rows of `parts` chunks (or slices) summed in chunk order into rows indexed
-// by `dest` (identity when null): the sums do not depend on how blocks were scheduled.
-__global__ void k_rows_reduce(Rows part, int stride, int parts, int n, const int* __restrict__ dest, Rows out,
-                              int track) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
+// Partial rows of `parts` chunks (or slices) summed into rows indexed by `dest` (identity
+// when null). A block takes 32 rows (a lane per row, coalesced) and kReduceWarps warps: warp
+// w sums chunks w, w + kReduceWarps, ... in order, then warp 0 adds the warps' sums in warp
+// order, so the sums do not depend on how blocks were scheduled. The nearest keeps the
+// earliest chunk among equal chords, as a walk through the chunks in order would.
+constexpr int kReduceWarps = 8;
+__global__ void __launch_bounds__(32 * kReduceWarps) k_rows_reduce(Rows part, int stride, int parts, int n,
+                                                                   const int* __restrict__ dest, Rows out, int track) {
+  __shared__ double4 sf[kReduceWarps][32];
+  __shared__ double se[kReduceWarps][32], sb[kReduceWarps][32];
+  __shared__ int sa[kReduceWarps][32], sc[kReduceWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int p = blockIdx.x * 32 + lane;
   double4 f = make_double4(0, 0, 0, 0);
   double e = 0, best = 4.0;
-  int best_at = -1;
-  for (int c = 0; c < parts; ++c) {
-    const size_t at = (size_t)c * stride + p;
-    const double4 g = part.force[at];
+  int best_at = -1, best_c = parts;
+  if (p < n) {
+    for (int c = w; c < parts; c += kReduceWarps) {
+      const size_t at = (size_t)c * stride + p;
+      const double4 g = part.force[at];
+      f.x += g.x;
+      f.y += g.y;
+      f.z += g.z;
+      f.w += g.w;
+      e += part.energy[at];
+      const double b = part.nearest[at];
+      if (b < best) {
+        best = b;
+        best_c = c;
+        if (track) best_at = part.nearest_at[at];
+      }
+    }
+  }
+  sf[w][lane] = f;
+  se[w][lane] = e;
+  sb[w][lane] = best;
+  sa[w][lane] = best_at;
+  sc[w][lane] = best_c;
+  __syncthreads();
+  if (w != 0 || p >= n) return;
+  for (int k = 1; k < kReduceWarps; ++k) {
+    const double4 g = sf[k][lane];
     f.x += g.x;
     f.y += g.y;
     f.z += g.z;
     f.w += g.w;
-    e += part.energy[at];
-    const double b = part.nearest[at];
-    if (b < best) {
+    e += se[k][lane];
+    const double b = sb[k][lane];
+    if (b < best || (b == best && sc[k][lane] < best_c)) {
       best = b;
-      if (track) best_at = part.nearest_at[at];
+      best_c = sc[k][lane];
+      best_at = sa[k][lane];
     }
   }
   const int i = dest ? dest[p] : p;
@@ -443,7 +474,8 @@ cudaError_t launch_pairs(int prec, bool track, const float4* q32, const double4*
   }
   probe_mark(s);
   probe_count(direct ? 1 : 2);
-  if (!direct) k_rows_reduce<<<(n + 255) / 256, 256, 0, s>>>(partial, n, pl.chunks, n, nullptr, out, track ? 1 : 0);
+  if (!direct)
+    k_rows_reduce<<<(n + 31) / 32, 32 * kReduceWarps, 0, s>>>(partial, n, pl.chunks, n, nullptr, out, track ? 1 : 0);
   return cudaGetLastError();
 }
 
