@@ -276,23 +276,27 @@ def batched_section(zo, samples=256, steps=50):
             "timing": "wall clock of zo_batch_relax (all steps and closing passes), samples created beforehand"}
 
 
-def served_section(zo, rate=0.8, duration=20.0, plain_requests=4):
-    """Config 5: Poisson arrivals (rate/s over `duration` s) of relax+measure requests, group
-    uniform, N log-uniform in [500, 1e6], steps uniform in [10, 200], all pairs below 5,000
-    orientations else neighbourhood 20; continuous batching in FP32-refined mode, and the
-    plain FP64 path one request at a time on the first requests of the same stream."""
+def served_section(zo, rates=(0.4, 0.8, 1.6), duration=15.0, plain_requests=4):
+    """Config 5: Poisson arrivals of relax+measure requests at a swept rate (each rate/s over
+    `duration` s), group uniform, N log-uniform in [500, 1e6], steps uniform in [10, 200],
+    all pairs below 5,000 orientations else neighbourhood 20; continuous batching in
+    FP32-refined mode, and the plain FP64 path one request at a time on the first requests
+    of the middle rate's stream. The middle rate's figures are also the section's own."""
     from zxtalori_b200 import serve
 
-    reqs = serve.poisson_requests(rate, duration, seed=5)
-    t = time.perf_counter()
-    served = serve.Server().run(reqs)
-    wall = time.perf_counter() - t
-    info = serve.summary(served)
+    sweep = []
+    for rate in rates:
+        reqs = serve.poisson_requests(rate, duration, seed=5)
+        t = time.perf_counter()
+        served = serve.Server().run(reqs)
+        wall = time.perf_counter() - t
+        sweep.append({"rate_per_s": rate, "arrival_window_s": duration, "wall_s": wall, **serve.summary(served)})
+    middle = sweep[len(sweep) // 2]
+    reqs = serve.poisson_requests(middle["rate_per_s"], duration, seed=5)
     first = sorted(reqs, key=lambda r: r.arrival)[:plain_requests]
     plain = serve.summary(serve.serve_one_at_a_time([serve.Request(r.id, r.group, r.count, r.steps, r.seed,
                                                                    r.neighbourhood, 0.0) for r in first]))
-    return {"rate_per_s": rate, "arrival_window_s": duration, "wall_s": wall, **info,
-            "plain_fp64_one_at_a_time": plain, "plain_requests": plain_requests}
+    return {**middle, "sweep": sweep, "plain_fp64_one_at_a_time": plain, "plain_requests": plain_requests}
 
 
 def _device_seconds(lib, handle, steps, warmup):

@@ -175,7 +175,7 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
 }
 
 void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_r, bool track,
-                     Rows out, int sms) {
+                     Rows out, int sms, bool nearest_only) {
   if (!ready_ || n != n_ || prec != prec_) setup(s, prec, q32, q64, n, mean_r, sms);
   if (dense_) {
     ZO_CUDA(launch_dense_near(prec, track, radius_ <= 0.4, q32, q64, n, gid_, plan_, chord_ * chord_, chord_,
@@ -193,6 +193,7 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
   L.slices32 = slices32_;
   L.track = track;
   L.short_atan = radius_ <= 0.4;
+  L.nearest_only = nearest_only && track;
   L.s_margin = s_margin_;
   L.cut2 = chord_ * chord_;
   L.chord = chord_;
@@ -303,7 +304,7 @@ void RelaxState::record_forces(cudaStream_t s, int prec, const float4* q32, cons
                                bool track, double budget_scale, int sms) {
   const int order = host_group_order(gid);
   if (near_) {
-    near_->pass(s, prec, q32, q64, n, mean_radius((double)n * order), track, rows_.rows(), sms);
+    near_->pass(s, prec, q32, q64, n, mean_radius((double)n * order), track, rows_.rows(), sms, nearest_only);
     return;
   }
   const PairsPlan pl = plan_pairs(n, order, budget_scale, sms);
@@ -837,6 +838,7 @@ void Engine::spacing() {
   if (n_ < 2) throw Failure("TooFewOrientations");
   ZO_CUDA(cudaSetDevice(device_));
   spacing_state_.set_near(group_, n_ > kSpacingAllPairs ? std::optional<double>(kSpacingDelta) : std::nullopt);
+  spacing_state_.nearest_only = true;
   spacing_state_.prepare(stream_, (int)n_, prec_);
   point_separation_.resize(n_);
   point_neighbours_.resize(n_);

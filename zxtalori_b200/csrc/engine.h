@@ -96,7 +96,7 @@ class NearField {
   double radius() const { return radius_; }
   // Records a pass writing rows of q into `out`.
   void pass(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_radius, bool track,
-            Rows out, int sms);
+            Rows out, int sms, bool nearest_only = false);
   // Whether the last pass produced more sites than the workspace holds (after a sync);
   // the next pass sizes it again.
   bool overflowed(cudaStream_t s);
@@ -152,6 +152,9 @@ class RelaxState {
   }
   Rows rows() const { return rows_.rows(); }
   bool current = false;
+  // Passes of this state only find each source's nearest site (the spacing pass): the FP32
+  // near-field gather then skips the pair terms, whose rows stay 0.
+  bool nearest_only = false;
 
   void prepare(cudaStream_t s, int n, int prec);
   void record_forces(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, int gid, bool track,

@@ -604,8 +604,8 @@ __device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], floa
 // each site's source is tested (the thread's own source gets no force from its images, and
 // its identity image is no neighbour); without it that test is left out. SHORT: cutoffs up
 // to 0.4 rad take the chord form (near_chord_pair32x2), wider ones the arctangent of near
-// over far. se sums energy / pi.
-template <bool TRACK, bool SHORT, bool OWN>
+// over far. se sums energy / pi. NEAREST: only the nearest site is tracked.
+template <bool TRACK, bool SHORT, bool OWN, bool NEAREST>
 __device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub, uint32_t i, float2 xw, float2 xx,
                                            float2 xy, float2 xz, float2 xn, float cut_hi, float cw, float czw,
                                            float pk, float2& sw, float2& sx, float2& sy, float2& sz, float2& sc,
@@ -645,6 +645,7 @@ __device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub
     } else {
       best = fminf(best, fminf(n0, n1));
     }
+    if (NEAREST) continue;
     // A site beyond the cutoff takes the chord at 1.25 r: its terms stay finite (a site
     // nearer the antipode, dm2 > 2, would drive the half-angle out of range) and the
     // window makes them exactly zero.
@@ -669,7 +670,7 @@ __device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub
   }
 }
 
-template <bool TRACK, bool SHORT>
+template <bool TRACK, bool SHORT, bool NEAREST = false>
 __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __restrict__ q, int n,
                                                               const uint32_t* __restrict__ src_perm,
                                                               const float4* __restrict__ sq,
@@ -819,13 +820,13 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
       __syncwarp();
       if (live) {
         if (tile_own)
-          near_slots<TRACK, SHORT, true>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy, sz, sc,
-                                         se, best, best_at);
+          near_slots<TRACK, SHORT, true, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
+                                                  sz, sc, se, best, best_at);
         else
-          near_slots<TRACK, SHORT, false>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy, sz, sc,
-                                          se, best, best_at);
+          near_slots<TRACK, SHORT, false, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
+                                                   sz, sc, se, best, best_at);
       }
-      if (++since == kNearMerge) {
+      if (!NEAREST && ++since == kNearMerge) {
         merge_sums(sums, sw, sx, sy, sz, sc, se);
         since = 0;
       }
@@ -1220,6 +1221,7 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   } else {
     auto kernel = L.track ? (L.short_atan ? k_near32<true, true> : k_near32<true, false>)
                           : (L.short_atan ? k_near32<false, true> : k_near32<false, false>);
+    if (L.nearest_only) kernel = k_near32<true, false, true>;
     kernel<<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, slices,
                                             dst, n);
   }

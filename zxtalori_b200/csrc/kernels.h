@@ -47,6 +47,7 @@ struct NearLaunch {
   int slices32;  // slices of the FP32 gather (kNearGroup sources per warp); <= slices
   bool track;
   bool short_atan;  // cutoff r <= 0.4 rad: the short-range arctangent applies
+  bool nearest_only;  // FP32 gather: nearest chord and site only (forces, curvature, energy left 0)
   double s_margin, cut2, chord, cut_z, cut_w;
   const float4* q32;
   const double4* q64;
