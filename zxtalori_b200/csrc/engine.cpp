@@ -368,10 +368,9 @@ void RelaxState::summarize_async(cudaStream_t s, int n, int order, RowSummary* s
 
 Measures RelaxState::summarize(cudaStream_t s, int n, int order, float* degrees, int* neighbours, int prec,
                                const float4* q32, int gid) {
-  RowSummary sum;
-  summarize_async(s, n, order, &sum, degrees, neighbours, prec, q32, gid);
+  summarize_async(s, n, order, &last_summary_, degrees, neighbours, prec, q32, gid);
   ZO_CUDA(cudaStreamSynchronize(s));
-  return measures_of(sum, n, order);
+  return measures_of(last_summary_, n, order);
 }
 
 Measures RelaxState::measures_of(const RowSummary& sum, int n, int order) const {
@@ -583,6 +582,7 @@ void Engine::finish_collect() {
     point_neighbours_.assign(stage_.neighbours, stage_.neighbours + n_);
     point_separation_iteration_ = iteration_;
     host_.assign(stage_.positions, stage_.positions + 4 * (size_t)n_);
+    identity_cache_.reset();
     relax_state_.current = true;
   }
   if (last) {
@@ -606,15 +606,22 @@ uint32_t Engine::ratio_limit() const {
 }
 
 std::optional<uint32_t> Engine::identity_index() const {
+  if (identity_cache_) return *identity_cache_;
+  std::optional<uint32_t> found;
   for (uint32_t i = 0; i < n_; ++i) {
     const float* a = &host_[(size_t)i * 4];
-    if (std::fabs(a[1]) + std::fabs(a[2]) + std::fabs(a[3]) < 1e-6f) return i;
+    if (std::fabs(a[1]) + std::fabs(a[2]) + std::fabs(a[3]) < 1e-6f) {
+      found = i;
+      break;
+    }
   }
-  return std::nullopt;
+  identity_cache_ = found;
+  return found;
 }
 
 void Engine::fetch() {
   host_.resize((size_t)n_ * 4);
+  identity_cache_.reset();
   ZO_CUDA(cudaMemcpyAsync(host_.data(), q32_.as<float4>(), (size_t)n_ * 16, cudaMemcpyDeviceToHost, stream_));
   ZO_CUDA(cudaStreamSynchronize(stream_));
 }
@@ -852,11 +859,11 @@ void Engine::spacing() {
   try {
     spacing_state_.summarize(stream_, (int)n_, (int)order(), point_separation_.data(), point_neighbours_.data(), prec_,
                              q32(), group_);
-  } catch (const Failure&) {
+  } catch (const Failure& x) {
     // A duplicate shows as a zero separation below.
+    if (std::strcmp(x.what(), "DuplicateOrientations") != 0) throw;
   }
-  float least = 180.0f;
-  for (float d : point_separation_) least = std::min(least, d);
+  const float least = spacing_state_.last_summary().least_degrees;  // the smallest point value
   if (!(least > 0)) throw Failure("DuplicateOrientations");
   if (measures_ && measure_iteration_ == iteration_) {
     measures_->separation_deg = least;
@@ -927,6 +934,7 @@ void Engine::identity(bool add, bool fixed) {
     const uint32_t i = *index;
     const float one[4] = {1.f, 0.f, 0.f, 0.f};
     std::memcpy(&host_[(size_t)i * 4], one, 16);
+    identity_cache_.reset();
     ZO_CUDA(cudaMemcpyAsync(q32() + i, one, 16, cudaMemcpyHostToDevice, stream_));
     if (prec_ == kFP64) {
       const double one64[4] = {1, 0, 0, 0};

@@ -155,6 +155,8 @@ class RelaxState {
   // Passes of this state only find each source's nearest site (the spacing pass): the FP32
   // near-field gather then skips the pair terms, whose rows stay 0.
   bool nearest_only = false;
+  // The row summary of the last summarize().
+  const RowSummary& last_summary() const { return last_summary_; }
 
   void prepare(cudaStream_t s, int n, int prec);
   void record_forces(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, int gid, bool track,
@@ -179,6 +181,7 @@ class RelaxState {
   bool sized(int n, int prec) const { return n_ == n && prec_ == prec && (!near_ || near_->ready()); }
 
  private:
+  RowSummary last_summary_{};
   uint64_t generation_ = 0;
   StepResult step_result(const RelaxDev& st) const;
   int n_ = 0, prec_ = -1, order_ = 0;
@@ -285,6 +288,9 @@ class Engine {
   Measures relax_state_measure();
   int fixed_arg() const { return fixed_index_ ? (int)*fixed_index_ : -1; }
   std::optional<uint32_t> identity_index() const;
+  // identity_index() of the current host copy (a scan of every orientation), kept until
+  // the host copy changes.
+  mutable std::optional<std::optional<uint32_t>> identity_cache_;
   float4* q32() { return q32_.as<float4>(); }
   double4* q64() { return prec_ == kFP64 ? q64_.as<double4>() : nullptr; }
 

@@ -212,6 +212,12 @@ __global__ void k_move_fold(float4* __restrict__ q32, double4* __restrict__ q64,
   if ((threadIdx.x & 31) == 0 && bits) atomicMax(&st->step_bits, bits);
 }
 
+// A nearest chord^2 as the SO(3) angle in degrees, rounded to float (pairs.wgsl:428-434).
+__device__ __forceinline__ float nearest_degrees_of(double chord2) {
+  const double c = fmin(1.0, sqrt(fmax(chord2, 0.0)) * 0.5);
+  return (float)(4.0 * asin(c) * (180.0 / kPi));
+}
+
 // Quick measures of a force pass (src/pairs.zig:130-140, 182-199): energy sum, force^2 sum
 // and the smallest nearest chord with its source, deterministic.
 __global__ void __launch_bounds__(kRelaxBlock) k_row_summary(Rows rows, int n, double* __restrict__ partials,
@@ -295,6 +301,7 @@ __global__ void __launch_bounds__(kRelaxBlock) k_row_summary(Rows rows, int n, d
     out->force2 = s[1];
     out->nearest = b;
     out->nearest_row = a;
+    out->least_degrees = nearest_degrees_of(b);  // the point value of the nearest source
   }
 }
 
@@ -302,8 +309,7 @@ __global__ void __launch_bounds__(kRelaxBlock) k_row_summary(Rows rows, int n, d
 __global__ void k_nearest_degrees(const double* __restrict__ nearest, int n, float* __restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double c = fmin(1.0, sqrt(fmax(nearest[i], 0.0)) * 0.5);
-  out[i] = (float)(4.0 * asin(c) * (180.0 / kPi));
+  out[i] = nearest_degrees_of(nearest[i]);
 }
 
 // FP32 mode: the nearest chord of each source's chosen neighbour recomputed in FP64 from

@@ -65,6 +65,7 @@ struct RowSummary {
   double force2;     // sum of |force|^2
   double nearest;    // min nearest chord^2
   int nearest_row;   // its source
+  float least_degrees;  // the smallest per-source nearest angle, degrees, rounded as the point values are
   unsigned int ticket;
 };
 
