@@ -677,7 +677,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
                                                               const uint32_t* __restrict__ scode,
                                                               const uint32_t* __restrict__ cell_off,
                                                               const NearGrid* __restrict__ gp, NearCut cut, int slices,
-                                                              Rows out, int stride) {
+                                                              Rows out, int stride, int direct) {
   __shared__ NearTile tiles[kNearWarps];
   __shared__ NearWalk walks[kNearWarps];
   __shared__ double sums[6][kNearWarps * 32];  // FP64 lane sums: force differences, curvature, energy
@@ -860,7 +860,8 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
     for (int l = 0; l < kNearSub; ++l) t[c] += sums[c][threadIdx.x + l];
   }
   const double3 f = force_from_differences(to_d4(x), make_double4(t[0], t[1], t[2], t[3]));
-  const size_t at = (size_t)slice * stride + p;
+  // direct (one slice): the source's own row; else row p of this slice's partial rows.
+  const size_t at = direct ? (size_t)i : (size_t)slice * stride + p;
   out.force[at] = make_double4(f.x, f.y, f.z, t[4]);
   out.energy[at] = kPi * t[5];
   out.nearest[at] = best;
@@ -1222,8 +1223,15 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
     auto kernel = L.track ? (L.short_atan ? k_near32<true, true> : k_near32<true, false>)
                           : (L.short_atan ? k_near32<false, true> : k_near32<false, false>);
     if (L.nearest_only) kernel = k_near32<true, false, true>;
+    // One slice: each warp writes its sources' rows in place, no partial rows to reduce.
+    const int direct = slices == 1 ? 1 : 0;
     kernel<<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, slices,
-                                            dst, n);
+                                            direct ? L.out : dst, n, direct);
+    if (direct) {
+      probe_mark(s);
+      probe_count(10 + shell_launches);
+      return cudaGetLastError();
+    }
   }
   probe_mark(s);
   k_rows_reduce<<<(n + 31) / 32, 32 * kReduceWarps, 0, s>>>(L.partial, n, slices, n, (const int*)L.src_perm, L.out,
