@@ -513,14 +513,11 @@ void Engine::Staging::ensure(size_t n) {
   const size_t cap = std::max<size_t>(n, 1);
   auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t o_state = up(sizeof(RowSummary)), o_overflow = o_state + up(sizeof(RelaxDev)),
-               o_degrees = o_overflow + 256, o_neighbours = o_degrees + up(cap * sizeof(float)),
-               o_positions = o_neighbours + up(cap * sizeof(int)), total = o_positions + up(cap * 4 * sizeof(float));
+               o_positions = o_overflow + 256, total = o_positions + up(cap * 4 * sizeof(float));
   char* base = static_cast<char*>(pinned_alloc(total));
   summary = reinterpret_cast<RowSummary*>(base);
   state = reinterpret_cast<RelaxDev*>(base + o_state);
   overflow = reinterpret_cast<unsigned int*>(base + o_overflow);
-  degrees = reinterpret_cast<float*>(base + o_degrees);
-  neighbours = reinterpret_cast<int*>(base + o_neighbours);
   positions = reinterpret_cast<float*>(base + o_positions);
   capacity = cap;
 }
@@ -530,8 +527,6 @@ void Engine::Staging::release() {
   summary = nullptr;
   state = nullptr;
   overflow = nullptr;
-  degrees = nullptr;
-  neighbours = nullptr;
   positions = nullptr;
   capacity = 0;
 }
@@ -558,8 +553,10 @@ void Engine::finish_async() {
   const unsigned int* flag = nf ? nf->overflow_flag() : nullptr;
   finish_has_overflow_ = flag != nullptr;
   if (flag) ZO_CUDA(cudaMemcpyAsync(stage_.overflow, flag, 4, cudaMemcpyDeviceToHost, stream_));
-  relax_state_.summarize_async(stream_, n, (int)order(), stage_.summary, stage_.degrees, stage_.neighbours, prec_,
-                               q32(), group_);
+  point_separation_.resize(n_);
+  point_neighbours_.resize(n_);
+  relax_state_.summarize_async(stream_, n, (int)order(), stage_.summary, point_separation_.data(),
+                               point_neighbours_.data(), prec_, q32(), group_);
   ZO_CUDA(cudaMemcpyAsync(stage_.positions, q32(), (size_t)n * 16, cudaMemcpyDeviceToHost, stream_));
   finishing_ = true;
 }
@@ -578,9 +575,7 @@ void Engine::finish_collect() {
     fetch();
   } else {
     m = relax_state_.measures_of(*stage_.summary, (int)n_, (int)order());
-    point_separation_.assign(stage_.degrees, stage_.degrees + n_);
-    point_neighbours_.assign(stage_.neighbours, stage_.neighbours + n_);
-    point_separation_iteration_ = iteration_;
+    point_separation_iteration_ = iteration_;  // the degrees and neighbours were copied in place
     host_.assign(stage_.positions, stage_.positions + 4 * (size_t)n_);
     identity_cache_.reset();
     relax_state_.current = true;

@@ -50,6 +50,34 @@ class AllocScope {
 void* pinned_alloc(size_t bytes);
 void pinned_free(void* p);
 
+// Host array in pinned memory (from the cache above) that only grows: device-to-host copies
+// into it run at full PCIe/C2C speed instead of through the driver's pageable staging.
+template <class T>
+class PinnedArray {
+ public:
+  PinnedArray() = default;
+  PinnedArray(const PinnedArray&) = delete;
+  PinnedArray& operator=(const PinnedArray&) = delete;
+  ~PinnedArray() { pinned_free(p_); }
+  void resize(size_t n) {
+    if (n > cap_) {
+      pinned_free(p_);
+      p_ = nullptr;
+      cap_ = 0;
+      p_ = static_cast<T*>(pinned_alloc(n * sizeof(T)));
+      cap_ = n;
+    }
+    n_ = n;
+  }
+  T* data() { return p_; }
+  const T* data() const { return p_; }
+  size_t size() const { return n_; }
+
+ private:
+  T* p_ = nullptr;
+  size_t n_ = 0, cap_ = 0;
+};
+
 // Device allocation that only grows; contents are not preserved across growth. Outside an
 // AllocScope it falls back to cudaMalloc/cudaFree.
 class DeviceBuffer {
@@ -256,13 +284,12 @@ class Engine {
   char err[2048] = {0};
 
  private:
-  // Pinned host copies of a closing pass's results (asynchronous finish).
+  // Pinned host copies of a closing pass's results (asynchronous finish); the nearest
+  // degrees and neighbours go straight to the pinned point arrays.
   struct Staging {
     RowSummary* summary = nullptr;
     RelaxDev* state = nullptr;
     unsigned int* overflow = nullptr;
-    float* degrees = nullptr;
-    int* neighbours = nullptr;
     float* positions = nullptr;
     size_t capacity = 0;
     void ensure(size_t n);
@@ -321,8 +348,8 @@ class Engine {
   bool full_measures_ = false;
   RelaxState relax_state_, spacing_state_;
   double neighbourhood_ = 0, measure_neighbourhood_ = 0;
-  std::vector<float> point_separation_;
-  std::vector<int> point_neighbours_;
+  PinnedArray<float> point_separation_;
+  PinnedArray<int> point_neighbours_;
   std::optional<uint32_t> point_separation_iteration_;
   double step_deg_ = 0, force_rms_ = 0;
   std::atomic<bool> cancelled_{false};
