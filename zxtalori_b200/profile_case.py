@@ -5,8 +5,9 @@ Compute), each a few relaxation steps of one sample through the public API:
     python -m zxtalori_b200.profile_case pairs     # O, N=16,384 Haar (seed 193), all pairs
     python -m zxtalori_b200.profile_case spacing   # I, N=1,000,000 Haar (seed 7), spacing pass
 
-`--steps` sets the number of relaxation steps (default 2). Prints the resulting energy or
-separation, so a run can be checked against a plain one.
+`--steps` sets the number of relaxation steps (default 2) or, for spacing, of spacing
+passes; `--count` the spacing sample's size. Prints the resulting energy or separation, so a
+run can be checked against a plain one.
 """
 from __future__ import annotations
 
@@ -19,6 +20,7 @@ def main(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("case", choices=["near", "pairs", "spacing"])
     p.add_argument("--steps", type=int, default=2)
+    p.add_argument("--count", type=int, default=1_000_000)
     args = p.parse_args(argv)
     if args.case == "near":
         with zo.haar("O", 100_000, 193) as g:
@@ -29,8 +31,10 @@ def main(argv=None):
             g.relax(args.steps)
             print(g.stats["energy"])
     else:
-        with zo.haar("I", 1_000_000, 7) as g:
-            print(g.spacing()["separation_deg"])
+        with zo.haar("I", args.count, 7) as g:
+            for _ in range(max(1, args.steps)):
+                separation = g.spacing()["separation_deg"]
+            print(separation)
     return 0
 
 
