@@ -1,0 +1,167 @@
+"""Host logic of the continuous-batching server, with a fake engine in place of the GPU:
+admission in arrival order within the memory budget and the concurrency cap, a request
+larger than the budget still served when nothing else is resident, every request relaxed
+for exactly its steps, and the Poisson workload generator's shape."""
+import numpy as np
+import pytest
+
+from zxtalori_b200 import serve
+
+
+class FakeLib:
+    def __init__(self, log):
+        self.log = log
+
+    def zo_idle(self, h):
+        return 1
+
+    def zo_relax_async(self, h, k):
+        h.done += k
+        self.log.append(("steps", h.request_id, k))
+        return 0
+
+    def zo_relax_finish(self, h):
+        self.log.append(("finish", h.request_id))
+        return 0
+
+
+class FakeGrid:
+    live = 0
+    most_live = 0
+
+    def __init__(self, request_id, count, group, log):
+        self._handle = self
+        self._lib = FakeLib(log)
+        self.request_id = request_id
+        self.count = count
+        self.group = group
+        self.done = 0
+        self.neighbourhood = 0.0
+        FakeGrid.live += 1
+        FakeGrid.most_live = max(FakeGrid.most_live, FakeGrid.live)
+
+    def _check(self, rc):
+        assert rc == 0
+
+    @property
+    def stats(self):
+        return {"count": self.count, "order": serve.ORDER[self.group], "iteration": self.done,
+                "relax_neighbourhood": self.neighbourhood or None}
+
+    @property
+    def quaternions(self):
+        return np.zeros((self.count, 4), np.float32)
+
+    def close(self):
+        FakeGrid.live -= 1
+
+
+class Clock:
+    """Advances 1 ms on every reading, so the loop's waits end."""
+
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        self.t += 1e-3
+        return self.t
+
+
+@pytest.fixture
+def fake(monkeypatch):
+    log = []
+    FakeGrid.live = 0
+    FakeGrid.most_live = 0
+    ids = {}
+
+    def haar(group, count, seed, precision="fp32"):
+        return FakeGrid(ids[seed], count, group, log)
+
+    def neighbourhood(h, delta):
+        h.neighbourhood = delta
+        return 0
+
+    monkeypatch.setattr(serve, "haar", haar)
+    monkeypatch.setattr(FakeLib, "zo_relax_neighbourhood", lambda self, h, d: neighbourhood(h, d), raising=False)
+    return log, ids
+
+
+def _requests(ids, specs):
+    out = []
+    for k, (group, count, steps, delta, arrival) in enumerate(specs):
+        seed = 1000 + k
+        ids[seed] = k
+        out.append(serve.Request(k, group, count, steps, seed, delta, arrival))
+    return out
+
+
+def test_every_request_runs_exactly_its_steps(fake):
+    log, ids = fake
+    reqs = _requests(ids, [("O", 2000, 37, 0.0, 0.0), ("I", 800, 5, 0.0, 0.002), ("C2", 9000, 120, 20.0, 0.004)])
+    results = serve.Server(memory_budget=1 << 40, chunk_seconds=1e-6).run(reqs, clock=Clock())
+    assert sorted(r.id for r in results) == [0, 1, 2]
+    for r in results:
+        assert r.stats["iteration"] == reqs[r.id].steps
+        assert r.finished >= r.admitted >= r.arrival
+    # Each sample is finished once, after all its steps.
+    for k in range(3):
+        events = [e for e in log if e[1] == k]
+        assert events[-1] == ("finish", k)
+        assert sum(e[2] for e in events if e[0] == "steps") == reqs[k].steps
+    assert FakeGrid.live == 0
+
+
+def test_admission_respects_budget_and_cap(fake):
+    log, ids = fake
+    specs = [("O", 3000, 10, 0.0, 0.0) for _ in range(6)]
+    reqs = _requests(ids, specs)
+    one = serve.estimate_bytes(3000, "O", 0.0)
+    serve.Server(memory_budget=2 * one + one // 2, chunk_seconds=1e-6).run(reqs, clock=Clock())
+    assert FakeGrid.most_live == 2
+    FakeGrid.most_live = 0
+    log.clear()
+    ids.clear()
+    reqs = _requests(ids, specs)
+    serve.Server(memory_budget=1 << 40, max_active=3, chunk_seconds=1e-6).run(reqs, clock=Clock())
+    assert FakeGrid.most_live == 3
+
+
+def test_oversize_request_runs_alone(fake):
+    log, ids = fake
+    reqs = _requests(ids, [("O", 50_000, 4, 20.0, 0.0), ("T", 1000, 4, 0.0, 0.0)])
+    results = serve.Server(memory_budget=1, chunk_seconds=1e-6).run(reqs, clock=Clock())
+    assert sorted(r.id for r in results) == [0, 1]
+    assert FakeGrid.most_live == 1
+
+
+def test_admission_follows_arrival_order(fake):
+    log, ids = fake
+    reqs = _requests(ids, [("O", 1000, 3, 0.0, 0.05), ("O", 1000, 3, 0.0, 0.01), ("O", 1000, 3, 0.0, 0.03)])
+    results = serve.Server(memory_budget=1, chunk_seconds=1e-6).run(reqs, clock=Clock())
+    assert [r.id for r in results] == [1, 2, 0]
+    assert all(r.admitted >= r.arrival for r in results)
+
+
+def test_poisson_workload_shape():
+    reqs = serve.poisson_requests(2.0, 200.0, seed=3)
+    again = serve.poisson_requests(2.0, 200.0, seed=3)
+    assert [(r.group, r.count, r.steps, r.seed, r.arrival) for r in reqs] == \
+        [(r.group, r.count, r.steps, r.seed, r.arrival) for r in again]
+    assert 300 < len(reqs) < 500  # 400 expected
+    arrivals = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(arrivals) > 0) and arrivals[-1] <= 200.0
+    assert {r.group for r in reqs} <= set(serve.ORDER)
+    assert all(500 <= r.count <= 1_000_000 and 10 <= r.steps <= 200 for r in reqs)
+    assert all((r.neighbourhood == 0.0) == (r.count < 5000) for r in reqs)
+    logs = np.log([r.count for r in reqs])
+    assert abs(np.median(logs) - 0.5 * (np.log(500) + np.log(1e6))) < 0.6  # log-uniform
+
+
+def test_summary_counts_pairs_as_the_reference():
+    res = [serve.Result(0, 0.0, 0.0, 2.0, {"count": 1000, "order": 24, "iteration": 10, "relax_neighbourhood": None}),
+           serve.Result(1, 1.0, 1.0, 4.0, {"count": 100_000, "order": 24, "iteration": 5, "relax_neighbourhood": 20.0})]
+    info = serve.summary(res)
+    evals = 11 * 1000 * 1000 * 24 + 6 * 100_000 * min(100_000 * 24, 0.94 * 20 ** 3 + 64)
+    assert info["pair_evals_per_s"] == pytest.approx(evals / 4.0)
+    assert info["requests"] == 2
+    assert info["latency_p50_s"] == pytest.approx(2.5)
