@@ -514,17 +514,18 @@ __device__ __forceinline__ bool row_run(const WarpBox& b, const NearGrid& g, con
 
 // The gather (pairs.wgsl:363-416). A warp holds kNearGroup sources (consecutive along the
 // Hilbert order), each on kNearSub = 32 / kNearGroup lanes that split its sites between
-// them. The warp walks the cell rows within reach of its sources' chart box 32 rows at a
-// time, one lane per row finding the row's run of sorted sites; the runs are concatenated
-// and streamed through shared memory in tiles of kNearTile sites, and every lane evaluates
-// its source against kNearTile / kNearSub sites of each tile, two per instruction with
-// packed FP32 arithmetic. For a site within the cutoff chord the windowed pair runs with
-// dp2 = 2(|x|^2+|y|^2) - dm2 (parallelogram law; the site is the near twin); sites beyond it
-// contribute exactly zero through the window, and the nearest chord is taken over every
-// site and reset to 4 when it exceeds the cutoff (no site within it), which is the same as
-// testing each site. The force is kept as sum c (x - y), turned into a force once per
-// source. Lane sums are FP32 over 32 sites, then FP64; the lanes of a source are added in
-// lane order at the end.
+// them. The warp walks the cell rows that its sources' chart balls reach 32 rows at a time,
+// one lane per row finding the row's run of sorted sites; the runs are concatenated and
+// streamed through shared memory in tiles of kNearTile sites, and every lane evaluates its
+// source against kNearTile / kNearSub sites of each tile, two per instruction with packed
+// FP32 arithmetic. For cutoffs up to 0.4 rad the windowed pair is a function of the chord
+// alone (near_chord_pair32x2); wider ones use dp2 = 2(|x|^2+|y|^2) - dm2 (parallelogram
+// law; the site is the near twin). Sites beyond the cutoff contribute exactly zero through
+// the window, and the nearest chord is taken over every site and reset to 4 when it exceeds
+// the cutoff (no site within it), which is the same as testing each site. The force is kept
+// as sum c (x - y), turned into a force once per source. Lane sums are FP32 over 32 sites,
+// then FP64; the lanes of a source are added in lane order at the end. With one slice each
+// warp writes its sources' rows in place; the spacing pass runs a nearest-only variant.
 constexpr int kNearSub = 32 / kNearGroup;          // lanes per source
 constexpr int kNearTile = 128;                      // sites per tile
 constexpr int kNearSlots = kNearTile / (2 * kNearSub);  // site pairs per lane and tile
