@@ -149,6 +149,7 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   perm_.ensure(capacity_ * 4ull);
   sq_.ensure(capacity_ * qsize);
   scode_.ensure(capacity_ * 4ull);
+  sx_.ensure(capacity_ * 4ull);
   simg_.ensure(capacity_ * 4ull);
   const size_t mcells = (size_t)kOrderDim * kOrderDim * kOrderDim + 1;
   src_key_.ensure((size_t)n * 4);
@@ -221,6 +222,7 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
   L.sq32 = prec == kFP64 ? nullptr : sq_.as<float4>();
   L.sq64 = prec == kFP64 ? sq_.as<double4>() : nullptr;
   L.scode = scode_.as<uint32_t>();
+  L.sx = sx_.as<float>();
   L.simg = simg_.as<uint32_t>();
   L.src_key = src_key_.as<uint32_t>();
   L.src_rank = src_rank_.as<uint32_t>();

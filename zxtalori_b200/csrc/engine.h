@@ -163,7 +163,7 @@ class NearField {
   double radius_ = 0, s_margin_ = 0, chord_ = 0;
   DeviceBuffer counts_, offsets_, scan_tmp_, shell_mask_, rim_list_, rim_q_, rim_count_;
   DeviceBuffer site_q_, site_code_, site_img_, site_cell_, site_rank_, site_pos_;
-  DeviceBuffer cell_count_, cell_off_, perm_, sq_, scode_, simg_, src_key_, src_rank_, mcount_, moff_, src_perm_;
+  DeviceBuffer cell_count_, cell_off_, perm_, sq_, scode_, simg_, sx_, src_key_, src_rank_, mcount_, moff_, src_perm_;
   DeviceBuffer grid_, cells_;
   RowBuffers partial_;
 };

@@ -350,10 +350,19 @@ __global__ void k_scatter(const uint32_t* __restrict__ key, const uint32_t* __re
   perm[offsets[key[s]] + rank[s]] = (uint32_t)s;
 }
 
-// Each bucket's items in index order (near.wgsl:270-282), so every pass sums in the same
-// order. Insertion sort; buckets hold a handful of items on average.
+// Each bucket's items in a fixed order, so every pass sums in the same order: by index
+// (near.wgsl:270-282), or with `pos` by chart x and then index (a cell row's sites are then
+// sorted along x, and the walk trims its runs to the balls' x extent). Insertion sort;
+// buckets hold a handful of items on average.
+__device__ __forceinline__ bool sorts_before(uint32_t a, uint32_t b, const float4* __restrict__ pos) {
+  if (pos) {
+    const float xa = pos[a].x, xb = pos[b].x;
+    if (xa != xb) return xa < xb;
+  }
+  return a < b;
+}
 __global__ void k_bucket_sort(const uint32_t* __restrict__ offsets, int max_buckets, const int* __restrict__ buckets,
-                              uint32_t* __restrict__ perm) {
+                              uint32_t* __restrict__ perm, const float4* __restrict__ pos = nullptr) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int count = buckets ? min(*buckets, max_buckets) : max_buckets;
   if (b >= count) return;
@@ -361,7 +370,7 @@ __global__ void k_bucket_sort(const uint32_t* __restrict__ offsets, int max_buck
   for (uint32_t at = begin + 1; at < end; ++at) {
     const uint32_t v = perm[at];
     uint32_t k = at;
-    while (k > begin && perm[k - 1] > v) {
+    while (k > begin && sorts_before(v, perm[k - 1], pos)) {
       perm[k] = perm[k - 1];
       --k;
     }
@@ -373,8 +382,8 @@ template <bool FP64>
 __global__ void k_site_gather(const uint32_t* __restrict__ perm, const NearGrid* __restrict__ gp,
                               const float4* __restrict__ q32, const double4* __restrict__ q64,
                               const uint32_t* __restrict__ code, const uint32_t* __restrict__ img,
-                              float4* __restrict__ sq32, double4* __restrict__ sq64, uint32_t* __restrict__ scode,
-                              uint32_t* __restrict__ simg) {
+                              const float4* __restrict__ pos, float4* __restrict__ sq32, double4* __restrict__ sq64,
+                              uint32_t* __restrict__ scode, uint32_t* __restrict__ simg, float* __restrict__ sx) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= gp->sites) return;
   const uint32_t s = perm[p];
@@ -382,6 +391,7 @@ __global__ void k_site_gather(const uint32_t* __restrict__ perm, const NearGrid*
   else sq32[p] = q32[s];
   scode[p] = code[s];
   simg[p] = img[s];
+  sx[p] = pos[s].x;
 }
 
 // ------------------------------------------------------------------ 3. sources in Hilbert order
@@ -558,8 +568,8 @@ struct NearWalk {
 
 // Row r of the walk's (y, z) cell rows: the run of sorted sites of the x cells that some
 // source's ball reaches in this row.
-__device__ __forceinline__ bool walk_row(const NearWalk& W, const uint32_t* cell_off, int r, uint32_t& start,
-                                         uint32_t& end) {
+__device__ __forceinline__ bool walk_row(const NearWalk& W, const uint32_t* cell_off, const float* site_x, int r,
+                                         uint32_t& start, uint32_t& end) {
   const int ny = W.chi[1] - W.clo[1] + 1;
   const int y = W.clo[1] + r % ny, z = W.clo[2] + r / ny;
   const float width = 1.0f / W.cells_per_unit;
@@ -583,6 +593,10 @@ __device__ __forceinline__ bool walk_row(const NearWalk& W, const uint32_t* cell
   const int row = W.sdim * (y + W.sdim * z);
   start = cell_off[row + c0];
   end = cell_off[row + c1 + 1];
+  // Each cell's sites are sorted by chart x: drop those of the end cells outside [x0, x1].
+  const uint32_t first_end = cell_off[row + c0 + 1], last_begin = cell_off[row + c1];
+  while (start < first_end && site_x[start] < x0) ++start;
+  while (end > last_begin && end > start && site_x[end - 1] > x1) --end;
   return start < end;
 }
 
@@ -677,6 +691,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
                                                               const float4* __restrict__ sq,
                                                               const uint32_t* __restrict__ scode,
                                                               const uint32_t* __restrict__ cell_off,
+                                                              const float* __restrict__ site_x,
                                                               const NearGrid* __restrict__ gp, NearCut cut, int slices,
                                                               Rows out, int stride, int direct) {
   __shared__ NearTile tiles[kNearWarps];
@@ -739,7 +754,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
     uint32_t start = 0, len = 0;
     if (rb + lane < mine) {
       uint32_t a, b;
-      if (walk_row(W, cell_off, slice + (rb + lane) * slices, a, b)) {
+      if (walk_row(W, cell_off, site_x, slice + (rb + lane) * slices, a, b)) {
         start = a;
         len = b - a;
       }
@@ -1193,13 +1208,15 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   if ((e = launch_scan(L.cell_count, L.cell_off, max_cells, L.cells, L.scan_tmp, s))) return e;
   k_scatter<<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.site_cell, L.site_rank, L.cell_off, L.capacity,
                                                       &L.grid->sites, L.perm);
-  k_bucket_sort<<<(max_cells + tb - 1) / tb, tb, 0, s>>>(L.cell_off, max_cells, L.cells, L.perm);
+  k_bucket_sort<<<(max_cells + tb - 1) / tb, tb, 0, s>>>(L.cell_off, max_cells, L.cells, L.perm, L.site_pos);
   if (fp64)
     k_site_gather<true><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_code,
-                                                                  L.site_img, L.sq32, L.sq64, L.scode, L.simg);
+                                                                  L.site_img, L.site_pos, L.sq32, L.sq64, L.scode,
+                                                                  L.simg, L.sx);
   else
     k_site_gather<false><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_code,
-                                                                   L.site_img, L.sq32, L.sq64, L.scode, L.simg);
+                                                                   L.site_img, L.site_pos, L.sq32, L.sq64, L.scode,
+                                                                   L.simg, L.sx);
   // 3. sources in Hilbert order
   const int mcells = kOrderDim * kOrderDim * kOrderDim;
   cudaMemsetAsync(L.mcount, 0, sizeof(uint32_t) * (mcells + 1), s);
@@ -1226,8 +1243,8 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
     if (L.nearest_only) kernel = k_near32<true, false, true>;
     // One slice: each warp writes its sources' rows in place, no partial rows to reduce.
     const int direct = slices == 1 ? 1 : 0;
-    kernel<<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.grid, cut, slices,
-                                            direct ? L.out : dst, n, direct);
+    kernel<<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.sx, L.grid, cut,
+                                            slices, direct ? L.out : dst, n, direct);
     if (direct) {
       probe_mark(s);
       probe_count(10 + shell_launches);

@@ -64,6 +64,7 @@ struct NearLaunch {
   float4* sq32;
   double4* sq64;
   uint32_t *scode, *simg;
+  float* sx;  // chart x of each sorted site (sites are sorted by x within each cell)
   uint32_t *src_key, *src_rank, *mcount, *moff, *src_perm;
   NearGrid* grid;
   int* cells;
