@@ -202,7 +202,12 @@ def _blocks(n, size):
         yield start, min(n, start + size)
 
 
-def pair_rows(q, ops, full=False, block=256):
+def _source_rows(n, sources):
+    """The source indices that get rows: all of them, or the given subset (in its order)."""
+    return np.arange(n) if sources is None else np.asarray(sources, np.int64)
+
+
+def pair_rows(q, ops, full=False, block=256, sources=None):
     """Dense FP64 per-source rows over every image j*g_k (shaders/pairs.wgsl:151-244, 266-308).
 
     Returns a dict of per-source arrays:
@@ -210,18 +215,22 @@ def pair_rows(q, ops, full=False, block=256):
       every image but the identity self pair) and nearest_source (its source index, first
       of equal chords in (k, j) order); with `full` also riesz1/2/3, green and log (all
       pairs but the identity self pair, plus the self pair's analytic antipode).
+    With `sources`, only those sources get rows (the arrays follow its order), still
+    summed over every image of the whole sample.
     """
     x_all = normalize(q)
     n = len(x_all)
+    src = _source_rows(n, sources)
+    m = len(src)
     ys = images(x_all, ops)
-    res = {"force": np.zeros((n, 3)), "curvature": np.zeros(n), "energy": np.zeros(n),
-           "nearest": np.full(n, 4.0), "nearest_source": np.full(n, -1, np.int64)}
+    res = {"force": np.zeros((m, 3)), "curvature": np.zeros(m), "energy": np.zeros(m),
+           "nearest": np.full(m, 4.0), "nearest_source": np.full(m, -1, np.int64)}
     if full:
         for key in ("riesz1", "riesz2", "riesz3", "green", "log"):
-            res[key] = np.zeros(n)
-    for i0, i1 in _blocks(n, block):
-        x = x_all[i0:i1, None, :]
-        rows = np.arange(i0, i1)
+            res[key] = np.zeros(m)
+    for i0, i1 in _blocks(m, block):
+        rows = src[i0:i1]
+        x = x_all[rows][:, None, :]
         for k in range(len(ops)):
             y = ys[k][None, :, :]
             minus, plus = x - y, x + y
@@ -285,44 +294,73 @@ def near_pair(x, y, dm2, dp2, r, taper=0.5):
     return force, curv, energy
 
 
-def near_rows(q, ops, delta, taper=0.5, block=256):
+def near_rows(q, ops, delta, taper=0.5, block=256, sources=None):
     """Dense FP64 near-field rows (shaders/pairs.wgsl:363-416 semantics, src/near.zig:1-11).
 
     Source i feels every orbit point (either sign of every image) whose chord to it is at
     most 2 sin(r/2), its own orbit excluded; the nearest is over those points and its own
     images other than the identity one (within the cutoff, as the kernel sees them).
+    Every image is tested (no shell, no grid), so this pins any faster membership rule.
+    With `sources`, only those sources get rows (the arrays follow its order).
     """
     x_all = normalize(q)
     n = len(x_all)
-    r, cut = near_radius(n, len(ops), delta)
-    ys = images(x_all, ops)
-    res = {"force": np.zeros((n, 3)), "curvature": np.zeros(n), "energy": np.zeros(n),
-           "nearest": np.full(n, 4.0), "nearest_source": np.full(n, -1, np.int64), "radius": r, "cut": cut}
-    for i0, i1 in _blocks(n, block):
-        x = x_all[i0:i1, None, :]
-        rows = np.arange(i0, i1)
-        for k in range(len(ops)):
-            for sign in (1.0, -1.0):
-                y = sign * ys[k][None, :, :]
-                minus, plus = x - y, x + y
-                dm2 = (minus * minus).sum(-1)
-                dp2 = (plus * plus).sum(-1)
-                inside = dm2 <= cut
-                own = rows[:, None] == np.arange(n)[None, :]
-                identity = own & (k == 0) & (sign > 0)
-                chord = np.where(inside & ~identity, dm2, 4.0)
-                j = chord.argmin(-1)
-                c = chord[np.arange(len(rows)), j]
-                better = c < res["nearest"][i0:i1]
-                res["nearest"][i0:i1] = np.where(better, c, res["nearest"][i0:i1])
-                res["nearest_source"][i0:i1] = np.where(better, j, res["nearest_source"][i0:i1])
-                pick = inside & ~own
-                if not pick.any():
-                    continue
-                force, curv, energy = near_pair(x, y, dm2, dp2, r, taper)
-                res["force"][i0:i1] += np.where(pick[..., None], force, 0).sum(1)
-                res["curvature"][i0:i1] += np.where(pick, curv, 0).sum(1)
-                res["energy"][i0:i1] += np.where(pick, energy, 0).sum(1)
+    src = _source_rows(n, sources)
+    m = len(src)
+    order = len(ops)
+    r, cut = near_radius(n, order, delta)
+    flat = images(x_all, ops).reshape(-1, 4)  # image k*n + j
+    res = {"force": np.zeros((m, 3)), "curvature": np.zeros(m), "energy": np.zeros(m),
+           "nearest": np.full(m, 4.0), "nearest_source": np.full(m, -1, np.int64), "radius": r, "cut": cut}
+    # Candidates first: for unit vectors |x - s y|^2 = 2 - 2 s x.y, which a matrix product
+    # gives for every image at once; a slack of 1e-12 keeps every point within the cutoff.
+    # Membership itself is then decided on the difference form, as the kernel's semantics
+    # state it, and only the members' pair terms are evaluated.
+    for i0, i1 in _blocks(m, block):
+        rows = src[i0:i1]
+        x = x_all[rows]
+        dot = x @ flat.T
+        for sgn, sign in enumerate((1.0, -1.0)):
+            bi, fi = np.nonzero(2.0 - 2.0 * sign * dot <= cut + 1e-12)
+            if len(bi) == 0:
+                continue
+            xs, y = x[bi], sign * flat[fi]
+            minus, plus = xs - y, xs + y
+            dm2 = (minus * minus).sum(-1)
+            dp2 = (plus * plus).sum(-1)
+            k, j = fi // n, fi % n
+            inside = dm2 <= cut
+            own = rows[bi] == j
+            identity = own & (k == 0) & (sign > 0)
+            # Nearest: smallest chord, first in (k, sign, j) order among equal ones.
+            cand = inside & ~identity
+            if cand.any():
+                b, c, kk, jj = bi[cand], dm2[cand], k[cand], j[cand]
+                pick_order = np.lexsort((jj, kk, c, b))  # by row, chord, then operator, then source
+                first = np.ones(len(pick_order), bool)
+                first[1:] = b[pick_order][1:] != b[pick_order][:-1]
+                win = pick_order[first]
+                rb, rc, rk, rj = b[win] + i0, c[win], kk[win], jj[win]
+                held_k = res.setdefault("_k", np.full(m, 1 << 30))
+                held_s = res.setdefault("_s", np.full(m, 2))
+                cur = res["nearest"][rb]
+                better = (rc < cur) | ((rc == cur) & ((rk < held_k[rb]) | ((rk == held_k[rb]) & (sgn < held_s[rb]))))
+                res["nearest"][rb[better]] = rc[better]
+                res["nearest_source"][rb[better]] = rj[better]
+                held_k[rb[better]] = rk[better]
+                held_s[rb[better]] = sgn
+            pick = inside & ~own
+            if not pick.any():
+                continue
+            xp, yp = xs[pick][:, None, :], y[pick][:, None, :]
+            force, curv, energy = near_pair(xp, yp, dm2[pick][:, None], dp2[pick][:, None], r, taper)
+            b = bi[pick]
+            for a in range(3):
+                res["force"][i0:i1, a] += np.bincount(b, force[:, 0, a], minlength=i1 - i0)
+            res["curvature"][i0:i1] += np.bincount(b, curv[:, 0], minlength=i1 - i0)
+            res["energy"][i0:i1] += np.bincount(b, energy[:, 0], minlength=i1 - i0)
+    res.pop("_k", None)
+    res.pop("_s", None)
     return res
 
 

@@ -77,10 +77,12 @@ static void quey_pair(const double* x, const double* y, double dm2, double dp2, 
 /* All-pairs force rows (quey_partial semantics). q: n x 4 (normalised here), ops: order x 4.
  * Outputs: force n x 3, curvature, energy, nearest chord^2 and its source (first minimum in
  * (k, j) order). Only the first `count` sources get rows (count <= 0: all), so a bounded
- * sample of a large workload can be timed. */
+ * sample of a large workload can be timed; with `sources` (count entries), row r belongs
+ * to source sources[r] instead. */
 void oracle_pair_rows(const double* q_in, int n, const double* ops_in, int order, double* force, double* curv,
-                      double* energy, double* nearest, int64_t* nearest_src, int threads, int count) {
-  const int rows = (count > 0 && count < n) ? count : n;
+                      double* energy, double* nearest, int64_t* nearest_src, int threads, int count,
+                      const int64_t* sources) {
+  const int rows = (count > 0 && (count < n || sources)) ? count : n;
   double* q = (double*)malloc(sizeof(double) * 4 * n);
   double* img = (double*)malloc(sizeof(double) * 4 * (size_t)n * order);
   memcpy(q, q_in, sizeof(double) * 4 * n);
@@ -95,7 +97,8 @@ void oracle_pair_rows(const double* q_in, int n, const double* ops_in, int order
       }
     }
 #pragma omp parallel for schedule(dynamic, 16) num_threads(threads)
-  for (int i = 0; i < rows; ++i) {
+  for (int r = 0; r < rows; ++r) {
+    const int i = sources ? (int)sources[r] : r;
     const double* x = q + 4 * i;
     double f[3] = {0, 0, 0}, c = 0, e = 0, best = 4.0;
     int64_t at = -1;
@@ -117,11 +120,11 @@ void oracle_pair_rows(const double* q_in, int n, const double* ops_in, int order
         if (j == i) continue;
         quey_pair(x, y, dm2, dp2, 0, 0, f, &c, &e);
       }
-    for (int t = 0; t < 3; ++t) force[3 * i + t] = f[t];
-    curv[i] = c;
-    energy[i] = e;
-    nearest[i] = best;
-    nearest_src[i] = at;
+    for (int t = 0; t < 3; ++t) force[3 * r + t] = f[t];
+    curv[r] = c;
+    energy[r] = e;
+    nearest[r] = best;
+    nearest_src[r] = at;
   }
   free(q);
   free(img);
@@ -141,11 +144,12 @@ static double chart_axis(const double* q, int a) { return q[1 + a] / (1.0 + q[0]
  * own orbit excluded from forces, windowed from taper*r (shaders/pairs.wgsl:328-416).
  * Candidate orbit points are the images within the shell of the zone (shell.wgsl:19-39),
  * binned in a grid of the stereographic chart; sources must be zone representatives.
- * Only the first `count` sources get rows (count <= 0: all). */
+ * Only the first `count` sources get rows (count <= 0: all); with `sources` (count entries),
+ * row r belongs to source sources[r] instead. */
 void oracle_near_rows(const double* q_in, int n, const double* ops_in, int order, double delta, double taper,
                       double* force, double* curv, double* energy, double* nearest, int64_t* nearest_src,
-                      int threads, int count) {
-  const int rows = (count > 0 && count < n) ? count : n;
+                      int threads, int count, const int64_t* sources) {
+  const int rows = (count > 0 && (count < n || sources)) ? count : n;
   const double r = fmin(1.5, delta * oracle_mean_radius((double)n * order));
   const double cut = pow(2.0 * sin(r / 2.0), 2), chord = 2.0 * sin(r / 2.0);
   const double cut_z = taper * r, cut_w = 1.0 / fmax(1e-9, (1.0 - taper) * r);
@@ -260,7 +264,8 @@ void oracle_near_rows(const double* q_in, int n, const double* ops_in, int order
   int* order_sites = (int*)malloc(sizeof(int) * S);
   for (int s = 0; s < S; ++s) order_sites[fill[cell_of[s]]++] = s;
 #pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
-  for (int i = 0; i < rows; ++i) {
+  for (int r = 0; r < rows; ++r) {
+    const int i = sources ? (int)sources[r] : r;
     const double* x = q + 4 * i;
     double p[3], f[3] = {0, 0, 0}, c = 0, e = 0, best = 4.0;
     int64_t at = -1;
@@ -309,11 +314,11 @@ void oracle_near_rows(const double* q_in, int n, const double* ops_in, int order
           quey_pair(x, s->q, dm2, dp2, cut_z, cut_w, f, &c, &e);
         }
       }
-    for (int t = 0; t < 3; ++t) force[3 * i + t] = f[t];
-    curv[i] = c;
-    energy[i] = e;
-    nearest[i] = best;
-    nearest_src[i] = at;
+    for (int t = 0; t < 3; ++t) force[3 * r + t] = f[t];
+    curv[r] = c;
+    energy[r] = e;
+    nearest[r] = best;
+    nearest_src[r] = at;
   }
   free(plane);
   free(q);
