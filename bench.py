@@ -49,11 +49,11 @@ FLOPS_PER_NEAR_PAIR = 120
 FLOPS_PER_PAIR = 91
 
 
-def neighbours(n, order, delta):
+def neighbours_of(n, order, delta):
     return min(n * order, 0.94 * delta ** 3 + 64) if delta > 0 else n * order
 
 
-EVALS_PER_PASS = COUNT * neighbours(COUNT, ORDER, DELTA)
+EVALS_PER_PASS = COUNT * neighbours_of(COUNT, ORDER, DELTA)
 
 
 def parse():
@@ -64,8 +64,6 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-extras", action="store_true",
                    help="skip the all-pairs, spacing, batched and served sections")
-    p.add_argument("--cpu-budget", type=float, default=None,
-                   help="seconds of CPU work per reference-arm step (default: a few minutes in all)")
     p.add_argument("--large", action="store_true",
                    help="also time the default measures of group I at N=1M (all pairs, about a minute)")
     return p.parse_args()
@@ -152,48 +150,63 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- CPU baseline (the oracle port)
-def cpu_sample(budget_s=12.0, threads=None):
-    """Time the FP64 C restatement's near-field force rows on the host cores for a bounded
-    subset of the workload's sources; returns pair-evals/s and the sample description."""
+def cpu_relaxation(threads=None):
+    """The workload's plain FP64 relaxation on the host cores: the oracle's BB step
+    (oracle/qvm.py Relax, restating shaders/relax.wgsl) over near-field rows from the C/OpenMP
+    restatement (oracle/qvm_ref.c: shell of images, chart grid, windowed pairs) of all
+    sources. Returns the relaxation and the thread count."""
     from oracle import cref, qvm
 
     ops = np.load(ROOT / "tests/golden/golden.npz")["ops_O"].astype(np.float32).astype(np.float64)
-    q = qvm.fold(qvm.haar(COUNT, SEED), qvm.GROUPS.index(GROUP), ops, f32=False)
+    gid = qvm.GROUPS.index(GROUP)
     threads = threads or cref.threads()
-    per = neighbours(COUNT, ORDER, DELTA)
-    probe = 256
-    t = time.perf_counter()
-    cref.near_rows(q, ops, DELTA, TAPER, nthreads=threads, count=probe)
-    t_probe = time.perf_counter() - t
-    count = int(min(COUNT, max(probe, probe * (budget_s / max(t_probe, 1e-3)) * 0.8)))
-    t = time.perf_counter()
-    cref.near_rows(q, ops, DELTA, TAPER, nthreads=threads, count=count)
-    dt = time.perf_counter() - t
-    return count * per / dt, threads, (f"FP64 near-field force rows of {count} of the {COUNT} sources "
-                                       f"(C/OpenMP restatement, shell+grid setup included), {dt:.1f} s")
+    q = qvm.fold(qvm.haar(COUNT, SEED), gid, ops, f32=False)
+    rows = lambda x: cref.near_rows(x, ops, DELTA, TAPER, nthreads=threads)  # noqa: E731
+    return qvm.Relax(q, gid, ops, delta=DELTA, rows_fn=rows), threads
+
+
+def cpu_steps(relax, count):
+    """Seconds of each of `count` whole BB steps (force pass over every source + update)."""
+    times = []
+    for _ in range(count):
+        t = time.perf_counter()
+        relax.step()
+        times.append(time.perf_counter() - t)
+    return times
+
+
+def cpu_sample(steps=3, warmup=1):
+    """Our line's cpu_baseline: a few whole FP64 steps of the workload on the host cores."""
+    relax, threads = cpu_relaxation()
+    cpu_steps(relax, warmup)
+    times = cpu_steps(relax, steps)
+    per_step = statistics.mean(times)
+    return EVALS_PER_PASS / per_step, threads, (
+        f"{steps} whole FP64 BB steps of the workload after {warmup} untimed (near-field rows of all {COUNT} "
+        f"sources by the C/OpenMP restatement, shell and chart grid rebuilt each step as on the GPU, then the "
+        f"BB update), {per_step:.2f} s per step")
 
 
 def run_reference(args, dist):
-    """Reference arm: the oracle port (the reference itself has no CPU path and cannot run
-    here), on the same workload, each step a bounded sample of one force pass."""
+    """Reference arm: the reference has no CPU implementation of this path and its own
+    engine (Zig + WGSL through wgpu-native) cannot run here, so the arm is the oracle port
+    of the same workload on the host cores: W untimed and K timed whole FP64 steps, each a
+    near-field force pass over all sources and the BB update; ms_per_step is measured."""
     if dist.rank != 0:
         return 0
-    from oracle import cref
-
-    budget = args.cpu_budget or max(2.0, min(15.0, 150.0 / max(1, args.steps + args.warmup)))
-    for _ in range(args.warmup):
-        cpu_sample(budget_s=budget / 4)
-    times, rates = [], []
-    desc, threads = "", cref.threads()
-    for _ in range(args.steps):
-        rate, threads, desc = cpu_sample(budget_s=budget)
-        rates.append(rate)
-    value = statistics.median(rates)
+    relax, threads = cpu_relaxation()
+    cpu_steps(relax, args.warmup)
+    times = cpu_steps(relax, args.steps)
+    per_step = statistics.mean(times)
+    value = EVALS_PER_PASS / per_step
+    desc = (f"{args.steps} timed whole FP64 BB steps after {args.warmup} untimed, all {COUNT} sources each "
+            f"(C/OpenMP near-field rows + oracle BB update), {threads} threads")
     line = {
         "impl": "reference", "metric": "pair-evals/s", "value": value, "unit": "pair-evals/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": EVALS_PER_PASS / value * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": config(args),
+        "step_ms": {"p50": 1e3 * float(np.percentile(times, 50)), "max": 1e3 * max(times)},
         "cpu_baseline": {"value": value, "unit": "pair-evals/s", "cores": threads, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": "pair-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -255,8 +268,10 @@ def e2e_requests(zo, seed, requests):
 
 def batched_section(zo, samples=256, steps=50):
     """Config 4: 256 samples (groups uniform over the eleven, N log-uniform in [1e3, 2e5],
-    seeds 0..255, neighbourhood 20), 50 BB steps each, relaxed side by side; pair-evals/s
-    over the whole batch (steps plus each sample's closing force pass), wall clock."""
+    seeds 0..255, neighbourhood 20), 50 BB steps each, relaxed together by zo_batch_relax:
+    each step is one CUDA graph over all samples, whose near-field gathers run in one
+    persistent launch per tile variant (tile shapes from the tuned table); pair-evals/s over
+    the whole batch (steps plus each sample's closing force pass), wall clock."""
     from zxtalori_b200 import batch, serve
 
     specs = batch.random_samples(samples)
@@ -271,32 +286,60 @@ def batched_section(zo, samples=256, steps=50):
     finally:
         for g in grids:
             g.close()
+    lib = zo.api._library()
+    out = (C.c_double * 2)()
+    shapes = {}
+    for sp in specs:
+        lib.zo_tiles_lookup(0, zo.GROUPS.index(sp.group), sp.count, out)
+        shapes[f"{int(out[0])}x{out[1]:g}"] = shapes.get(f"{int(out[0])}x{out[1]:g}", 0) + 1
     return {"samples": samples, "steps": steps, "sum_n": sum(s.count for s in specs), "pair_evals_per_s": evals / dt,
-            "seconds": dt, "setup_seconds": setup,
+            "seconds": dt, "setup_seconds": setup, "tile_shapes_from_table": shapes,
             "timing": "wall clock of zo_batch_relax (all steps and closing passes), samples created beforehand"}
 
 
-def served_section(zo, rates=(0.4, 0.8, 1.6), duration=15.0, plain_requests=4):
-    """Config 5: Poisson arrivals of relax+measure requests at a swept rate (each rate/s over
-    `duration` s), group uniform, N log-uniform in [500, 1e6], steps uniform in [10, 200],
-    all pairs below 5,000 orientations else neighbourhood 20; continuous batching in
-    FP32-refined mode, and the plain FP64 path one request at a time on the first requests
-    of the middle rate's stream. The middle rate's figures are also the section's own."""
+def served_section(zo, device_rate, factors=(0.6, 1.0, 1.4), per_rate=200, plain_requests=20):
+    """Config 5: Poisson arrivals of relax+measure requests (group uniform, N log-uniform in
+    [500, 1e6], steps uniform in [10, 200], all pairs below 5,000 orientations else
+    neighbourhood 20), served by the continuous-batching loop in FP32-refined mode, at
+    rates below, near and above the GPU's capacity: capacity = the headline's device
+    pair-evals/s over the mean pair evaluations of a request. `per_rate` requests per rate
+    (p50 and p99 from that many latencies). The plain FP64 path serves a fixed subsample
+    (every k-th request of the capacity-rate stream) one at a time; both throughputs count
+    pair evaluations as the reference does (relax steps and closing pass)."""
     from zxtalori_b200 import serve
 
+    probe = serve.poisson_requests(1.0, 20_000.0, seed=11)
+    mean_evals = float(np.mean([(r.steps + 1) * r.count * serve.neighbours(r.count, serve.ORDER[r.group],
+                                                                           r.neighbourhood) for r in probe]))
+    capacity = device_rate / mean_evals
     sweep = []
-    for rate in rates:
-        reqs = serve.poisson_requests(rate, duration, seed=5)
+    streams = {}
+    for f in factors:
+        rate = f * capacity
+        reqs = serve.poisson_requests(rate, 1.5 * per_rate / rate, seed=5)[:per_rate]
+        streams[f] = reqs
         t = time.perf_counter()
         served = serve.Server().run(reqs)
         wall = time.perf_counter() - t
-        sweep.append({"rate_per_s": rate, "arrival_window_s": duration, "wall_s": wall, **serve.summary(served)})
+        sweep.append({"rate_per_s": rate, "rate_over_capacity": f, "wall_s": wall,
+                      "arrival_window_s": reqs[-1].arrival, **serve.summary(served)})
     middle = sweep[len(sweep) // 2]
-    reqs = serve.poisson_requests(middle["rate_per_s"], duration, seed=5)
-    first = sorted(reqs, key=lambda r: r.arrival)[:plain_requests]
-    plain = serve.summary(serve.serve_one_at_a_time([serve.Request(r.id, r.group, r.count, r.steps, r.seed,
-                                                                   r.neighbourhood, 0.0) for r in first]))
-    return {**middle, "sweep": sweep, "plain_fp64_one_at_a_time": plain, "plain_requests": plain_requests}
+    stream = streams[factors[len(factors) // 2]]
+    stride = max(1, len(stream) // plain_requests)
+    chosen = stream[::stride][:plain_requests]
+    plain_in = [serve.Request(r.id, r.group, r.count, r.steps, r.seed, r.neighbourhood, 0.0) for r in chosen]
+    t = time.perf_counter()
+    plain = serve.summary(serve.serve_one_at_a_time(plain_in))
+    plain["wall_s"] = time.perf_counter() - t
+    # The same subsample served by the batching loop, for a like-for-like throughput ratio.
+    same = serve.summary(serve.Server().run([serve.Request(r.id, r.group, r.count, r.steps, r.seed,
+                                                           r.neighbourhood, 0.0) for r in chosen]))
+    return {**{k: middle[k] for k in ("requests", "pair_evals_per_s", "latency_p50_s", "latency_p99_s")},
+            "capacity_requests_per_s": capacity, "mean_pair_evals_per_request": mean_evals,
+            "sweep": sweep, "plain_fp64_one_at_a_time": plain, "served_same_subsample": same,
+            "served_over_plain_same_subsample": same["pair_evals_per_s"] / plain["pair_evals_per_s"],
+            "requests_measured": "every request runs measure() after its steps (every energy ratio below "
+                                 "the ratio limit)"}
 
 
 def _device_seconds(lib, handle, steps, warmup):
@@ -341,10 +384,12 @@ def allpairs_section(zo, peak, count=1048, steps=30, kernel_count=16384):
     return result
 
 
-def spacing_section(zo, count=10_000_000, seed=7, measure_count=None):
+def spacing_section(zo, peak, count=10_000_000, seed=7, measure_count=None):
     """Config 3: the spacing pass (per-orientation nearest SO(3) angle and neighbour index;
-    neighbourhood 4 above 20,000 orientations) over group I, N=10M Haar seed 7, wall clock
-    through the public API (the second of two calls: the first sizes the workspace); with
+    neighbourhood 4 above 20,000 orientations) over group I, N=10M Haar seed 7: wall clock
+    through the public API (the second of two calls: the first sizes the workspace), device
+    time per pass and the gather kernel's HBM roofline from zo_bench_spacing, and the
+    indices and angles checked against the FP64 method on the same float32 sample. With
     `measure_count`, the default measures of I at that size (all pairs, FP32)."""
     g = zo.haar("I", count, seed)
     t = time.perf_counter()
@@ -354,11 +399,36 @@ def spacing_section(zo, count=10_000_000, seed=7, measure_count=None):
     sep = g.spacing()["separation_deg"]
     dt = time.perf_counter() - t
     degrees = g.point_values("separation")
+    neighbours = g.point_neighbours()
+    exact = g.spacing_exact()
+    q = g.quaternions
+    out = np.zeros(6, np.float64)
+    g._check(g._lib.zo_bench_spacing(g._handle, 5, 1, float(FLUSH_BYTES), out.ctypes.data_as(C.POINTER(C.c_double)),
+                                     len(out)))
     g.close()
-    n_pairs = count * neighbours(count, 60, 4.0)
+    n_pairs = count * neighbours_of(count, 60, 4.0)
+    # Algorithmic bytes of one gather launch: every source read once (16 B), every shell
+    # site read once (16 B position + 4 B code + 4 B chart x), the nearest chord (8 B) and
+    # site (4 B) written per source.
+    sites = out[3]
+    algorithmic = count * 16 + sites * 24 + count * 12
+    achieved = algorithmic / (out[1] * 1e-3) / 1e9
     result = {"workload": f"I, N={count} Haar (seed {seed}), spacing with neighbourhood 4",
               "seconds": dt, "first_call_seconds": first, "pair_evals_per_s": n_pairs / dt,
-              "separation_deg": sep, "median_nearest_deg": float(np.median(degrees))}
+              "device_ms_per_pass": out[0], "separation_deg": sep, "median_nearest_deg": float(np.median(degrees)),
+              "exact_search_points": exact["exact_search"], "exact_ties": exact["exact_ties"],
+              "roofline": {"bound": "hbm", "kernel": "k_near32<nearest only> (spacing gather)",
+                           "kernel_ms_avg": out[1], "launches": int(out[2]), "shell_sites": int(sites),
+                           "algorithmic_bytes": algorithmic, "achieved": achieved, "peak": peak[0],
+                           "peak_source": peak[1], "unit": "GB/s", "frac": achieved / peak[0]}}
+    # The same float32 sample through the FP64 method: indices must agree except exact ties.
+    g64 = zo.from_quaternions(q, "I", precision="fp64")
+    g64.spacing()
+    d64, n64 = g64.point_values("separation"), g64.point_neighbours()
+    g64.close()
+    mismatched = int(np.count_nonzero(neighbours != n64))
+    result["vs_fp64"] = {"index_mismatches": mismatched, "index_mismatches_allowed": exact["exact_ties"],
+                         "degrees_max_rel_error": float(np.max(np.abs(degrees - d64) / d64))}
     if measure_count:
         g = zo.haar("I", measure_count, seed)
         t = time.perf_counter()
@@ -369,6 +439,111 @@ def spacing_section(zo, count=10_000_000, seed=7, measure_count=None):
         result["measure"] = {"n": measure_count, "seconds": dt, "pair_evals_per_s": pairs / dt,
                              "quey_energy": m["quey_energy"], "separation_deg": m["separation_deg"]}
     return result
+
+
+def hbm_peak():
+    """HBM copy bandwidth in GB/s and where it comes from: the measured figure in
+    MEASURED_PEAKS.json when present, else an earlier copy measurement on B200 (6,650 GB/s)."""
+    try:
+        data = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        for key in ("hbm_gbs", "hbm_GBs", "hbm_copy_gbs"):
+            if isinstance(data.get(key), (int, float)):
+                return float(data[key]), "measured (MEASURED_PEAKS.json)"
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "fallback (earlier B200 copy measurement)"
+
+
+def _rel(a, b):
+    return abs(a - b) / abs(b) if b else abs(a - b)
+
+
+def _chord(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.minimum(np.linalg.norm(a - b, axis=1), np.linalg.norm(a + b, axis=1))
+
+
+def _nudged(q):
+    """Every component moved by one float32 ulp, in a seeded random direction."""
+    q = np.asarray(q, np.float32)
+    up = np.random.default_rng(0).random(q.shape) < 0.5
+    return np.nextafter(q, np.where(up, np.float32(np.inf), np.float32(-np.inf))).astype(np.float32)
+
+
+def errors_section(zo):
+    """Every result's error against the FP64 method (the plain path: FP64 arithmetic,
+    positions and sums throughout), for configs 1 and 2, three ways:
+    - trajectory: the FP32-refined run against the FP64 run from the same start;
+    - same sample: the FP32-refined engine's measures of its own relaxed sample against the
+      FP64 method's measures of that same float32 sample (the arithmetic alone);
+    - conditioning: the FP64 run against itself started one float32 ulp away. A relaxed
+      sample's minimum separation follows the trajectory's sensitivity to its start, so
+      this is the floor below which no trajectory comparison can go."""
+    keys = ("quey_energy", "separation_deg", "riesz_1", "riesz_2", "riesz_3", "green_ratio", "log_ratio")
+    out = {}
+    # Config 1: O, N=1,048, all pairs, 30 steps, then every measure.
+    def run1(precision, q=None):
+        g = zo.haar("O", 1048, SEED, precision=precision) if q is None else zo.from_quaternions(q, "O", precision)
+        start = g.quaternions
+        g.relax(30)
+        m, q_end = g.measure(), g.quaternions
+        g.close()
+        return m, q_end, start
+
+    m64, q64, start = run1("fp64")
+    m32, q32, _ = run1("fp32")
+    g = zo.from_quaternions(q32, "O", precision="fp64")
+    same = g.measure()
+    g.close()
+    m64n, q64n, _ = run1("fp64", _nudged(start))
+    m64s, _, _ = run1("fp64", start)  # the same start imported, for the comparison above
+    out["config1"] = {
+        "workload": "O, N=1048 Haar (seed 193), all pairs, 30 BB steps, then measure()",
+        "trajectory": {**{k: _rel(m32[k], m64[k]) for k in keys}, "positions_chord_max": float(_chord(q32, q64).max())},
+        "same_sample": {k: _rel(m32[k], same[k]) for k in keys},
+        "conditioning": {**{k: _rel(m64n[k], m64s[k]) for k in keys},
+                         "positions_chord_max": float(_chord(q64n, q64).max())},
+    }
+    # Config 2: O, N=100,000, neighbourhood 20, 100 steps.
+    def run2(precision, q=None):
+        g = zo.haar(GROUP, COUNT, SEED, precision=precision) if q is None else zo.from_quaternions(q, GROUP, precision)
+        start = g.quaternions
+        g.relax(STEPS_PER_REQUEST, neighbourhood=DELTA)
+        st, q_end = g.stats, g.quaternions
+        g.close()
+        return st, q_end, start
+
+    def all_pairs(q):
+        g = zo.from_quaternions(q, GROUP, precision="fp64")
+        g.relax(0, neighbourhood=0)
+        m = g.measure()  # above O's ratio limit: energy and separation over all pairs
+        g.close()
+        return m
+
+    s64, p64, start = run2("fp64")
+    s32, p32, _ = run2("fp32")
+    s64n, p64n, _ = run2("fp64", _nudged(start))
+    s64s, p64s, _ = run2("fp64", start)
+    g = zo.from_quaternions(p32, GROUP, precision="fp64")
+    g.relax(0, neighbourhood=DELTA)
+    near_same = g.stats
+    g.close()
+    a32, a64, a64s, a64n = all_pairs(p32), all_pairs(p64), all_pairs(p64s), all_pairs(p64n)
+    near = ("quey_energy", "separation_deg")
+    chords = _chord(p32, p64)
+    out["config2"] = {
+        "workload": f"{GROUP}, N={COUNT} Haar (seed {SEED}), neighbourhood {DELTA:g}, {STEPS_PER_REQUEST} BB steps",
+        "trajectory": {**{f"near_{k}": _rel(s32[k], s64[k]) for k in near},
+                       **{f"allpairs_{k}": _rel(a32[k], a64[k]) for k in near},
+                       "positions_chord_max": float(chords.max()),
+                       "positions_chord_p99": float(np.percentile(chords, 99))},
+        "same_sample": {f"near_{k}": _rel(s32[k], near_same[k]) for k in near},
+        "conditioning": {**{f"near_{k}": _rel(s64n[k], s64s[k]) for k in near},
+                         **{f"allpairs_{k}": _rel(a64n[k], a64s[k]) for k in near},
+                         "positions_chord_max": float(_chord(p64n, p64s).max())},
+        "fp64_allpairs": {k: a64[k] for k in near},
+    }
+    return out
 
 
 def traffic_from_profile():
@@ -419,9 +594,10 @@ def run_ours(args, dist):
     extras = {}
     if args.gpus == 1 and not args.no_extras:
         extras["allpairs"] = allpairs_section(zo, peak)
-        extras["spacing"] = spacing_section(zo, measure_count=1_000_000 if args.large else None)
+        extras["spacing"] = spacing_section(zo, hbm_peak(), measure_count=1_000_000 if args.large else None)
+        extras["errors_vs_fp64"] = errors_section(zo)
         extras["batched"] = batched_section(zo)
-        extras["served"] = served_section(zo)
+        extras["served"] = served_section(zo, value)
     kernel_avg_s = kernel_ms / max(1, kernel_launches) / 1e3
     achieved = EVALS_PER_PASS * FLOPS_PER_NEAR_PAIR / kernel_avg_s / 1e12
     traffic = traffic_from_profile()

@@ -98,6 +98,27 @@ uint32_t zo_get_precision(void* h);
 /* Extension: the nearest orbit neighbour's source index of every point (same pass as
  * zo_point_values kind 0), or NULL before such a pass. */
 const int32_t* zo_point_neighbours(void* h);
+/* Tuning extension, no reference counterpart: the tile shape of this engine's FP32
+ * near-field gathers (relaxation and spacing), instead of the tile table's choice:
+ * sources per warp 2, 4 or 8 and target shell sites per chart cell (0.5..16); applies from
+ * the next pass (the workspace is sized again). sources_per_warp 0 returns to the table.
+ * The reference's tiling knobs are constants (src/pairs.zig:100-128, src/near.zig:22-29). */
+int zo_near_tiles(void* h, uint32_t sources_per_warp, float sites_per_cell);
+/* The tile table's choice for a pass kind (0 relaxation, 1 spacing), group and sample size:
+ * out[0] sources per warp, out[1] sites per chart cell. The table (near_tiles.txt beside the
+ * library's folder, or $ZXTALORI_TILES) is read once per process. Needs no GPU; -1 on a bad
+ * argument. */
+int zo_tiles_lookup(uint32_t kind, uint32_t group, uint32_t n, double* out);
+/* Extension, no reference counterpart: the device memory the engine holds now, in bytes
+ * (positions, rows, BB history, near-field workspace, measure scratch; all of it from the
+ * library's per-device pool). A request server admits samples by it. */
+uint64_t zo_device_bytes(void* h);
+/* Extension, no reference counterpart: of the last zo_spacing pass (FP32 mode, near field
+ * above 20,000 points), out[0] = points whose nearest neighbour the exact FP64 search
+ * settled (the FP32 gather could not prove its own choice), out[1] = points whose nearest
+ * distance two different points share exactly (exact ties, broken by the lower index).
+ * Zeros for all-pairs or FP64-mode passes. Waits for the engine's stream. */
+int zo_spacing_exact(void* h, uint32_t* out);
 /* Development hook, in the spirit of the reference's dev symbols (src/native_api.zig:150-175):
  * one pass's raw per-source rows into `out` (the caller's n * width doubles).
  * what 0: the relaxation's force pass (all pairs, or the near field when a neighbourhood is
@@ -107,12 +128,22 @@ const int32_t* zo_point_neighbours(void* h);
  *   Riesz 1, 2, 3, Green, log sums (the self pair's antipode not yet added), degenerate
  *   flag (width 12). */
 int zo_debug_rows(void* h, uint32_t what, double* out);
+/* Development hook (no reference counterpart): the next near-field pass, of the relaxation
+ * or of the spacing pass, sizes its shell workspace for only `sites` sites, once (0
+ * cancels). A pass that then produces more sites than that overflows, and the engine's
+ * resize-and-redo path runs as after a real overflow (src/pairs.zig:391-394, near.zig:191-195). */
+int zo_debug_shell_capacity(void* h, uint32_t sites);
 /* Measurement hook (no reference counterpart): `steps` relaxation steps of the current
  * sample after `warmup`, each timed with CUDA events on the engine's stream and preceded,
  * outside its events, by a memset of flush_bytes (an L2 flush when larger than L2).
  * out[0] total step ms, out[1] ms of the force pass's row kernel, out[2] its launches,
  * out[3] kernel launches per step, out[4 ..] per-step ms while out_len allows. */
 int zo_bench(void* h, uint32_t steps, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len);
+/* Measurement hook (no reference counterpart): `passes` spacing passes after `warmup`
+ * (src/engine.zig:334-347 is one pass), timed like zo_bench. out[0] ms per pass, out[1] ms
+ * per launch of the nearest-only gather kernel, out[2] its launches, out[3] shell sites,
+ * out[4] points settled by the exact FP64 search, out[5] kernel launches per pass. */
+int zo_bench_spacing(void* h, uint32_t passes, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len);
 /* Extensions (no reference counterpart): relaxation in two halves, so many engines relax
  * concurrently. zo_relax_async enqueues `steps` BB steps on the engine's stream and returns
  * at once (in FP32 mode each step replays a CUDA graph captured from the first one);
@@ -123,8 +154,11 @@ int zo_relax_async(void* h, uint32_t steps);
 int zo_relax_finish(void* h);
 int zo_idle(void* h);
 int zo_graphs(void* h, uint32_t enabled);
-/* Extension: relax `count` engines by `steps` each, side by side on their own streams, then
- * finish each; status[k] is 0 or -1 (message in zo_error(handles[k])). Returns failures. */
+/* Extension: relax `count` engines by `steps` each, then finish each; status[k] is 0 or -1
+ * (message in zo_error(handles[k])); returns the failures. FP32 engines with graphs on (per
+ * device) step together: each step is one CUDA graph over all of them, and the near-field
+ * gathers of all of them run in one persistent launch. Each result is the same as the
+ * engine's own zo_relax would give. Other engines step one launch at a time alongside. */
 int zo_batch_relax(void* const* handles, uint32_t count, uint32_t steps, int32_t* status);
 /* Measurement hook (no reference counterpart): FP32 FMA throughput of the engine's device
  * in TFLOP/s (2 flops per FMA), the denominator of the pair kernels' roofline; -1 on error. */
@@ -152,7 +186,9 @@ int64_t zo_hopf_points(uint32_t group, uint32_t freq, float* out, uint64_t capac
  *                smallest squared chord to another orbit point;
  *   stream:      the cudaStream_t to run on (NULL: the default stream).
  * Returns 0, or -1 bad argument, -2 n outside 1..65,536 (the scratch's limit), -3 CUDA
- * error; the message goes to `error` (error_len bytes) when given. The first call on a
+ * error (also when an error from the caller's earlier work is still pending on the thread:
+ * the call then launches nothing and leaves that error pending); the message goes to
+ * `error` (error_len bytes) when given. The first call on a
  * device sets it up (scratch address, group tables); make it before any stream capture.
  * Calls share the scratch: calls that overlap on the GPU race and must be serialised. */
 int zo_pair_rows_noalloc(uint32_t group, const float* q_device, uint32_t n, double* rows_device, void* stream,

@@ -46,10 +46,11 @@ def test_barrier_and_reductions_over_two_ranks(tmp_path):
 
 def test_reference_arm_under_torchrun_prints_one_line():
     """bench.py --impl reference launched as the driver launches it for N=2: rank 0 times the
-    oracle port and prints one JSON line, the other rank exits 0 without work."""
+    oracle port (one whole FP64 step here) and prints one JSON line, the other rank exits 0
+    without work."""
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
            "127.0.0.1", "--master-port", str(free_port()), str(ROOT / "bench.py"), "--impl", "reference", "--gpus",
-           "2", "--steps", "1", "--warmup", "1", "--cpu-budget", "0.5"]
+           "2", "--steps", "1", "--warmup", "0"]
     env = dict(os.environ, OMP_NUM_THREADS="2")
     done = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT, env=env)
     assert done.returncode == 0, done.stderr[-2000:]
@@ -58,5 +59,6 @@ def test_reference_arm_under_torchrun_prints_one_line():
     line = lines[0]
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["metric"] == "pair-evals/s"
     assert line["value"] > 0 and line["cpu_baseline"]["kind"] == "port"
+    assert line["ms_per_step"] == line["step_ms"]["p50"]  # measured, one step
     assert line["e2e"] == {"value": line["value"], "unit": "pair-evals/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}

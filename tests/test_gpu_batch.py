@@ -44,6 +44,48 @@ def test_batch_matches_alone(engine, ops32):
         assert s_mix["iteration"] == 10
 
 
+# (group, N, seed, neighbourhood, tile shape forced or None, precision): the shared gather's
+# chord form (O 40k, cutoff 0.27 rad) and arctangent form (O 3000, I 1500: 0.59-0.64 rad),
+# a forced tile shape (8 sources per warp, 3 sites per cell), a dense cutoff (C2 2000: every
+# image tested), all pairs, and an FP64 engine, which steps alongside the shared launches.
+MIX = [("O", 40000, 11, 20.0, None, "fp32"), ("O", 3000, 12, 20.0, None, "fp32"),
+       ("I", 1500, 13, 20.0, (8, 3.0), "fp32"), ("D6", 6000, 14, 20.0, (2, 1.5), "fp32"),
+       ("C2", 2000, 15, 20.0, None, "fp32"), ("C4", 900, 16, 0.0, None, "fp32"), ("T", 1200, 17, 20.0, None, "fp64")]
+
+
+def _mix_grid(engine, group, n, seed, delta, tiles, precision):
+    g = engine.haar(group, n, seed, precision=precision)
+    if tiles:
+        g._check(g._lib.zo_near_tiles(g._handle, tiles[0], tiles[1]))
+    g._check(g._lib.zo_relax_neighbourhood(g._handle, delta))
+    return g
+
+
+def test_shared_gather_batch_matches_alone(engine):
+    """zo_batch_relax with every kind of sample: each result equals its own zo_relax, bit for
+    bit, over 12 steps (the first direct, then one graph for the whole batch, replayed), and
+    again over a second call (the step after a closing pass)."""
+    from zxtalori_b200 import batch
+
+    grids = [_mix_grid(engine, *m) for m in MIX]
+    try:
+        first = batch.relax_batch(grids, 12)
+        q_first = [g.quaternions for g in grids]
+        second = batch.relax_batch(grids, 5)
+        q_second = [g.quaternions for g in grids]
+    finally:
+        for g in grids:
+            g.close()
+    for m, s1, q1, s2, q2 in zip(MIX, first, q_first, second, q_second):
+        with _mix_grid(engine, *m) as alone:
+            alone.relax(12)
+            assert np.array_equal(alone.quaternions, q1), m
+            assert alone.stats["energy"] == s1["energy"] and s1["iteration"] == 12
+            alone.relax(5)
+            assert np.array_equal(alone.quaternions, q2), m
+            assert alone.stats["energy"] == s2["energy"] and s2["iteration"] == 17
+
+
 def test_server_results_same_alone_and_in_mix(engine):
     from zxtalori_b200 import serve
 

@@ -132,3 +132,30 @@ def test_near_relax_fp32_vs_fp64(engine):
     assert s["energy"] == pytest.approx(s64["energy"], rel=1e-6)
     assert s["separation_deg"] == pytest.approx(s64["separation_deg"], rel=1e-4)
     assert np.minimum(np.linalg.norm(q - q64, axis=1), np.linalg.norm(q + q64, axis=1)).max() < 1e-4
+
+
+@pytest.mark.parametrize("sources_per_warp,sites_per_cell", [(2, 1.5), (2, 3.0), (8, 1.5), (8, 3.0), (4, 2.0)])
+def test_every_tile_shape_matches_the_oracle(engine, ops32, sources_per_warp, sites_per_cell):
+    """Each tile shape the tuner may choose (zo_near_tiles) gives the oracle's rows (near
+    field, O 30k) and the oracle's spacing indices (I 40k)."""
+    with engine.haar("O", 30000, 23) as grid:
+        grid._check(grid._lib.zo_near_tiles(grid._handle, sources_per_warp, sites_per_cell))
+        grid.relax(0, neighbourhood=20)
+        rows = grid.debug_rows(0)
+        q = grid.quaternions.astype(np.float64)
+    compare(rows, cref.near_rows(q, ops32["O"], 20), "fp32")
+    with engine.haar("I", 40000, 29) as grid:
+        grid._check(grid._lib.zo_near_tiles(grid._handle, sources_per_warp, sites_per_cell))
+        grid.spacing()
+        neighbours = grid.point_neighbours()
+        q = grid.quaternions.astype(np.float64)
+    assert np.array_equal(neighbours, cref.near_rows(q, ops32["I"], 4)["nearest_source"])
+
+
+def test_tile_override_rejects_bad_shapes(engine):
+    with engine.haar("O", 1000, 3) as grid:
+        with pytest.raises(RuntimeError, match="InvalidTiles"):
+            grid._check(grid._lib.zo_near_tiles(grid._handle, 3, 2.0))
+        with pytest.raises(RuntimeError, match="InvalidTiles"):
+            grid._check(grid._lib.zo_near_tiles(grid._handle, 4, 100.0))
+        grid._check(grid._lib.zo_near_tiles(grid._handle, 0, 0.0))  # back to the table

@@ -1,8 +1,12 @@
 """Spacing pass: per-point nearest orbit neighbour (SO(3) degrees) and its source index.
 
 Indices are compared exactly with the FP64 oracle (documented exception: exact-distance
-ties, which seeded Haar samples do not produce); degrees to 1e-6 relative. Above 20,000
-orientations the pass uses the near field of 4 mean radii, compared with the FP64 C oracle.
+ties, which seeded Haar samples do not produce; the engine counts them); degrees to 1e-6
+relative. Above 20,000 orientations the pass uses the near field of 4 mean radii, compared
+with the FP64 C oracle (pinned to the dense oracle by tests/test_oracle_pin.py). The FP32
+gather walks 2.5 of the 4 mean radii first and keeps the two best chords; a point whose
+choice it cannot prove (second best within the FP32 chord error, or nearest possibly beyond
+the first ball) goes to the exact FP64 search.
 """
 import numpy as np
 import pytest
@@ -53,3 +57,57 @@ def test_point_values_track_runs(engine):
         grid.relax(10)
         assert grid.point_values("separation") is not None
         assert grid.stats["point_separation_iteration"] == grid.stats["iteration"]
+
+
+def _spacing_vs_oracle(engine, ops32, group, count, seed, q_in=None):
+    gid = GROUPS.index(group)
+    ops = ops32[group]
+    grid = engine.haar(group, count, seed) if q_in is None else engine.from_quaternions(q_in, group)
+    with grid:
+        grid.spacing()
+        degrees = grid.point_values("separation")
+        neighbours = grid.point_neighbours()
+        report = grid.spacing_exact()
+        q = grid.quaternions.astype(np.float64)
+    rows = cref.near_rows(q, ops, 4)
+    expected = qvm.nearest_degrees(rows)
+    mismatched = np.flatnonzero(neighbours != rows["nearest_source"])
+    assert len(mismatched) == 0, (len(mismatched), mismatched[:10], report)
+    np.testing.assert_allclose(degrees, expected, rtol=1e-6)
+    assert report["exact_ties"] == 0
+    return report
+
+
+def test_spacing_indices_exact_at_one_million(engine, ops32):
+    """Config 3's group and seed at N=1M: every index equals the FP64 oracle's; the exact
+    search settles the few hundred points whose two best FP32 chords are within error."""
+    report = _spacing_vs_oracle(engine, ops32, "I", 1_000_000, 7)
+    assert 0 < report["exact_search"] < 20_000
+
+
+@pytest.mark.slow
+def test_spacing_indices_exact_at_ten_million(engine, ops32):
+    """Config 3's spacing workload itself: I, N=10M, seed 7."""
+    report = _spacing_vs_oracle(engine, ops32, "I", 10_000_000, 7)
+    assert report["exact_search"] < 200_000
+
+
+def test_spacing_exact_search_beyond_first_ball(engine, ops32):
+    """A point whose whole neighbourhood within 3.2 mean radii is emptied has its nearest
+    beyond the first walk's 2.5 radii: the exact search over the full 4 radii finds it."""
+    group, count = "I", 60_000
+    gid = GROUPS.index(group)
+    ops = ops32[group]
+    q = qvm.fold(qvm.haar(count, 13), gid, ops, f32=True).astype(np.float64)
+    radius = qvm.mean_radius(count * len(ops))
+    x = qvm.normalize(q)
+    chord = 2 * np.sin(3.2 * radius / 2)
+    far = np.ones(count, bool)
+    for k in range(len(ops)):
+        y = qvm.normalize(qvm.qmul(x, ops[k]))
+        d = np.minimum(np.linalg.norm(y - x[0], axis=1), np.linalg.norm(y + x[0], axis=1))
+        far &= d > chord
+    far[0] = True
+    q_in = q[far].astype(np.float32)
+    report = _spacing_vs_oracle(engine, ops32, group, int(far.sum()), 0, q_in=q_in)
+    assert report["exact_search"] >= 1

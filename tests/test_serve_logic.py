@@ -24,6 +24,13 @@ class FakeLib:
         self.log.append(("finish", h.request_id))
         return 0
 
+    def zo_measure(self, h):
+        self.log.append(("measure", h.request_id))
+        return 0
+
+    def zo_device_bytes(self, h):
+        return serve.estimate_bytes(h.count, h.group, h.neighbourhood)
+
 
 class FakeGrid:
     live = 0
@@ -103,10 +110,10 @@ def test_every_request_runs_exactly_its_steps(fake):
     for r in results:
         assert r.stats["iteration"] == reqs[r.id].steps
         assert r.finished >= r.admitted >= r.arrival
-    # Each sample is finished once, after all its steps.
+    # Each sample is finished and measured once, after all its steps.
     for k in range(3):
         events = [e for e in log if e[1] == k]
-        assert events[-1] == ("finish", k)
+        assert events[-2:] == [("finish", k), ("measure", k)]
         assert sum(e[2] for e in events if e[0] == "steps") == reqs[k].steps
     assert FakeGrid.live == 0
 
@@ -124,6 +131,23 @@ def test_admission_respects_budget_and_cap(fake):
     reqs = _requests(ids, specs)
     serve.Server(memory_budget=1 << 40, max_active=3, chunk_seconds=1e-6).run(reqs, clock=Clock())
     assert FakeGrid.most_live == 3
+
+
+def test_admission_uses_the_engines_reported_bytes(fake, monkeypatch):
+    """Once a sample's workspace is sized, admission counts the bytes its engine reports:
+    engines that hold twice their estimate leave room for fewer samples."""
+    log, ids = fake
+    specs = [("O", 3000, 200, 0.0, 0.01 * k) for k in range(6)]
+    one = serve.estimate_bytes(3000, "O", 0.0)
+    reqs = _requests(ids, specs)
+    serve.Server(memory_budget=3 * one, chunk_seconds=1e-6).run(reqs, clock=Clock())
+    assert FakeGrid.most_live == 3
+    monkeypatch.setattr(FakeLib, "zo_device_bytes", lambda self, h: 2 * one)
+    FakeGrid.most_live = 0
+    ids.clear()
+    reqs = _requests(ids, specs)
+    results = serve.Server(memory_budget=3 * one, chunk_seconds=1e-6).run(reqs, clock=Clock())
+    assert FakeGrid.most_live == 2 and len(results) == 6
 
 
 def test_oversize_request_runs_alone(fake):

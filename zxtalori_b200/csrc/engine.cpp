@@ -7,7 +7,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <dlfcn.h>
+
+#include <map>
 #include <mutex>
+#include <tuple>
 
 namespace zo {
 
@@ -17,6 +21,10 @@ constexpr uint32_t kMaxCount = 10000000;          // hopf.max_count (src/hopf.zi
 constexpr double kFullMeasurePairs = 5e10;        // src/engine.zig:1123
 constexpr uint32_t kSpacingAllPairs = 20000;      // src/engine.zig:1126
 constexpr double kSpacingDelta = 4;               // src/engine.zig:1127
+// The spacing pass's first walk covers 2.5 of the 4 mean radii (about 15 neighbours
+// expected, against about 60): nearly every source's nearest lies within it, and the
+// few that do not are searched again over the whole cutoff.
+constexpr double kSpacingWalk = 2.5 / 4.0;
 // Near field over every image ("dense") or over the chart grid. FP64 mode: dense from a
 // 0.5 rad cutoff on. FP32 mode (the gather walks exact chart balls): dense from 0.9 rad on,
 // or from 0.5 rad for samples of at most 1e8 image pairs, where the grid's fixed cost and
@@ -26,21 +34,30 @@ constexpr double kDenseRadius32 = 0.9;
 constexpr double kDenseSmallPairs = 1e8;
 constexpr const char* kVersion = "0.3.0";
 
-std::mutex g_tables_mutex;
-bool g_tables_uploaded[64] = {false};
-
 void ensure_tables(int device) {
-  std::lock_guard<std::mutex> lock(g_tables_mutex);
-  if (device < 0 || device >= 64) throw Failure("InvalidDevice");
-  if (g_tables_uploaded[device]) return;
-  ZO_CUDA(upload_tables(host_tables()));
-  g_tables_uploaded[device] = true;
+  if (device < 0 || device >= kMaxTableDevices) throw Failure("InvalidDevice");
+  ZO_CUDA(ensure_device_tables(device));
 }
 
 double separation_of(double chord2) {
   return 4.0 * std::asin(std::min(1.0, std::sqrt(std::max(chord2, 0.0)) / 2.0)) * 180.0 / kPiH;
 }
 }  // namespace
+
+// One upload flag per device, shared by engines and the allocation-free entry point.
+namespace {
+std::mutex g_tables_mutex;
+bool g_tables_uploaded[kMaxTableDevices] = {false};
+}  // namespace
+
+cudaError_t ensure_device_tables(int device) {
+  if (device < 0 || device >= kMaxTableDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_tables_mutex);
+  if (g_tables_uploaded[device]) return cudaSuccess;
+  const cudaError_t e = upload_tables(host_tables());
+  if (e == cudaSuccess) g_tables_uploaded[device] = true;
+  return e;
+}
 
 void check_cuda(cudaError_t e, const char* what) {
   if (e == cudaSuccess) return;
@@ -95,11 +112,73 @@ Rows RowBuffers::ensure(size_t n) {
 }
 
 // ------------------------------------------------------------------ near field
-void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_r, int sms) {
+// ------------------------------------------------------------------ tile table
+namespace {
+struct TileTable {
+  std::map<std::tuple<int, int, int>, NearTiles> entries;  // (kind, group, log2 bucket)
+};
+
+std::string tile_table_path() {
+  if (const char* env = std::getenv("ZXTALORI_TILES")) return env;
+  Dl_info info;
+  if (dladdr(reinterpret_cast<void*>(&lookup_tiles), &info) && info.dli_fname) {
+    std::string lib = info.dli_fname;
+    const size_t slash = lib.rfind('/');
+    const std::string dir = slash == std::string::npos ? std::string(".") : lib.substr(0, slash);
+    return dir + "/../near_tiles.txt";
+  }
+  return "near_tiles.txt";
+}
+
+const TileTable& tile_table() {
+  static std::once_flag once;
+  static TileTable table;
+  std::call_once(once, [] {
+    FILE* f = std::fopen(tile_table_path().c_str(), "r");
+    if (!f) return;
+    char line[256];
+    while (std::fgets(line, sizeof line, f)) {
+      char kind[32], group[8];
+      int bucket = 0, g = 0;
+      double spc = 0;
+      if (line[0] == '#' || std::sscanf(line, "%31s %7s %d %d %lf", kind, group, &bucket, &g, &spc) != 5) continue;
+      const int k = std::strcmp(kind, "spacing") == 0 ? kTilesSpacing : std::strcmp(kind, "relax") == 0 ? kTilesRelax : -1;
+      int gid = -1;
+      for (int c = 0; c < 11; ++c)
+        if (std::strcmp(group, host_group_name(c)) == 0) gid = c;
+      if (k < 0 || gid < 0 || (g != 2 && g != 4 && g != 8) || !(spc >= 0.5 && spc <= 16)) continue;
+      table.entries[{k, gid, bucket}] = NearTiles{g, spc};
+    }
+    std::fclose(f);
+  });
+  return table;
+}
+}  // namespace
+
+NearTiles lookup_tiles(int kind, int gid, int n) {
+  const TileTable& t = tile_table();
+  const int bucket = n > 0 ? 31 - __builtin_clz((unsigned)n) : 0;
+  const NearTiles* best = nullptr;
+  int distance = 1 << 30;
+  for (auto it = t.entries.lower_bound({kind, gid, -1000}); it != t.entries.end(); ++it) {
+    const auto& [k, g, b] = it->first;
+    if (k != kind || g != gid) break;
+    const int d = std::abs(b - bucket);
+    if (d < distance) {  // the nearest bucket; the lower one on a tie
+      distance = d;
+      best = &it->second;
+    }
+  }
+  return best ? *best : NearTiles{};
+}
+
+void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_r, int sms,
+                      int kind) {
   ready_ = false;
   ++generation_;
   n_ = n;
   prec_ = prec;
+  tiles_ = forced_ ? *forced_ : lookup_tiles(kind, gid_, n);
   radius_ = std::min(1.5, delta_ * mean_r);
   s_margin_ = std::sin(radius_ + 1e-4);
   chord_ = 2.0 * std::sin(radius_ / 2.0);
@@ -132,9 +211,11 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   uint64_t cap = (uint64_t)total + total / 4 + 1024;
   cap = std::min<uint64_t>(cap, 2 * order * (uint64_t)n);
   cap = std::max<uint64_t>(cap, (uint64_t)total);
+  if (next_capacity_ > 0) cap = next_capacity_;  // development override, once
+  next_capacity_ = 0;
   if (cap > (1ull << 31) - 1) throw Failure("NearShellTooLarge");
   capacity_ = (int)cap;
-  sdim_max_ = (int)std::lround(std::cbrt((double)capacity_ / kSitesPerCell));
+  sdim_max_ = (int)std::lround(std::cbrt((double)capacity_ / tiles_.sites_per_cell));
   sdim_max_ = std::max(1, std::min(sdim_max_, kMaxCellDim));
   const size_t cells = (size_t)sdim_max_ * sdim_max_ * sdim_max_ + 1;
   const size_t qsize = prec == kFP64 ? sizeof(double4) : sizeof(float4);
@@ -159,6 +240,9 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   src_perm_.ensure((size_t)n * 4);
   grid_.ensure(sizeof(NearGrid));
   cells_.ensure(sizeof(int));
+  exact_list_.ensure((size_t)n * 4);
+  exact_count_.ensure(2 * sizeof(uint32_t));
+  ZO_CUDA(cudaMemsetAsync(exact_count_.as<void>(), 0, 2 * sizeof(uint32_t), s));
   NearGrid g{};
   for (int a = 0; a < 3; ++a) {
     g.box_bits[a] = 0xffffffffu;
@@ -168,22 +252,15 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   // Warp tasks (32 sources x one slice of their cell rows): several waves of resident warps.
   const int warps = (n + 31) / 32;
   slices_ = std::max(1, std::min(64, (sms * 48 + warps - 1) / warps));
-  const int warps32 = (n + kNearGroup - 1) / kNearGroup;
+  const int warps32 = (n + tiles_.group_size - 1) / tiles_.group_size;
   slices32_ = std::max(1, std::min(slices_, (sms * 48 + warps32 - 1) / warps32));
   partial_.ensure((size_t)slices_ * n);
   ZO_CUDA(cudaStreamSynchronize(s));
   ready_ = true;
 }
 
-void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_r, bool track,
-                     Rows out, int sms, bool nearest_only) {
-  if (!ready_ || n != n_ || prec != prec_) setup(s, prec, q32, q64, n, mean_r, sms);
-  if (dense_) {
-    ZO_CUDA(launch_dense_near(prec, track, radius_ <= 0.4, q32, q64, n, gid_, plan_, chord_ * chord_, chord_,
-                              taper_ * radius_, 1.0 / std::max(1e-9, (1.0 - taper_) * radius_),
-                              plan_.chunks > 1 ? partial_.rows() : Rows{}, out, s));
-    return;
-  }
+NearLaunch NearField::make_launch(int prec, const float4* q32, const double4* q64, int n, bool track, Rows out,
+                                  bool nearest_only) {
   NearLaunch L{};
   L.prec = prec;
   L.gid = gid_;
@@ -192,9 +269,15 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
   L.sdim_max = sdim_max_;
   L.slices = slices_;
   L.slices32 = slices32_;
+  L.group_size = tiles_.group_size;
+  L.sites_per_cell = tiles_.sites_per_cell;
   L.track = track;
   L.short_atan = radius_ <= 0.4;
   L.nearest_only = nearest_only && track;
+  const double walk = 2.0 * std::sin(0.5 * kSpacingWalk * radius_);
+  L.walk_cut2 = walk * walk;
+  L.exact_list = exact_list_.as<uint32_t>();
+  L.exact_count = exact_count_.as<uint32_t>();
   L.s_margin = s_margin_;
   L.cut2 = chord_ * chord_;
   L.chord = chord_;
@@ -233,7 +316,67 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
   L.cells = cells_.as<int>();
   L.partial = partial_.rows();
   L.out = out;
-  ZO_CUDA(launch_near(L, s));
+  return L;
+}
+
+void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_r, bool track,
+                     Rows out, int sms, bool nearest_only) {
+  if (!ready_ || n != n_ || prec != prec_)
+    setup(s, prec, q32, q64, n, mean_r, sms, nearest_only ? kTilesSpacing : kTilesRelax);
+  if (dense_) {
+    ZO_CUDA(launch_dense_near(prec, track, radius_ <= 0.4, q32, q64, n, gid_, plan_, chord_ * chord_, chord_,
+                              taper_ * radius_, 1.0 / std::max(1e-9, (1.0 - taper_) * radius_),
+                              plan_.chunks > 1 ? partial_.rows() : Rows{}, out, s));
+    return;
+  }
+  ZO_CUDA(launch_near(make_launch(prec, q32, q64, n, track, out, nearest_only), s));
+}
+
+bool NearField::pass_structure(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n,
+                               double mean_r, Rows out, int sms, NearTask* task) {
+  if (prec != kFP32 || !ready_ || n != n_ || prec != prec_ || dense_) {
+    pass(s, prec, q32, q64, n, mean_r, false, out, sms);  // the whole pass, on this stream
+    return false;
+  }
+  const NearLaunch L = make_launch(prec, q32, q64, n, false, out, false);
+  int launches = 0;
+  ZO_CUDA(launch_near_structure(L, s, &launches));
+  probe_count(launches);
+  *task = near_task(L);
+  return true;
+}
+
+void NearField::pass_reduce(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, Rows out) {
+  ZO_CUDA(launch_near_reduce(make_launch(prec, q32, q64, n, false, out, false), s));
+}
+
+void NearField::exact_report(cudaStream_t s, uint32_t* listed, uint32_t* ties) {
+  uint32_t c[2] = {0, 0};
+  if (ready_ && !dense_) {
+    ZO_CUDA(cudaMemcpyAsync(c, exact_count_.as<uint32_t>(), sizeof c, cudaMemcpyDeviceToHost, s));
+    ZO_CUDA(cudaStreamSynchronize(s));
+  }
+  *listed = c[0];
+  *ties = c[1];
+}
+
+size_t NearField::bytes() const {
+  const DeviceBuffer* all[] = {&counts_,    &offsets_,  &scan_tmp_, &shell_mask_, &rim_list_,  &rim_q_,
+                               &rim_count_, &site_q_,   &site_code_, &site_img_,  &site_cell_, &site_rank_,
+                               &site_pos_,  &cell_count_, &cell_off_, &perm_,     &sq_,        &scode_,
+                               &simg_,      &sx_,       &src_key_,  &src_rank_,  &mcount_,    &moff_,
+                               &src_perm_,  &grid_,     &cells_,    &exact_list_, &exact_count_};
+  size_t total = partial_.bytes();
+  for (const DeviceBuffer* b : all) total += b->bytes();
+  return total;
+}
+
+int NearField::site_count(cudaStream_t s) {
+  if (!ready_ || dense_) return 0;
+  int sites = 0;
+  ZO_CUDA(cudaMemcpyAsync(&sites, &grid_.as<NearGrid>()->sites, sizeof sites, cudaMemcpyDeviceToHost, s));
+  ZO_CUDA(cudaStreamSynchronize(s));
+  return sites;
 }
 
 bool NearField::overflowed(cudaStream_t s) {
@@ -256,6 +399,15 @@ void RelaxState::reset() {
   // its allocations where they are large enough (a new sample of similar size frees and
   // allocates nothing).
   if (near_) near_->invalidate();
+}
+
+size_t RelaxState::bytes() const {
+  const DeviceBuffer* all[] = {&prev_f_,           &prev_d_,        &state_,       &stats_partials_,
+                               &hist_,             &summary_,       &summary_partials_, &near_partials_,
+                               &near_rows_,        &degrees_,       &neighbours_};
+  size_t total = rows_.bytes() + partial_.bytes() + (near_ ? near_->bytes() : 0);
+  for (const DeviceBuffer* b : all) total += b->bytes();
+  return total;
 }
 
 void RelaxState::set_near(int gid, std::optional<double> delta) {
@@ -319,6 +471,28 @@ void RelaxState::step(cudaStream_t s, int prec, float4* q32, double4* q64, int n
                       double budget_scale, int sms) {
   prepare(s, n, prec);
   if (!current) record_forces(s, prec, q32, q64, n, gid, false, budget_scale, sms);
+  step_update(s, prec, q32, q64, n, gid, fixed, sms);
+}
+
+bool RelaxState::step_structure(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, int gid,
+                                double budget_scale, int sms, NearTask* task) {
+  prepare(s, n, prec);
+  if (current) return false;  // the forces of these positions are recorded already
+  if (!near_) {
+    record_forces(s, prec, q32, q64, n, gid, false, budget_scale, sms);
+    return false;
+  }
+  return near_->pass_structure(s, prec, q32, q64, n, mean_radius((double)n * host_group_order(gid)), rows_.rows(),
+                               sms, task);
+}
+
+void RelaxState::step_finish(cudaStream_t s, int prec, float4* q32, double4* q64, int n, int gid, int fixed, int sms,
+                             bool had_task) {
+  if (had_task) near_->pass_reduce(s, prec, q32, q64, n, rows_.rows());
+  step_update(s, prec, q32, q64, n, gid, fixed, sms);
+}
+
+void RelaxState::step_update(cudaStream_t s, int prec, float4* q32, double4* q64, int n, int gid, int fixed, int sms) {
   current = false;
   order_ = host_group_order(gid);
   const double radius = mean_radius((double)n * order_);
@@ -503,6 +677,34 @@ void Engine::relax_async(uint32_t steps) {
   }
 }
 
+void Engine::batch_begin() {
+  if (n_ < 2) throw Failure("TooFewOrientations");
+  ZO_CUDA(cudaSetDevice(device_));
+  if (!relaxing_) {
+    cancelled_.store(false);
+    sync_neighbourhood();
+    relaxing_ = true;
+  }
+}
+
+bool Engine::batch_structure(NearTask* task) {
+  if (fix_identity_ && !fixed_index_) throw Failure("IdentityMissingEnableAddIdentity");
+  return relax_state_.step_structure(stream_, prec_, q32(), q64(), (int)n_, group_, budget_scale_, sms_, task);
+}
+
+void Engine::batch_finish(bool had_task) {
+  relax_state_.step_finish(stream_, prec_, q32(), q64(), (int)n_, group_, fixed_arg(), sms_, had_task);
+}
+
+void Engine::batch_stepped() {
+  ++iteration_;
+  recorded_ = true;
+}
+
+bool Engine::batch_ready() const {
+  return use_graphs_ && prec_ == kFP32 && !relax_state_.current && relax_state_.sized((int)n_, prec_);
+}
+
 void Engine::relax_finish() {
   finish_async();
   finish_collect();
@@ -657,7 +859,7 @@ void Engine::set(int gid, const float* values, size_t count) {
   const uint32_t n = (uint32_t)count;
   q32_.ensure((size_t)n * 16);
   ZO_CUDA(cudaMemcpyAsync(q32_.as<float4>(), values, (size_t)n * 16, cudaMemcpyHostToDevice, stream_));
-  if (prec_ == kFP64) q64_.ensure((size_t)n * 32);
+  q64_.ensure((size_t)n * 32);
   ZO_CUDA(launch_fold(q32_.as<float4>(), q64(), (int)n, gid, prec_, true, stream_));
   group_ = gid;
   n_ = n;
@@ -673,7 +875,7 @@ void Engine::generate_random(int gid, uint32_t count, uint32_t seed) {
   if (count < 1 || count > kMaxCount) throw Failure("InvalidCount");
   ZO_CUDA(cudaSetDevice(device_));
   q32_.ensure((size_t)count * 16);
-  if (prec_ == kFP64) q64_.ensure((size_t)count * 32);
+  q64_.ensure((size_t)count * 32);
   ZO_CUDA(launch_haar(q32_.as<float4>(), (int)count, seed, stream_));
   group_ = gid;
   ZO_CUDA(launch_fold(q32_.as<float4>(), q64(), (int)count, gid, prec_, true, stream_));
@@ -699,7 +901,7 @@ void Engine::generate_grid(int gid, uint32_t freq, uint32_t target, uint32_t see
   ZO_CUDA(cudaSetDevice(device_));
   q32_.ensure((size_t)n * 16);
   ZO_CUDA(cudaMemcpyAsync(q32_.as<float4>(), rows.data(), (size_t)n * 16, cudaMemcpyHostToDevice, stream_));
-  if (prec_ == kFP64) q64_.ensure((size_t)n * 32);
+  q64_.ensure((size_t)n * 32);
   ZO_CUDA(launch_fold(q32_.as<float4>(), q64(), (int)n, gid, prec_, true, stream_));
   group_ = gid;
   n_ = n;
@@ -735,6 +937,23 @@ void Engine::set_neighbourhood(double delta) {
 void Engine::sync_neighbourhood() {
   relax_state_.set_near(group_, neighbourhood_ > 0 ? std::optional<double>(neighbourhood_) : std::nullopt);
   measure_neighbourhood_ = neighbourhood_;
+  apply_overrides(relax_state_);
+}
+
+void Engine::force_tiles(std::optional<NearTiles> tiles) {
+  if (tiles && tiles->group_size != 2 && tiles->group_size != 4 && tiles->group_size != 8) throw Failure("InvalidTiles");
+  if (tiles && !(tiles->sites_per_cell >= 0.5 && tiles->sites_per_cell <= 16)) throw Failure("InvalidTiles");
+  forced_tiles_ = tiles;
+  for (RelaxState* st : {&relax_state_, &spacing_state_})
+    if (NearField* nf = st->near_field()) nf->force_tiles(tiles);
+}
+
+void Engine::apply_overrides(RelaxState& state) {
+  NearField* nf = state.near_field();
+  if (nf) nf->force_tiles(forced_tiles_);
+  if (!shell_override_ || !nf) return;
+  nf->override_capacity(shell_override_);
+  shell_override_ = 0;
 }
 
 Measures Engine::relax_state_measure() {
@@ -843,6 +1062,7 @@ void Engine::spacing() {
   ZO_CUDA(cudaSetDevice(device_));
   spacing_state_.set_near(group_, n_ > kSpacingAllPairs ? std::optional<double>(kSpacingDelta) : std::nullopt);
   spacing_state_.nearest_only = true;
+  apply_overrides(spacing_state_);
   spacing_state_.prepare(stream_, (int)n_, prec_);
   point_separation_.resize(n_);
   point_neighbours_.resize(n_);
@@ -933,10 +1153,8 @@ void Engine::identity(bool add, bool fixed) {
     std::memcpy(&host_[(size_t)i * 4], one, 16);
     identity_cache_.reset();
     ZO_CUDA(cudaMemcpyAsync(q32() + i, one, 16, cudaMemcpyHostToDevice, stream_));
-    if (prec_ == kFP64) {
-      const double one64[4] = {1, 0, 0, 0};
-      ZO_CUDA(cudaMemcpyAsync(q64() + i, one64, 32, cudaMemcpyHostToDevice, stream_));
-    }
+    const double one64[4] = {1, 0, 0, 0};
+    ZO_CUDA(cudaMemcpyAsync(q64() + i, one64, 32, cudaMemcpyHostToDevice, stream_));
     ZO_CUDA(cudaStreamSynchronize(stream_));
     relax_state_.current = false;
   }
@@ -1063,6 +1281,73 @@ void Engine::bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* 
   relax_state_.current = false;
   measures_.reset();
   fetch();
+}
+
+size_t Engine::device_bytes() const {
+  return q32_.bytes() + q64_.bytes() + relax_state_.bytes() + spacing_state_.bytes() + full_rows_.bytes() +
+         full_partial_.bytes() + full_extra_.bytes() + full_pextra_.bytes() + full_degen_.bytes() +
+         full_pdegen_.bytes();
+}
+
+void Engine::spacing_exact(uint32_t* listed, uint32_t* ties) {
+  *listed = 0;
+  *ties = 0;
+  NearField* nf = spacing_state_.near_field();
+  if (!nf || prec_ != kFP32) return;
+  ZO_CUDA(cudaSetDevice(device_));
+  nf->exact_report(stream_, listed, ties);
+}
+
+void Engine::bench_spacing(uint32_t passes, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len) {
+  if (passes == 0 || out_len < 6) throw Failure("InvalidBench");
+  for (uint32_t w = 0; w < std::max<uint32_t>(warmup, 1); ++w) spacing();  // sizes the workspace
+  ZO_CUDA(cudaSetDevice(device_));
+  DeviceBuffer flush;
+  const size_t fbytes = flush_bytes > 0 ? (size_t)flush_bytes : 0;
+  if (fbytes) flush.ensure(fbytes);
+  std::vector<cudaEvent_t> ev(4 * (size_t)passes);
+  for (auto& e : ev) ZO_CUDA(cudaEventCreate(&e));
+  LaunchProbe probe;
+  probe.events = ev.data() + 2 * (size_t)passes;
+  probe.capacity = 2 * (int)passes;
+  t_probe = &probe;
+  RowSummary summary{};
+  try {
+    for (uint32_t k = 0; k < passes; ++k) {
+      if (fbytes) ZO_CUDA(cudaMemsetAsync(flush.as<void>(), (int)(k & 0xff), fbytes, stream_));
+      ZO_CUDA(cudaEventRecord(ev[2 * k], stream_));
+      spacing_state_.record_forces(stream_, prec_, q32(), q64(), (int)n_, group_, true, budget_scale_, sms_);
+      spacing_state_.summarize_async(stream_, (int)n_, (int)order(), &summary, point_separation_.data(),
+                                     point_neighbours_.data(), prec_, q32(), group_);
+      ZO_CUDA(cudaEventRecord(ev[2 * k + 1], stream_));
+    }
+  } catch (...) {
+    t_probe = nullptr;
+    throw;
+  }
+  t_probe = nullptr;
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  double total = 0, kernel = 0;
+  for (uint32_t k = 0; k < passes; ++k) {
+    float ms = 0;
+    ZO_CUDA(cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]));
+    total += ms;
+  }
+  for (int k = 0; k + 1 < probe.used; k += 2) {
+    float ms = 0;
+    ZO_CUDA(cudaEventElapsedTime(&ms, probe.events[k], probe.events[k + 1]));
+    kernel += ms;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  NearField* nf = spacing_state_.near_field();
+  uint32_t listed = 0, ties = 0;
+  if (nf) nf->exact_report(stream_, &listed, &ties);
+  out[0] = total / passes;
+  out[1] = probe.used ? kernel / (probe.used / 2) : 0;
+  out[2] = probe.used / 2;
+  out[3] = nf ? nf->site_count(stream_) : 0;
+  out[4] = listed;
+  out[5] = (double)probe.launches / passes;
 }
 
 const float* Engine::point_values(uint32_t kind) const {

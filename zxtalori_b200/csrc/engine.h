@@ -112,8 +112,24 @@ struct StepResult {
 struct RowBuffers {
   DeviceBuffer force, energy, nearest, nearest_at;
   Rows ensure(size_t n);
+  size_t bytes() const { return force.bytes() + energy.bytes() + nearest.bytes() + nearest_at.bytes(); }
   Rows rows() const { return Rows{force.as<double4>(), energy.as<double>(), nearest.as<double>(), nearest_at.as<int>()}; }
 };
+
+// Tile shape of the FP32 near-field gather: sources per warp (2, 4 or 8) and target shell
+// sites per chart cell.
+struct NearTiles {
+  int group_size = kNearGroup;
+  double sites_per_cell = kSitesPerCell;
+};
+// Which near-field pass a tile choice is for.
+enum TileKind : int { kTilesRelax = 0, kTilesSpacing = 1 };
+// The tile table's choice for a group and sample size: the entry of (kind, group,
+// floor(log2 n)), else the group's entry of the nearest size bucket, else the defaults. The
+// table is read once per process from $ZXTALORI_TILES, or near_tiles.txt in the package
+// directory beside the library's _lib folder; lines "kind group bucket sources_per_warp
+// sites_per_cell" (kind relax|spacing, group by name), '#' comments.
+NearTiles lookup_tiles(int kind, int gid, int n);
 
 // Near-field workspace (src/near.zig:31-196): sized by one shell pass, then reused.
 class NearField {
@@ -125,6 +141,13 @@ class NearField {
   // Records a pass writing rows of q into `out`.
   void pass(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_radius, bool track,
             Rows out, int sms, bool nearest_only = false);
+  // The pass in parts, for a batch whose samples share one gather launch. pass_structure
+  // records the shell, chart grid, site sort and source order and returns the FP32 gather
+  // as a task (true); a pass with no such gather (FP64, dense, or a workspace still to be
+  // sized) is recorded whole instead (false). pass_reduce then sums the task's slices.
+  bool pass_structure(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_radius,
+                      Rows out, int sms, NearTask* task);
+  void pass_reduce(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, Rows out);
   // Whether the last pass produced more sites than the workspace holds (after a sync);
   // the next pass sizes it again.
   bool overflowed(cudaStream_t s);
@@ -132,6 +155,13 @@ class NearField {
   const uint32_t* sorted_images() const { return simg_.as<uint32_t>(); }
   int capacity() const { return capacity_; }
   int slices() const { return slices_; }
+  // Spacing pass: of the last nearest-only pass, how many sources the first walk left to the
+  // exact FP64 search and how many of those had an exact tie (waits for the stream).
+  void exact_report(cudaStream_t s, uint32_t* listed, uint32_t* ties);
+  // Shell sites of the last pass (waits for the stream).
+  int site_count(cudaStream_t s);
+  // Device bytes the workspace holds.
+  size_t bytes() const;
   // Changes whenever the workspace is sized again (buffers move): captured graphs go stale.
   uint64_t generation() const { return generation_; }
   bool ready() const { return ready_; }
@@ -144,6 +174,22 @@ class NearField {
   // The next pass sizes the workspace again (after an observed overflow, or for a new
   // sample); allocations large enough are reused.
   void invalidate() { ready_ = false; }
+  // Development: the next sizing of the workspace holds only `sites` shell sites (once), so
+  // a pass overflows and the resize-and-redo path runs without a GPU fault.
+  void override_capacity(uint32_t sites) {
+    next_capacity_ = sites;
+    ready_ = false;
+  }
+  // The tile shape to use instead of the table's (none: the table), from the next sizing on.
+  void force_tiles(std::optional<NearTiles> tiles) {
+    const bool same = tiles.has_value() == forced_.has_value() &&
+                      (!tiles || (tiles->group_size == forced_->group_size &&
+                                  tiles->sites_per_cell == forced_->sites_per_cell));
+    if (same) return;
+    forced_ = tiles;
+    ready_ = false;
+  }
+  const NearTiles& tiles() const { return tiles_; }
   void reconfigure(int gid, double delta) {
     gid_ = gid;
     delta_ = delta;
@@ -154,17 +200,24 @@ class NearField {
   uint64_t generation_ = 0;
   bool dense_ = false;
   PairsPlan plan_;
-  void setup(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_radius, int sms);
+  void setup(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, double mean_radius, int sms,
+             int kind);
+  NearLaunch make_launch(int prec, const float4* q32, const double4* q64, int n, bool track, Rows out,
+                         bool nearest_only);
   int gid_;
   double delta_;
   double taper_ = 0.5;
+  NearTiles tiles_;
+  std::optional<NearTiles> forced_;
   bool ready_ = false;
   int n_ = 0, prec_ = -1, capacity_ = 0, sdim_max_ = 1, slices_ = 1, slices32_ = 1;
+  uint32_t next_capacity_ = 0;
   double radius_ = 0, s_margin_ = 0, chord_ = 0;
   DeviceBuffer counts_, offsets_, scan_tmp_, shell_mask_, rim_list_, rim_q_, rim_count_;
   DeviceBuffer site_q_, site_code_, site_img_, site_cell_, site_rank_, site_pos_;
   DeviceBuffer cell_count_, cell_off_, perm_, sq_, scode_, simg_, sx_, src_key_, src_rank_, mcount_, moff_, src_perm_;
   DeviceBuffer grid_, cells_;
+  DeviceBuffer exact_list_, exact_count_;
   RowBuffers partial_;
 };
 
@@ -190,6 +243,13 @@ class RelaxState {
   void record_forces(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, int gid, bool track,
                      double budget_scale, int sms);
   void step(cudaStream_t s, int prec, float4* q32, double4* q64, int n, int gid, int fixed, double budget_scale, int sms);
+  // The same step in two parts around a shared gather launch: step_structure records what
+  // comes before the near-field gather and returns it as a task (true), or records the whole
+  // force pass (false); step_finish sums the task's slices (had_task) and makes the BB update.
+  bool step_structure(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n, int gid,
+                      double budget_scale, int sms, NearTask* task);
+  void step_finish(cudaStream_t s, int prec, float4* q32, double4* q64, int n, int gid, int fixed, int sms,
+                   bool had_task);
   StepResult finish(cudaStream_t s);
   // Quick measures of `rows()` (after a force pass), nearest degrees and neighbours to host.
   Measures summarize(cudaStream_t s, int n, int order, float* degrees, int* neighbours, int prec, const float4* q32,
@@ -203,6 +263,8 @@ class RelaxState {
   StepResult result_of(const RelaxDev& st) const { return step_result(st); }
   bool near_overflowed(cudaStream_t s) { return near_ && near_->overflowed(s); }
   NearField* near_field() { return near_.get(); }
+  // Device bytes the state (and its near-field workspace) holds.
+  size_t bytes() const;
   // Identifies the buffers and settings a captured step reads; any change makes it stale.
   uint64_t generation() const { return generation_ * 1000003ull + (near_ ? near_->generation() * 7 + 1 : 0); }
   // Whether a step would run without sizing anything (so it can be captured in a graph).
@@ -212,6 +274,7 @@ class RelaxState {
   RowSummary last_summary_{};
   uint64_t generation_ = 0;
   StepResult step_result(const RelaxDev& st) const;
+  void step_update(cudaStream_t s, int prec, float4* q32, double4* q64, int n, int gid, int fixed, int sms);
   int n_ = 0, prec_ = -1, order_ = 0;
   RowBuffers rows_, partial_;
   DeviceBuffer prev_f_, prev_d_, state_, stats_partials_, hist_, summary_, summary_partials_, near_partials_,
@@ -235,6 +298,11 @@ class Engine {
   const char* stats();
   const float* point_values(uint32_t kind) const;
   const int* point_neighbours() const;
+  // Device memory this engine holds now (every buffer it sized, from the pool).
+  size_t device_bytes() const;
+  // Of the last spacing pass: sources settled by the exact FP64 search instead of the FP32
+  // gather, and sources whose nearest distance two different sources share exactly.
+  void spacing_exact(uint32_t* listed, uint32_t* ties);
   void cancel() { cancelled_.store(true); }
   // Extensions.
   void set_precision(int prec);
@@ -254,10 +322,30 @@ class Engine {
   void finish_collect();
   // Whether the engine's stream has no work pending.
   bool idle();
+  // A batch's part of this engine (zo_batch_relax): batch_begin as relax_async starts a run;
+  // each step is batch_structure (on the engine's stream; true when it leaves its near-field
+  // gather to the batch's shared launch, as `task`), then batch_finish after that launch.
+  // batch_ready: FP32 with graphs on and everything sized, so a step can be captured.
+  void batch_begin();
+  bool batch_structure(NearTask* task);
+  void batch_finish(bool had_task);
+  // Counts one step that the batch recorded or replayed (host bookkeeping, once per step).
+  void batch_stepped();
+  bool batch_ready() const;
+  uint64_t batch_key() const { return graph_key(); }
+  int device() const { return device_; }
+  int sms() const { return sms_; }
   void set_graphs(bool enabled) {
     use_graphs_ = enabled;
     drop_graph();
   }
+  bool graphs_enabled() const { return use_graphs_; }
+  // Tuning: the tile shape of this engine's near-field gathers (relaxation and spacing)
+  // instead of the table's; nullopt returns to the table.
+  void force_tiles(std::optional<NearTiles> tiles);
+  // Development: the next near-field pass (of the relaxation and of the spacing pass) sizes
+  // its workspace for only `sites` shell sites, once; 0 cancels.
+  void debug_shell_capacity(uint32_t sites) { shell_override_ = sites; }
   // Development: one pass's raw rows to host. what 0: force pass of the relaxation
   // (8 doubles per source), 1: full measure rows (12 doubles per source).
   void debug_rows(uint32_t what, double* out);
@@ -266,6 +354,12 @@ class Engine {
   // events. out[0] total step ms, out[1] dominant-kernel ms, out[2] its launches, out[3]
   // kernel launches per step, out[4 ..] each step's ms (as room allows).
   void bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len);
+  // Measurement of the spacing pass: `passes` passes after `warmup`, each bracketed by CUDA
+  // events (an L2 flush before it, outside the events). out[0] ms per pass (gather, exact
+  // search, refinement, degrees and neighbours into host memory), out[1] ms per launch of
+  // the gather kernel, out[2] its launches, out[3] shell sites, out[4] points settled by
+  // the exact search, out[5] kernel launches per pass.
+  void bench_spacing(uint32_t passes, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len);
   // Measured FP32 FMA throughput of this engine's device, TFLOP/s, with scalar FMAs or
   // with packed (f32x2) FMAs.
   double fp32_peak(bool packed = false) {
@@ -310,6 +404,10 @@ class Engine {
   void adopt(uint32_t n);
   void reset_run();
   void sync_neighbourhood();
+  // The development shell capacity (once) and the forced tile shape, onto the state's near field.
+  void apply_overrides(RelaxState& state);
+  uint32_t shell_override_ = 0;
+  std::optional<NearTiles> forced_tiles_;
   void fetch();
   Measures full_measure();
   Measures relax_state_measure();
@@ -318,8 +416,12 @@ class Engine {
   // identity_index() of the current host copy (a scan of every orientation), kept until
   // the host copy changes.
   mutable std::optional<std::optional<uint32_t>> identity_cache_;
+  // Positions: the FP64 master copy, moved by every BB step in both modes, and its float32
+  // rounding, which FP32 mode's pair kernels read and the host copy mirrors. Keeping the
+  // master in FP64 stops the float32 rounding of each step from accumulating along the
+  // trajectory (it dominated the relaxed sample's drift from the FP64 method).
   float4* q32() { return q32_.as<float4>(); }
-  double4* q64() { return prec_ == kFP64 ? q64_.as<double4>() : nullptr; }
+  double4* q64() { return q64_.as<double4>(); }
 
   int device_ = 0, sms_ = 148;
   std::string adapter_;  // the device's name, for stats

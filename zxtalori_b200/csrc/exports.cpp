@@ -150,12 +150,41 @@ int zo_precision(void* h, uint32_t mode) {
 uint32_t zo_get_precision(void* h) { return (uint32_t) static_cast<Engine*>(h)->precision(); }
 const int32_t* zo_point_neighbours(void* h) { return static_cast<Engine*>(h)->point_neighbours(); }
 
+int zo_near_tiles(void* h, uint32_t sources_per_warp, float sites_per_cell) {
+  return guarded(h, "Tiles", [&](Engine& e) {
+    if (sources_per_warp == 0) e.force_tiles(std::nullopt);
+    else e.force_tiles(zo::NearTiles{(int)sources_per_warp, (double)sites_per_cell});
+  });
+}
+
+int zo_tiles_lookup(uint32_t kind, uint32_t group, uint32_t n, double* out) {
+  if (group >= 11 || kind > 1 || !out) return -1;
+  const zo::NearTiles t = zo::lookup_tiles((int)kind, (int)group, (int)n);
+  out[0] = t.group_size;
+  out[1] = t.sites_per_cell;
+  return 0;
+}
+
+uint64_t zo_device_bytes(void* h) { return h ? (uint64_t) static_cast<Engine*>(h)->device_bytes() : 0; }
+
+int zo_spacing_exact(void* h, uint32_t* out) {
+  return guarded(h, "Spacing", [&](Engine& e) { e.spacing_exact(out, out + 1); });
+}
+
+int zo_debug_shell_capacity(void* h, uint32_t sites) {
+  return guarded(h, "Rows", [&](Engine& e) { e.debug_shell_capacity(sites); });
+}
+
 int zo_debug_rows(void* h, uint32_t what, double* out) {
   return guarded(h, "Rows", [&](Engine& e) { e.debug_rows(what, out); });
 }
 
 int zo_bench(void* h, uint32_t steps, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len) {
   return guarded(h, "Bench", [&](Engine& e) { e.bench(steps, warmup, flush_bytes, out, out_len); });
+}
+
+int zo_bench_spacing(void* h, uint32_t passes, uint32_t warmup, double flush_bytes, double* out, uint32_t out_len) {
+  return guarded(h, "Bench", [&](Engine& e) { e.bench_spacing(passes, warmup, flush_bytes, out, out_len); });
 }
 
 int zo_relax_async(void* h, uint32_t steps) {
@@ -172,25 +201,6 @@ int zo_idle(void* h) {
 
 int zo_graphs(void* h, uint32_t enabled) {
   return guarded(h, "Graphs", [&](Engine& e) { e.set_graphs(enabled != 0); });
-}
-
-int zo_batch_relax(void* const* handles, uint32_t count, uint32_t steps, int32_t* status) {
-  // Every engine has its own stream, so the samples' kernels run side by side. Steps are
-  // enqueued round-robin (one step of every sample, then the next), so samples that share
-  // a hardware queue interleave instead of waiting for each other; then every closing pass
-  // is enqueued before any is waited for.
-  for (uint32_t k = 0; k < count; ++k) status[k] = 0;
-  for (uint32_t s = 0; s < steps; ++s)
-    for (uint32_t k = 0; k < count; ++k)
-      if (status[k] == 0) status[k] = guarded(handles[k], "Relaxation failed", [&](Engine& e) { e.relax_async(1); });
-  for (uint32_t k = 0; k < count; ++k)
-    if (status[k] == 0) status[k] = guarded(handles[k], "Relaxation failed", [](Engine& e) { e.finish_async(); });
-  int failures = 0;
-  for (uint32_t k = 0; k < count; ++k) {
-    if (status[k] == 0) status[k] = guarded(handles[k], "Relaxation failed", [](Engine& e) { e.finish_collect(); });
-    failures += status[k] != 0;
-  }
-  return failures;
 }
 
 int64_t zo_hopf_points(uint32_t group, uint32_t freq, float* out, uint64_t capacity) {

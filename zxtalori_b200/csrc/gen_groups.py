@@ -51,4 +51,6 @@ def main(path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/tests/fixtures/pair-operators.npz")
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_groups.py <reference checkout>/tests/fixtures/pair-operators.npz")
+    main(sys.argv[1])

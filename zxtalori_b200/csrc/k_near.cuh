@@ -10,7 +10,7 @@
 //      sites into row-major cells with each cell ordered by site index;
 //   3. sources counting-sorted along a Hilbert curve of a 64^3 grid (then by index), so
 //      consecutive sources are close together;
-//   4. one warp per kNearGroup sources (FP32; 32 in FP64) and slice: the warp's chart box,
+//   4. one warp per G sources (FP32, G = 2, 4 or 8; 32 in FP64) and slice: the warp's chart box,
 //      the cell rows within the chart reach of the cutoff chord, each row's x-run trimmed;
 //      runs stream through shared memory 32 sites at a time and the lanes test their
 //      sources against each site;
@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(256) k_shell_write(const float4* __restrict__ 
 // concatenates runs, so short rows cost nothing extra).
 // The box is reset for the next pass.
 __global__ void k_grid_setup(NearGrid* g, const uint32_t* __restrict__ total, int capacity, int sdim_max,
-                             int* __restrict__ cells) {
+                             float sites_per_cell, int* __restrict__ cells) {
   const uint32_t s = *total;
   g->sites = (int)min((uint32_t)capacity, s);
   if (s > (uint32_t)capacity) g->overflow = 1u;
@@ -311,7 +311,7 @@ __global__ void k_grid_setup(NearGrid* g, const uint32_t* __restrict__ total, in
   }
   for (int a = 0; a < 3; ++a) g->lower[a] = lo[a] - 0.05f * width;
   width *= 1.1f;
-  int sdim = (int)rint(cbrt((double)g->sites / kSitesPerCell));
+  int sdim = (int)rint(cbrt((double)g->sites / sites_per_cell));
   sdim = max(1, min(sdim, sdim_max));
   g->width = width;
   g->sdim = sdim;
@@ -443,17 +443,21 @@ __global__ void k_source_count(const float4* __restrict__ q32, const double4* __
 }
 
 // ------------------------------------------------------------------ 4. the gather
-struct NearCut {
-  double cut2, chord, cut_z, cut_w;
-  // Squared chord at angle 1.25 r, where the window is exactly zero: the packed gather
-  // evaluates an out-of-cutoff site with its chord clamped to this (finite terms, zero
-  // contribution) when the other site of its pair is within the cutoff.
-  double cut_hi;
-};
 inline NearCut near_cut(double cut2, double chord, double cut_z, double cut_w) {
   const double r = cut_z + 1.0 / cut_w;
   const double s = 2.0 * std::sin(0.5 * std::min(1.25 * r, 1.5));
-  return NearCut{cut2, chord, cut_z, cut_w, s * s};
+  return NearCut{cut2, chord, cut_z, cut_w, s * s, cut2};
+}
+
+// Bound on |FP32 chord^2 - FP64 chord^2| of a source x and a site y of the FP32 gather, at
+// chord^2 d, against the oracle's definition (unit x and y formed in FP64). The gather
+// reads x as stored (float32, |x| = 1 within 2^-24) and y as the float32 rounding of the
+// FP64 image (within 2^-24 per component), and forms |x - y|^2 with four FP32 roundings:
+//   |x - y|^2 - |x^ - y^|^2 <= 2 |m| 2^-24 + 2^-24 d + (2^-23)^2, m = x^ - y^, |m|^2 = d,
+//   FP32 differences and the sum of squares add at most 6 2^-24 d.
+// That is 4.2e-7 d + 1.2e-7 sqrt(d) + 1.5e-14; the bound below is 2.4 times it.
+__host__ __device__ __forceinline__ double chord_error32(double d) {
+  return 1e-6 * d + 3e-7 * sqrt(fmax(d, 0.0)) + 1e-13;
 }
 
 constexpr int kNearWarps = 4;
@@ -522,12 +526,12 @@ __device__ __forceinline__ bool row_run(const WarpBox& b, const NearGrid& g, con
   return start < end;
 }
 
-// The gather (pairs.wgsl:363-416). A warp holds kNearGroup sources (consecutive along the
-// Hilbert order), each on kNearSub = 32 / kNearGroup lanes that split its sites between
+// The gather (pairs.wgsl:363-416). A warp holds G sources (consecutive along the
+// Hilbert order), each on 32 / G lanes that split its sites between
 // them. The warp walks the cell rows that its sources' chart balls reach 32 rows at a time,
 // one lane per row finding the row's run of sorted sites; the runs are concatenated and
 // streamed through shared memory in tiles of kNearTile sites, and every lane evaluates its
-// source against kNearTile / kNearSub sites of each tile, two per instruction with packed
+// source against kNearTile G / 32 sites of each tile, two per instruction with packed
 // FP32 arithmetic. For cutoffs up to 0.4 rad the windowed pair is a function of the chord
 // alone (near_chord_pair32x2); wider ones use dp2 = 2(|x|^2+|y|^2) - dm2 (parallelogram
 // law; the site is the near twin). Sites beyond the cutoff contribute exactly zero through
@@ -536,13 +540,20 @@ __device__ __forceinline__ bool row_run(const WarpBox& b, const NearGrid& g, con
 // as sum c (x - y), turned into a force once per source. Lane sums are FP32 over 32 sites,
 // then FP64; the lanes of a source are added in lane order at the end. With one slice each
 // warp writes its sources' rows in place; the spacing pass runs a nearest-only variant.
-constexpr int kNearSub = 32 / kNearGroup;          // lanes per source
-constexpr int kNearTile = 128;                      // sites per tile
-constexpr int kNearSlots = kNearTile / (2 * kNearSub);  // site pairs per lane and tile
-constexpr int kNearMerge = kNearSlots >= 16 ? 1 : 16 / kNearSlots;  // tiles between FP64 merges
+//
+// The tile shape is a template parameter G, the sources per warp (2, 4 or 8; 4 unless the
+// tile table picks another for the sample's group and size): G sources on 32 / G lanes each.
+constexpr int kNearTile = 128;  // sites per tile
+template <int G>
+struct NearShape {
+  static_assert(G == 2 || G == 4 || G == 8, "sources per warp");
+  static constexpr int sub = 32 / G;                           // lanes per source
+  static constexpr int slots = kNearTile / (2 * sub);         // site pairs per lane and tile
+  static constexpr int merge = slots >= 16 ? 1 : 16 / slots;  // tiles between FP64 merges
+};
 
 // One tile. Slot u holds elements 2u and 2u + 1; lane (source s, sub-lane j) evaluates
-// slots j + kNearSub m, m < kNearSlots.
+// slots j + sub m, m < slots.
 struct NearTile {
   float4 wx[kNearTile / 2];  // (w, w', x, x')
   float4 yz[kNearTile / 2];  // (y, y', z, z')
@@ -556,10 +567,11 @@ struct NearTile {
 // spheres: the sites within the cutoff of source x (x . y >= k, k = 1 - cut2/2) are the
 // chart points within rho = sqrt(1 - k^2) / (x_w + k) of c = x_v / (x_w + k) (exactly, for
 // a unit x and k > -x_w). The walk covers the union of its sources' balls.
+template <int G>
 struct NearWalk {
-  float cen[kNearGroup][3];
-  float rad[kNearGroup];  // < 0: no source in this place
-  uint32_t src[kNearGroup];  // the sources' indices (codes' low bits); 0xfffffffe when absent
+  float cen[G][3];
+  float rad[G];      // < 0: no source in this place
+  uint32_t src[G];   // the sources' indices (codes' low bits); 0xfffffffe when absent
   int clo[3], chi[3];     // cells of the balls' bounding box
   float lower[3], cells_per_unit;
   int sdim;
@@ -568,7 +580,8 @@ struct NearWalk {
 
 // Row r of the walk's (y, z) cell rows: the run of sorted sites of the x cells that some
 // source's ball reaches in this row.
-__device__ __forceinline__ bool walk_row(const NearWalk& W, const uint32_t* cell_off, const float* site_x, int r,
+template <int G>
+__device__ __forceinline__ bool walk_row(const NearWalk<G>& W, const uint32_t* cell_off, const float* site_x, int r,
                                          uint32_t& start, uint32_t& end) {
   const int ny = W.chi[1] - W.clo[1] + 1;
   const int y = W.clo[1] + r % ny, z = W.clo[2] + r / ny;
@@ -576,7 +589,7 @@ __device__ __forceinline__ bool walk_row(const NearWalk& W, const uint32_t* cell
   const float cy = W.lower[1] + (float)y * width, cz = W.lower[2] + (float)z * width;
   float x0 = 3e38f, x1 = -3e38f;
 #pragma unroll
-  for (int s = 0; s < kNearGroup; ++s) {
+  for (int s = 0; s < G; ++s) {
     const float rho = W.rad[s];
     if (rho < 0.f) continue;
     const float gy = fmaxf(0.f, fmaxf(cy - W.cen[s][1], W.cen[s][1] - (cy + width)));
@@ -612,7 +625,7 @@ __device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], floa
   sw = sx = sy = sz = sc = se = splat(0.f);
 }
 
-// The slots of one tile for one lane of k_near32: slot u = sub + kNearSub m holds elements
+// The slots of one tile for one lane of k_near32: slot u = sub + (32 / G) m holds elements
 // 2u and 2u + 1. No branches in the slot: sites past the batch's end are blank and sites
 // beyond the cutoff contribute zero, so every slot runs the same arithmetic and the compiler
 // can overlap consecutive slots. OWN: the tile may hold images of the warp's sources, so
@@ -620,18 +633,19 @@ __device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], floa
 // its identity image is no neighbour); without it that test is left out. SHORT: cutoffs up
 // to 0.4 rad take the chord form (near_chord_pair32x2), wider ones the arctangent of near
 // over far. se sums energy / pi. NEAREST: only the nearest site is tracked.
-template <bool TRACK, bool SHORT, bool OWN, bool NEAREST>
+template <int G, bool TRACK, bool SHORT, bool OWN, bool NEAREST>
 __device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub, uint32_t i, float2 xw, float2 xx,
                                            float2 xy, float2 xz, float2 xn, float cut_hi, float cw, float czw,
                                            float pk, float2& sw, float2& sx, float2& sy, float2& sz, float2& sc,
-                                           float2& se, float& best, int& best_at) {
+                                           float2& se, float& best, int& best_at, float& second) {
+  constexpr int kSub = NearShape<G>::sub;
 #pragma unroll
-  for (int m = 0; m < kNearSlots; ++m) {
-    // Slots m.. hold elements from 2 kNearSub m on; in a batch's last tile (count < 128)
-    // the warp stops at a 32-element boundary once they are all blank (count is
-    // warp-uniform, so the branch is too).
-    if (m > 0 && m % 2 == 0 && 2 * kNearSub * m >= count) break;
-    const int u = sub + kNearSub * m;
+  for (int m = 0; m < NearShape<G>::slots; ++m) {
+    // Slots m.. hold elements from 2 kSub m on; in a batch's last tile (count < 128) the
+    // warp stops at a 32-element boundary once they are all blank (count is warp-uniform,
+    // so the branch is too).
+    if (m > 0 && (2 * kSub * m) % 32 == 0 && 2 * kSub * m >= count) break;
+    const int u = sub + kSub * m;
     const int first = 2 * u;
     const float4 A = T.wx[u], B = T.yz[u];
     const float2 mw = fma2(make_float2(A.x, A.y), splat(-1.0f), xw);
@@ -648,6 +662,20 @@ __device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub
       if (own0 && c.x != i) n0 = 4.0f;
       if (own1 && c.y != i) n1 = 4.0f;
     }
+    if (NEAREST) {
+      // The two smallest chords (of distinct sites) and where the smallest is.
+      second = fminf(second, fmaxf(best, fminf(n0, n1)));
+      second = fminf(second, fmaxf(n0, n1));
+      if (n0 < best) {
+        best = n0;
+        best_at = (int)T.at[first];
+      }
+      if (n1 < best) {
+        best = n1;
+        best_at = (int)T.at[first + 1];
+      }
+      continue;
+    }
     if (TRACK) {
       if (n0 < best) {
         best = n0;
@@ -660,7 +688,6 @@ __device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub
     } else {
       best = fminf(best, fminf(n0, n1));
     }
-    if (NEAREST) continue;
     // A site beyond the cutoff takes the chord at 1.25 r: its terms stay finite (a site
     // nearer the antipode, dm2 > 2, would drive the half-angle out of range) and the
     // window makes them exactly zero.
@@ -685,34 +712,30 @@ __device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub
   }
 }
 
-template <bool TRACK, bool SHORT, bool NEAREST = false>
-__global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __restrict__ q, int n,
-                                                              const uint32_t* __restrict__ src_perm,
-                                                              const float4* __restrict__ sq,
-                                                              const uint32_t* __restrict__ scode,
-                                                              const uint32_t* __restrict__ cell_off,
-                                                              const float* __restrict__ site_x,
-                                                              const NearGrid* __restrict__ gp, NearCut cut, int slices,
-                                                              Rows out, int stride, int direct) {
-  __shared__ NearTile tiles[kNearWarps];
-  __shared__ NearWalk walks[kNearWarps];
-  __shared__ double sums[6][kNearWarps * 32];  // FP64 lane sums: force differences, curvature, energy
+// One warp task of the gather: warp `warp` (G sources along the Hilbert order) and slice
+// `slice` of the sample in A; T, W and sums are the warp's shared memory.
+template <int G, bool TRACK, bool SHORT, bool NEAREST>
+__device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int slice, NearTile& T, NearWalk<G>& W,
+                                            double (*sums)[kNearWarps * 32]) {
+  constexpr int kSub = NearShape<G>::sub;
   const unsigned full = 0xffffffffu;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  NearTile& T = tiles[w];
-  NearWalk& W = walks[w];
-  const int warp = blockIdx.x * kNearWarps + w;
-  const int slice = blockIdx.y;
-  if (warp * kNearGroup >= n) return;
-  const int sub = lane % kNearSub;
-  const int p = warp * kNearGroup + lane / kNearSub;
+  const int lane = threadIdx.x & 31;
+  const int n = A.n, slices = A.slices;
+  const uint32_t* __restrict__ cell_off = A.cell_off;
+  const float* __restrict__ site_x = A.site_x;
+  const float4* __restrict__ sq = A.sq;
+  const uint32_t* __restrict__ scode = A.scode;
+  const NearCut& cut = A.cut;
+  if (warp * G >= n) return;
+  const int sub = lane % kSub;
+  const int p = warp * G + lane / kSub;
   const bool live = p < n;
-  const uint32_t i = live ? src_perm[p] : 0u;
-  const float4 x = q[i];
+  const uint32_t i = live ? A.src_perm[p] : 0u;
+  const float4 x = A.q[i];
   {
     // This source's chart ball, 0.1% wider (plus 1e-6) for the FP32 rounding of the chart.
-    const NearGrid g = *gp;
-    const double kappa = 1.0 - 0.5 * cut.cut2;
+    const NearGrid g = *A.gp;
+    const double kappa = 1.0 - 0.5 * cut.walk2;
     const double den = 1.0 / ((double)x.x + kappa);
     const float c[3] = {(float)(x.y * den), (float)(x.z * den), (float)(x.w * den)};
     const float rho = (float)(sqrt(1.0 - kappa * kappa) * den) * 1.001f + 1e-6f;
@@ -723,7 +746,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
     }
     if (!(lo[0] <= hi[0])) return;  // no live source in this warp
     if (sub == 0) {
-      const int s = lane / kNearSub;
+      const int s = lane / kSub;
       for (int a = 0; a < 3; ++a) W.cen[s][a] = c[a];
       W.rad[s] = live ? rho : -1.0f;
       W.src[s] = live ? i : 0xfffffffeu;
@@ -744,7 +767,7 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
               czw = (float)(cut.cut_z * cut.cut_w), pk = (float)(-6.0 * kPi * cut.cut_w);
   const float nx2 = 2.0f * fmaf(x.x, x.x, fmaf(x.y, x.y, fmaf(x.z, x.z, x.w * x.w)));
   const float2 xw = splat(x.x), xx = splat(x.y), xy = splat(x.z), xz = splat(x.w), xn = splat(nx2);
-  float best = 4.0f;
+  float best = 4.0f, second = 4.0f;
   int best_at = -1;
   float2 sw = splat(0.f), sx = splat(0.f), sy = splat(0.f), sz = splat(0.f), sc = splat(0.f), se = splat(0.f);
   int since = 0;  // tiles since the last FP64 merge
@@ -822,12 +845,12 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
         T.wx[slot] = make_float4(y[0].x, y[1].x, y[0].y, y[1].y);
         T.yz[slot] = make_float4(y[0].z, y[1].z, y[0].w, y[1].w);
         T.code[slot] = make_uint2(code[0], code[1]);
-        if (!SHORT)
+        if (!SHORT && !NEAREST)
           T.norm[slot] = make_float2(2.0f * fmaf(y[0].x, y[0].x, fmaf(y[0].y, y[0].y, fmaf(y[0].z, y[0].z, y[0].w * y[0].w))),
                                      2.0f * fmaf(y[1].x, y[1].x, fmaf(y[1].y, y[1].y, fmaf(y[1].z, y[1].z, y[1].w * y[1].w))));
         if (TRACK) reinterpret_cast<uint2*>(T.at)[slot] = make_uint2(site[0], site[1]);
 #pragma unroll
-        for (int s2 = 0; s2 < kNearGroup; ++s2)
+        for (int s2 = 0; s2 < G; ++s2)
           mine |= ((code[0] & ~kIdentityBit) == W.src[s2]) | ((code[1] & ~kIdentityBit) == W.src[s2]);
       }
       // Whether the tile holds an image of one of the warp's sources (rare): only then does
@@ -836,13 +859,13 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
       __syncwarp();
       if (live) {
         if (tile_own)
-          near_slots<TRACK, SHORT, true, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
-                                                  sz, sc, se, best, best_at);
+          near_slots<G, TRACK, SHORT, true, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
+                                                  sz, sc, se, best, best_at, second);
         else
-          near_slots<TRACK, SHORT, false, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
-                                                   sz, sc, se, best, best_at);
+          near_slots<G, TRACK, SHORT, false, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
+                                                   sz, sc, se, best, best_at, second);
       }
-      if (!NEAREST && ++since == kNearMerge) {
+      if (!NEAREST && ++since == NearShape<G>::merge) {
         merge_sums(sums, sw, sx, sy, sz, sc, se);
         since = 0;
       }
@@ -852,8 +875,12 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
   // The nearest over the source's lanes: smallest chord, then smallest sorted-site index
   // (the first such site in the walk's order).
 #pragma unroll
-  for (int o = kNearSub / 2; o > 0; o >>= 1) {
+  for (int o = kSub / 2; o > 0; o >>= 1) {
     const float ob = __shfl_xor_sync(full, best, o);
+    if (NEAREST) {
+      const float os = __shfl_xor_sync(full, second, o);
+      second = fminf(fminf(second, os), fmaxf(best, ob));
+    }
     if (TRACK) {
       const int oa = __shfl_xor_sync(full, best_at, o);
       if (ob < best || (ob == best && (unsigned)oa < (unsigned)best_at)) {
@@ -866,6 +893,17 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
   }
   __syncwarp();
   if (!live || sub != 0) return;
+  if (NEAREST) {
+    // The FP32 winner is the FP64 nearest when no other site's FP32 chord is within twice
+    // the chord error of it, and when the FP64 nearest cannot lie outside the walked ball;
+    // any other source is listed for the exact FP64 search (k_nearest_exact), which
+    // overwrites its row.
+    const double b = best, margin = 2.0 * chord_error32(b);
+    if ((double)second <= b + margin || b + margin > cut.walk2) {
+      const uint32_t slot = atomicAdd(A.exact_count, 1u);
+      A.exact_list[slot] = i;
+    }
+  }
   if (best > cut2) {  // no site within the cutoff
     best = 4.0f;
     best_at = -1;
@@ -873,15 +911,115 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const float4* __r
   double t[6];
   for (int c = 0; c < 6; ++c) {
     t[c] = 0.0;
-    for (int l = 0; l < kNearSub; ++l) t[c] += sums[c][threadIdx.x + l];
+    for (int l = 0; l < kSub; ++l) t[c] += sums[c][threadIdx.x + l];
   }
   const double3 f = force_from_differences(to_d4(x), make_double4(t[0], t[1], t[2], t[3]));
   // direct (one slice): the source's own row; else row p of this slice's partial rows.
-  const size_t at = direct ? (size_t)i : (size_t)slice * stride + p;
-  out.force[at] = make_double4(f.x, f.y, f.z, t[4]);
-  out.energy[at] = kPi * t[5];
-  out.nearest[at] = best;
-  if (TRACK) out.nearest_at[at] = best_at;
+  const size_t at = A.direct ? (size_t)i : (size_t)slice * A.stride + p;
+  A.out.force[at] = make_double4(f.x, f.y, f.z, t[4]);
+  A.out.energy[at] = kPi * t[5];
+  A.out.nearest[at] = best;
+  if (TRACK) A.out.nearest_at[at] = best_at;
+}
+
+template <int G, bool TRACK, bool SHORT, bool NEAREST>
+__global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const NearArgs A) {
+  __shared__ NearTile tiles[kNearWarps];
+  __shared__ NearWalk<G> walks[kNearWarps];
+  __shared__ double sums[6][kNearWarps * 32];  // FP64 lane sums: force differences, curvature, energy
+  const int w = threadIdx.x >> 5;
+  near32_warp<G, TRACK, SHORT, NEAREST>(A, blockIdx.x * kNearWarps + w, blockIdx.y, tiles[w], walks[w], sums);
+}
+
+// The exact nearest orbit neighbour of each source the FP32 spacing gather listed: every
+// site in the chart ball of the cutoff (the whole shell's reach, not the first walk's
+// smaller ball), its chord in FP64 from the float32 positions with the image formed in FP64
+// and both normalised (the oracle's definition), and the smallest chord kept, then the
+// smallest source index, then the first sorted site. A warp per listed source, its lanes
+// over the ball's cell rows. Writes the source's nearest chord and site (the refinement
+// that follows recomputes the chord of that site and its source index), and counts the
+// sources whose nearest chord is shared exactly by two different sources (exact ties).
+__global__ void __launch_bounds__(128) k_nearest_exact(const float4* __restrict__ q, int gid,
+                                                       const uint32_t* __restrict__ scode,
+                                                       const uint32_t* __restrict__ simg,
+                                                       const uint32_t* __restrict__ cell_off,
+                                                       const NearGrid* __restrict__ gp, double cut2,
+                                                       const uint32_t* __restrict__ list,
+                                                       const uint32_t* __restrict__ listed, Rows out,
+                                                       unsigned int* __restrict__ ties) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const uint32_t count = *listed;
+  const int off = c_group_offset[gid];
+  const NearGrid g = *gp;
+  const uint32_t stride = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += stride) {
+    const uint32_t i = list[w];
+    const double4 x = normalize4(to_d4(q[i]));
+    // The cutoff's chart ball (as in k_near32), 0.1% wider plus 1e-6.
+    const double kappa = 1.0 - 0.5 * cut2;
+    const double den = 1.0 / (x.x + kappa);
+    const double cen[3] = {x.y * den, x.z * den, x.w * den};
+    const double rho = sqrt(1.0 - kappa * kappa) * den * 1.001 + 1e-6;
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = cell_axis((float)(cen[a] - rho), g.lower[a], g.cells_per_unit, g.sdim);
+      hi[a] = cell_axis((float)(cen[a] + rho), g.lower[a], g.cells_per_unit, g.sdim);
+    }
+    const int ny = hi[1] - lo[1] + 1, rows = ny * (hi[2] - lo[2] + 1);
+    double best = 4.0;
+    uint32_t best_src = 0xffffffffu, best_site = 0xffffffffu;
+    bool tie = false;
+    for (int r = lane; r < rows; r += 32) {
+      const int row = g.sdim * (lo[1] + r % ny + g.sdim * (lo[2] + r / ny));
+      const uint32_t end = cell_off[row + hi[0] + 1];
+      for (uint32_t t = cell_off[row + lo[0]]; t < end; ++t) {
+        const uint32_t code = scode[t];
+        if (code == (i | kIdentityBit)) continue;  // the source itself
+        const uint32_t j = code & ~kIdentityBit, im = simg[t];
+        const int op = (int)(im >> 1);
+        double4 y = normalize4(op == 0 ? to_d4(q[j]) : qmul(to_d4(q[j]), c_ops32[off + op]));
+        if (im & 1u) y = neg4(y);
+        const double mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
+        const double d = mw * mw + mx * mx + my * my + mz * mz;
+        if (d < best) {
+          best = d;
+          best_src = j;
+          best_site = t;
+          tie = false;
+        } else if (d == best) {
+          tie |= j != best_src;
+          if (j < best_src || (j == best_src && t < best_site)) {
+            best_src = j;
+            best_site = t;
+          }
+        }
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      const double ob = __shfl_xor_sync(full, best, o);
+      const uint32_t os = __shfl_xor_sync(full, best_src, o), ot = __shfl_xor_sync(full, best_site, o);
+      const bool otie = __shfl_xor_sync(full, tie ? 1 : 0, o) != 0;
+      if (ob < best) {
+        best = ob;
+        best_src = os;
+        best_site = ot;
+        tie = otie;
+      } else if (ob == best) {
+        tie = tie || otie || (os != best_src && ob < 4.0);
+        if (os < best_src || (os == best_src && ot < best_site)) {
+          best_src = os;
+          best_site = ot;
+        }
+      }
+    }
+    if (lane == 0) {
+      const bool found = best <= cut2;
+      out.nearest[i] = found ? best : 4.0;
+      out.nearest_at[i] = found ? (int)best_site : -1;
+      if (found && tie) atomicAdd(ties, 1u);
+    }
+  }
 }
 
 template <bool TRACK>
@@ -1170,6 +1308,26 @@ cudaError_t launch_dense_near(int prec, bool track, bool short_atan, const float
 }
 
 // ------------------------------------------------------------------ the pass
+// The FP32 gather kernel of a tile shape (G sources per warp) and variant.
+template <int G>
+cudaError_t launch_near32_shape(bool track, bool short_atan, bool nearest, dim3 grid, const NearArgs& A,
+                                cudaStream_t s) {
+  auto kernel = nearest ? k_near32<G, true, false, true>
+                        : track ? (short_atan ? k_near32<G, true, true, false> : k_near32<G, true, false, false>)
+                                : (short_atan ? k_near32<G, false, true, false> : k_near32<G, false, false, false>);
+  kernel<<<grid, kNearWarps * 32, 0, s>>>(A);
+  return cudaGetLastError();
+}
+inline cudaError_t launch_near32(int G, bool track, bool short_atan, bool nearest, dim3 grid, const NearArgs& A,
+                                 cudaStream_t s) {
+  switch (G) {
+    case 2: return launch_near32_shape<2>(track, short_atan, nearest, grid, A, s);
+    case 4: return launch_near32_shape<4>(track, short_atan, nearest, grid, A, s);
+    case 8: return launch_near32_shape<8>(track, short_atan, nearest, grid, A, s);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 // Site count of a shell pass (offsets[n] after the scan), for sizing the workspace.
 cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, int n, int gid, double s_margin,
                                uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, uint4* masks,
@@ -1181,7 +1339,8 @@ cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, 
   return launch_scan(counts, offsets, n, nullptr, scan_tmp, s);
 }
 
-cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
+// Parts 1-3 of a pass: shell, chart grid and site sort, sources in Hilbert order.
+cudaError_t launch_near_structure(const NearLaunch& L, cudaStream_t s, int* launches) {
   const int n = L.n;
   const bool fp64 = L.prec == kFP64;
   const int tb = 256;
@@ -1201,9 +1360,9 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
                                                           L.site_q32, L.site_q64, L.site_code, L.site_img, L.site_pos,
                                                           L.grid);
   // 2. grid and the site sort
-  k_grid_setup<<<1, 1, 0, s>>>(L.grid, L.offsets + n, L.capacity, L.sdim_max, L.cells);
+  k_grid_setup<<<1, 1, 0, s>>>(L.grid, L.offsets + n, L.capacity, L.sdim_max, (float)L.sites_per_cell, L.cells);
   const int max_cells = L.sdim_max * L.sdim_max * L.sdim_max;
-  cudaMemsetAsync(L.cell_count, 0, sizeof(uint32_t) * (max_cells + 1), s);
+  if ((e = cudaMemsetAsync(L.cell_count, 0, sizeof(uint32_t) * (max_cells + 1), s))) return e;
   k_cell_count<<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.site_pos, L.grid, L.site_cell, L.site_rank, L.cell_count);
   if ((e = launch_scan(L.cell_count, L.cell_off, max_cells, L.cells, L.scan_tmp, s))) return e;
   k_scatter<<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.site_cell, L.site_rank, L.cell_off, L.capacity,
@@ -1219,7 +1378,7 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
                                                                    L.simg, L.sx);
   // 3. sources in Hilbert order
   const int mcells = kOrderDim * kOrderDim * kOrderDim;
-  cudaMemsetAsync(L.mcount, 0, sizeof(uint32_t) * (mcells + 1), s);
+  if ((e = cudaMemsetAsync(L.mcount, 0, sizeof(uint32_t) * (mcells + 1), s))) return e;
   if (fp64)
     k_source_count<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.grid, L.src_key, L.src_rank, L.mcount);
   else
@@ -1227,37 +1386,151 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   if ((e = launch_scan(L.mcount, L.moff, mcells, nullptr, L.scan_tmp, s))) return e;
   k_scatter<<<(n + tb - 1) / tb, tb, 0, s>>>(L.src_key, L.src_rank, L.moff, n, nullptr, L.src_perm);
   k_bucket_sort<<<(mcells + tb - 1) / tb, tb, 0, s>>>(L.moff, mcells, nullptr, L.src_perm);
+  // shell masks (1 or 3), shell write, grid, cell count, scatter, bucket sort, site gather,
+  // source count, scatter, bucket sort (scans counted by launch_scan; memsets aside)
+  *launches = 9 + shell_launches;
+  return cudaGetLastError();
+}
+
+// Slices of the gather of a pass: the FP32 spacing pass writes rows in place (one slice), so
+// that its exact search can overwrite the rows of the sources it takes over.
+inline int near_slices(const NearLaunch& L) {
+  return L.prec == kFP64 ? L.slices : (L.nearest_only ? 1 : L.slices32);
+}
+
+NearTask near_task(const NearLaunch& L) {
+  const int slices = near_slices(L);
+  const int direct = slices == 1 ? 1 : 0;
+  NearTask t{};
+  t.a = NearArgs{L.q32, L.n, L.src_perm, L.sq32, L.scode, L.cell_off, L.sx, L.grid,
+                 near_cut(L.cut2, L.chord, L.cut_z, L.cut_w), slices, direct ? L.out : L.partial, L.n, direct,
+                 L.exact_list, L.exact_count};
+  t.group_size = L.group_size;
+  t.short_atan = L.short_atan ? 1 : 0;
+  t.warps = (L.n + L.group_size - 1) / L.group_size;
+  t.slices = slices;
+  return t;
+}
+
+// Part 5: the slices' partial rows summed in slice order into the rows (more than one slice).
+cudaError_t launch_near_reduce(const NearLaunch& L, cudaStream_t s) {
+  const int slices = near_slices(L);
+  if (L.prec != kFP64 && slices == 1) return cudaSuccess;
+  k_rows_reduce<<<(L.n + 31) / 32, 32 * kReduceWarps, 0, s>>>(L.partial, L.n, slices, L.n, (const int*)L.src_perm,
+                                                             L.out, L.track ? 1 : 0);
+  probe_count();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
+  const int n = L.n;
+  const bool fp64 = L.prec == kFP64;
+  int structure_launches = 0;
+  cudaError_t e = launch_near_structure(L, s, &structure_launches);
+  if (e) return e;
+  probe_count(structure_launches);
   // 4. gather, 5. slices summed into rows
-  const int warps = fp64 ? (n + 31) / 32 : (n + kNearGroup - 1) / kNearGroup;
-  const int slices = fp64 ? L.slices : L.slices32;
+  const int G = L.group_size;
+  const int warps = fp64 ? (n + 31) / 32 : (n + G - 1) / G;
+  const bool nearest_only = !fp64 && L.nearest_only;
+  const int slices = near_slices(L);
   const dim3 grid((warps + kNearWarps - 1) / kNearWarps, slices);
-  const NearCut cut = near_cut(L.cut2, L.chord, L.cut_z, L.cut_w);
-  const Rows dst = L.partial;
-  probe_mark(s);
-  if (fp64) {
-    if (L.track) k_near64<true><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
-    else k_near64<false><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, dst, n);
-  } else {
-    auto kernel = L.track ? (L.short_atan ? k_near32<true, true> : k_near32<true, false>)
-                          : (L.short_atan ? k_near32<false, true> : k_near32<false, false>);
-    if (L.nearest_only) kernel = k_near32<true, false, true>;
-    // One slice: each warp writes its sources' rows in place, no partial rows to reduce.
-    const int direct = slices == 1 ? 1 : 0;
-    kernel<<<grid, kNearWarps * 32, 0, s>>>(L.q32, n, L.src_perm, L.sq32, L.scode, L.cell_off, L.sx, L.grid, cut,
-                                            slices, direct ? L.out : dst, n, direct);
-    if (direct) {
-      probe_mark(s);
-      probe_count(10 + shell_launches);
-      return cudaGetLastError();
-    }
+  NearCut cut = near_cut(L.cut2, L.chord, L.cut_z, L.cut_w);
+  if (nearest_only) {
+    cut.walk2 = std::min(L.walk_cut2, L.cut2);
+    if ((e = cudaMemsetAsync(L.exact_count, 0, 2 * sizeof(uint32_t), s))) return e;
   }
   probe_mark(s);
-  k_rows_reduce<<<(n + 31) / 32, 32 * kReduceWarps, 0, s>>>(L.partial, n, slices, n, (const int*)L.src_perm, L.out,
-                                                           L.track ? 1 : 0);
-  // shell masks (1 or 3), shell write, grid, cell count, scatter, bucket sort, site gather,
-  // source count, scatter, bucket sort, gather, reduce (scans counted by launch_scan;
-  // memsets aside)
-  probe_count(11 + shell_launches);
+  if (fp64) {
+    if (L.track) k_near64<true><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, L.partial, n);
+    else k_near64<false><<<grid, kNearWarps * 32, 0, s>>>(L.q64, n, L.src_perm, L.sq64, L.scode, L.cell_off, L.grid, cut, L.slices, L.partial, n);
+  } else {
+    NearTask t = near_task(L);
+    t.a.cut = cut;
+    if ((e = launch_near32(G, L.track, L.short_atan, nearest_only, grid, t.a, s))) return e;
+  }
+  probe_mark(s);
+  probe_count();
+  if (nearest_only) {
+    // A warp per listed source, grid-stride; the list's length is read on the device.
+    const int blocks = std::max(1, std::min((n + 3) / 4, 148 * 8));
+    k_nearest_exact<<<blocks, 128, 0, s>>>(L.q32, L.gid, L.scode, L.simg, L.cell_off, L.grid, L.cut2, L.exact_list,
+                                           L.exact_count, L.out, L.exact_count + 1);
+    probe_count();
+  }
+  if ((e = launch_near_reduce(L, s))) return e;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ many samples, one gather
+// The gathers of many samples' passes in one persistent launch per tile variant (sources per
+// warp and pair form; a batch has one or a few): every resident warp takes the next warp
+// task (a sample's warp of sources and slice) from a device counter until all are done, so
+// samples of any size share the GPU without a tail per sample. Tasks are in the order of
+// `tasks` (largest first); prefix[k] is the first warp task of sample k. Each task runs the
+// same warp function as the sample's own gather launch, so its rows are the same bit for
+// bit. Relaxation steps only (no neighbour tracking, no spacing pass).
+template <int G, bool SHORT>
+__global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32_batch(const NearTask* __restrict__ tasks,
+                                                                    const uint32_t* __restrict__ prefix, int count,
+                                                                    uint32_t total, uint32_t* __restrict__ counter) {
+  __shared__ NearTile tiles[kNearWarps];
+  __shared__ NearWalk<G> walks[kNearWarps];
+  __shared__ double sums[6][kNearWarps * 32];
+  __shared__ NearTask mine[kNearWarps];  // the warp's current task, copied in by its lanes
+  static_assert(sizeof(NearTask) % 4 == 0, "task words");
+  constexpr int kWords = (int)(sizeof(NearTask) / 4);
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (;;) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(counter, 1u);
+    t = __shfl_sync(full, t, 0);
+    if (t >= total) break;
+    int lo = 0, hi = count - 1;  // the last sample whose first task is at most t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const uint32_t* from = reinterpret_cast<const uint32_t*>(&tasks[lo]);
+    uint32_t* to = reinterpret_cast<uint32_t*>(&mine[w]);
+    for (int k = lane; k < kWords; k += 32) to[k] = from[k];
+    __syncwarp();
+    const uint32_t local = t - prefix[lo];
+    const uint32_t warps = (uint32_t)mine[w].warps;
+    near32_warp<G, false, SHORT, false>(mine[w].a, (int)(local % warps), (int)(local / warps), tiles[w], walks[w],
+                                        sums);
+    __syncwarp();
+  }
+}
+
+// Tile variant of a task: index into the six (sources per warp 2, 4, 8) x (pair form) kernels.
+int near_variant(const NearTask& t) {
+  return (t.group_size == 2 ? 0 : t.group_size == 4 ? 1 : 2) * 2 + (t.short_atan ? 1 : 0);
+}
+
+cudaError_t launch_near32_batch(const NearTask* tasks, const uint32_t* prefix, int count, uint32_t total,
+                                uint32_t* counter, int variant, int sms, cudaStream_t s) {
+  if (count <= 0 || total == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+  if (e) return e;
+  const uint32_t resident = (uint32_t)sms * 7;  // blocks of four warps, seven per SM
+  const uint32_t blocks = std::max(1u, std::min(resident, (total + kNearWarps - 1) / kNearWarps));
+  decltype(&k_near32_batch<4, true>) kernel;
+  switch (variant) {
+    case 0: kernel = k_near32_batch<2, false>; break;
+    case 1: kernel = k_near32_batch<2, true>; break;
+    case 2: kernel = k_near32_batch<4, false>; break;
+    case 3: kernel = k_near32_batch<4, true>; break;
+    case 4: kernel = k_near32_batch<8, false>; break;
+    case 5: kernel = k_near32_batch<8, true>; break;
+    default: return cudaErrorInvalidValue;
+  }
+  probe_mark(s);
+  kernel<<<blocks, kNearWarps * 32, 0, s>>>(tasks, prefix, count, total, counter);
+  probe_mark(s);
+  probe_count();
   return cudaGetLastError();
 }
 

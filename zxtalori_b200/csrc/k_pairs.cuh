@@ -85,10 +85,10 @@ __global__ void k_fold(float4* __restrict__ q32, double4* __restrict__ q64, int 
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const bool fp64 = prec == kFP64;
-  double4 p = (from_q32 || !fp64) ? flush_normalize(q32[i]) : normalize4(q64[i]);
+  double4 p = (from_q32 || !q64) ? flush_normalize(q32[i]) : normalize4(q64[i]);
   p = fold64(p, gid, !fp64);
   q32[i] = to_f4(p);
-  if (fp64) q64[i] = p;
+  if (q64) q64[i] = p;  // the FP64 master positions (both modes)
 }
 
 // ------------------------------------------------------------------ device-wide scan

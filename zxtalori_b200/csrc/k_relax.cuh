@@ -169,8 +169,10 @@ __global__ void __launch_bounds__(256) k_median_round(Rows rows, int n, int roun
 }
 
 // relax_move (relax.wgsl:140-165) fused with the fold: d = f alpha/max(1e-6, c/median+0.01),
-// clipped to 0.5 d_r, q <- normalize(exp(d) q), w >= 0, folded; FP64, stored as float32
-// (and FP64 in FP64 mode). A held identity stays (1,0,0,0); after a flag nothing moves.
+// clipped to 0.5 d_r, q <- normalize(exp(d) q), w >= 0, folded; FP64. The move starts from
+// the FP64 master positions q64 and writes them back with their float32 rounding q32, which
+// the pair kernels of FP32 mode read (without a master, q64 null, it starts from q32).
+// A held identity stays (1,0,0,0); after a flag nothing moves.
 __global__ void k_move_fold(float4* __restrict__ q32, double4* __restrict__ q64, int n, int gid, int prec, Rows rows,
                             double4* __restrict__ prev_f, double4* __restrict__ prev_d, RelaxDev* st, int fixed,
                             double radius, double step_scale) {
@@ -182,7 +184,7 @@ __global__ void k_move_fold(float4* __restrict__ q32, double4* __restrict__ q64,
     prev_f[i] = make_double4(0, 0, 0, 0);
     prev_d[i] = make_double4(0, 0, 0, 0);
     q32[i] = make_float4(1.f, 0.f, 0.f, 0.f);
-    if (fp64) q64[i] = make_double4(1, 0, 0, 0);
+    if (q64) q64[i] = make_double4(1, 0, 0, 0);
   } else if (i < n) {
     const double alpha = st->alpha, median = st->median;
     const double4 f = rows.force[i];
@@ -197,11 +199,11 @@ __global__ void k_move_fold(float4* __restrict__ q32, double4* __restrict__ q64,
     const double angle = sqrt(dx * dx + dy * dy + dz * dz);
     const double sinc = angle > 1e-4 ? sin(angle) / angle : 1.0 - angle * angle / 6.0;
     const double4 rot = make_double4(cos(angle), dx * sinc, dy * sinc, dz * sinc);
-    const double4 qi = fp64 ? q64[i] : to_d4(q32[i]);
+    const double4 qi = q64 ? q64[i] : to_d4(q32[i]);
     double4 moved = normalize4(qmul(rot, qi));
     moved = fold64(moved, gid, !fp64);
     q32[i] = to_f4(moved);
-    if (fp64) q64[i] = moved;
+    if (q64) q64[i] = moved;
   }
   // The largest step: non-negative doubles order as their bit patterns; one atomic per warp.
   unsigned long long bits = (unsigned long long)__double_as_longlong(moved_by);

@@ -20,8 +20,12 @@ const HostTables& host_tables();
 int host_group_offset(int gid);
 int host_group_order(int gid);
 
-// Copies the group tables into the current device's constant memory (once per device).
+// Copies the group tables into the current device's constant memory.
 cudaError_t upload_tables(const HostTables& t);
+// upload_tables once per device (device current; the first caller uploads, under a lock),
+// for engines and the allocation-free entry point alike.
+constexpr int kMaxTableDevices = 64;
+cudaError_t ensure_device_tables(int device);
 
 cudaError_t launch_haar(float4* q, int n, uint32_t seed, cudaStream_t s);
 cudaError_t launch_fold(float4* q32, double4* q64, int n, int gid, int prec, bool from_q32, cudaStream_t s);
@@ -41,14 +45,62 @@ cudaError_t launch_pairs(int prec, bool track, const float4* q32, const double4*
 cudaError_t launch_full(int prec, const float4* q32, const double4* q64, int n, int gid, const PairsPlan& pl,
                         Rows partial, double* pextra, int* pdegen, Rows out, double* extra, int* degen, cudaStream_t s);
 
+// Cutoff of a near-field pass (pairs.wgsl:352-361): squared chord and chord of r, the
+// window's start taper r and inverse width 1/((1 - taper) r).
+struct NearCut {
+  double cut2, chord, cut_z, cut_w;
+  // Squared chord at angle 1.25 r, where the window is exactly zero: the packed gather
+  // evaluates an out-of-cutoff site with its chord clamped to this (finite terms, zero
+  // contribution) when the other site of its pair is within the cutoff.
+  double cut_hi;
+  // Squared chord of the ball the FP32 gather walks: the cutoff's, except in the spacing
+  // pass, whose first walk takes a smaller ball (sources it cannot settle are searched
+  // again over the whole cutoff).
+  double walk2;
+};
+
+// The arguments of one FP32 gather: one sample's sources, sorted sites and chart grid.
+struct NearArgs {
+  const float4* q;
+  int n;
+  const uint32_t* src_perm;
+  const float4* sq;
+  const uint32_t* scode;
+  const uint32_t* cell_off;
+  const float* site_x;
+  const NearGrid* gp;
+  NearCut cut;
+  int slices;
+  Rows out;
+  int stride;
+  int direct;  // one slice: rows written in place by source (else partial rows by slice)
+  uint32_t* exact_list;   // spacing pass: the sources left to the exact search
+  uint32_t* exact_count;
+};
+
+// One sample's FP32 gather as a task of a shared launch: its arguments, tile shape (sources
+// per warp), pair form (chord form for cutoffs up to 0.4 rad), warps and slices.
+struct NearTask {
+  NearArgs a;
+  int group_size, short_atan, warps, slices;
+};
+
 // One near-field pass; every pointer is device memory sized by the host (Near workspace).
 struct NearLaunch {
   int prec, gid, n, capacity, sdim_max, slices;
-  int slices32;  // slices of the FP32 gather (kNearGroup sources per warp); <= slices
+  int slices32;  // slices of the FP32 gather (group_size sources per warp); <= slices
+  int group_size;  // FP32 gather tile shape: sources per warp (2, 4 or 8)
+  double sites_per_cell;  // target shell sites per chart cell (sets the grid's side)
   bool track;
   bool short_atan;  // cutoff r <= 0.4 rad: the short-range arctangent applies
   bool nearest_only;  // FP32 gather: nearest chord and site only (forces, curvature, energy left 0)
   double s_margin, cut2, chord, cut_z, cut_w;
+  // Spacing pass (nearest_only): squared chord of the first walk's ball (at most cut2), and
+  // the sources it leaves to the exact FP64 search: their list (n entries) and two counters
+  // (listed sources, sources with an exact tie).
+  double walk_cut2;
+  uint32_t* exact_list;
+  uint32_t* exact_count;
   const float4* q32;
   const double4* q64;
   uint32_t *counts, *offsets, *scan_tmp;
@@ -72,6 +124,19 @@ struct NearLaunch {
   Rows out;
 };
 cudaError_t launch_near(const NearLaunch& L, cudaStream_t s);
+// The same pass in parts, for many samples sharing one gather launch: the structure (shell,
+// chart grid, site sort, source order), the FP32 gather as a task (near_task), and the
+// slices' reduction into the rows.
+cudaError_t launch_near_structure(const NearLaunch& L, cudaStream_t s, int* launches);
+NearTask near_task(const NearLaunch& L);
+cudaError_t launch_near_reduce(const NearLaunch& L, cudaStream_t s);
+// The FP32 gathers of many samples of one tile variant (near_variant; device arrays: `count`
+// tasks, prefix[k] the first warp task of sample k, `total` warp tasks) in one persistent
+// launch; `counter` is a device word.
+int near_variant(const NearTask& t);
+constexpr int kNearVariants = 6;
+cudaError_t launch_near32_batch(const NearTask* tasks, const uint32_t* prefix, int count, uint32_t total,
+                                uint32_t* counter, int variant, int sms, cudaStream_t s);
 // The near field for wide cutoffs, summed over every image (all-pairs tiles, near-field
 // cutoff and window); `partial` holds chunks*n rows when chunks > 1.
 cudaError_t launch_dense_near(int prec, bool track, bool short_atan, const float4* q32, const double4* q64, int n,

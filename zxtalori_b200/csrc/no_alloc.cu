@@ -45,7 +45,7 @@ void put_error(char* error, size_t error_len, const char* message) {
 
 // Once per device, with that device current: the scratch array's device address (the
 // array's name is only a host-side stand-in), the SM count, and the group tables in
-// constant memory. No allocation.
+// constant memory (through the engine's own once-per-device upload). No allocation.
 int setup(int device, char* error, size_t error_len) {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (g_ready[device]) return 0;
@@ -59,7 +59,7 @@ int setup(int device, char* error, size_t error_len) {
   }
   int sms = 0;
   e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  if (e == cudaSuccess) e = zo::upload_tables(zo::host_tables());
+  if (e == cudaSuccess) e = zo::ensure_device_tables(device);
   if (e != cudaSuccess) {
     char msg[256];
     std::snprintf(msg, sizeof msg, "device set-up: %s", cudaGetErrorString(e));
@@ -90,8 +90,18 @@ extern "C" int zo_pair_rows_noalloc(uint32_t group, const float* q_device, uint3
   }
   int device = 0;
   cudaError_t e = cudaGetDevice(&device);
-  if (e != cudaSuccess || device < 0 || device >= kMaxDevices) {
+  if (e != cudaSuccess || device < 0 || device >= kMaxDevices || device >= zo::kMaxTableDevices) {
     put_error(error, error_len, "no current CUDA device");
+    return -3;
+  }
+  // An error left pending by the caller's earlier work would otherwise be reported (and
+  // cleared) as this call's launch failure: refuse, and leave it pending for its owner.
+  e = cudaPeekAtLastError();
+  if (e != cudaSuccess) {
+    char msg[256];
+    std::snprintf(msg, sizeof msg, "a CUDA error is pending from earlier work on this thread: %s",
+                  cudaGetErrorString(e));
+    put_error(error, error_len, msg);
     return -3;
   }
   const int rc = setup(device, error, error_len);

@@ -12,10 +12,11 @@ constexpr int kMaxCellDim = 128;        // chart grid side (src/near.zig:135)
 // reference sorts them into a 32^3 Morton grid, src/near.zig:23).
 constexpr int kOrderBits = 6;
 constexpr int kOrderDim = 1 << kOrderBits;
-// Target sites per cell of the chart grid (the reference uses 8, src/near.zig:135).
+// Default tile shape of the FP32 near-field gather (the tile table can pick others per group
+// and size): target shell sites per chart cell (the reference uses 8, src/near.zig:135) and
+// sources per warp (each source's sites split over 32 / kNearGroup lanes; small groups keep
+// the union of the sources' neighbourhoods close to each one's).
 constexpr double kSitesPerCell = 2.0;
-// FP32 near-field gather: sources per warp (each source's sites split over 32 / kNearGroup
-// lanes). Small groups keep the union of the sources' neighbourhoods close to each one's.
 constexpr int kNearGroup = 4;
 
 // Precision of one sample's arithmetic.

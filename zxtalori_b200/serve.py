@@ -1,18 +1,22 @@
 """Continuous-batching relax + measure service on one GPU.
 
 Requests (group, N, steps, seed, neighbourhood) arrive over time. The loop admits waiting
-requests in arrival order while their estimated device memory fits the budget, keeps each
-admitted sample resident in its own engine (own CUDA stream, FP32 steps replayed from a
-captured graph), and advances every active sample a chunk of steps whenever its stream is
-idle, so the kernels of all active samples overlap on the device. A request finishes -
-closing force pass, Quey energy and separation, positions read back - as soon as its steps
-are done, and its memory goes to the next admission. Results do not depend on what else
-is running: every sample's kernels read only its own buffers and sum in a fixed order.
+requests in arrival order while their device memory fits the budget, keeps each admitted
+sample resident in its own engine (own CUDA stream, FP32 steps replayed from a captured
+graph), and advances every active sample a chunk of steps whenever its stream is idle, so
+the kernels of all active samples overlap on the device. A request whose steps are done is
+handed to a worker thread for its blocking part - closing force pass, measure() (every
+energy ratio below the ratio limit), positions read back, engine closed - while the loop
+keeps feeding the others; its memory then goes to the next admission. Admission counts
+each resident sample at the device bytes its engine reports once its workspace is sized
+(an estimate before that). Results do not depend on what else is running: every sample's
+kernels read only its own buffers and sum in a fixed order.
 """
 from __future__ import annotations
 
 import math
 import time
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -77,20 +81,23 @@ class _Active:
     admitted: float
     bytes: int
     per_step_s: float = 0.0
-    started: bool = False
+    sized: bool = False  # bytes is the engine's own report (its workspace is sized)
 
 
 @dataclass
 class Server:
     """Continuous-batching loop. `memory_budget` bytes (default: 80% of free device memory)
     bound the resident samples; `max_active` caps concurrency; each chunk aims at
-    `chunk_seconds` of estimated device work per sample."""
+    `chunk_seconds` of estimated device work per sample; `workers` threads run the finishing
+    part of completed requests; `measure` runs measure() on each result."""
     precision: str = "fp32"
     memory_budget: int | None = None
     max_active: int = 64
     chunk_seconds: float = 0.02
     keep_quaternions: bool = False
-    pair_rate: float = 1.2e11  # pair evaluations per second, for chunk sizing only
+    measure: bool = True
+    workers: int = 4
+    pair_rate: float = 2.5e11  # pair evaluations per second, for chunk sizing only
     results: list = field(default_factory=list)
 
     def _admit(self, r, now):
@@ -100,56 +107,78 @@ class Server:
         return _Active(r, g, r.steps, now, estimate_bytes(r.count, r.group, r.neighbourhood),
                        per_step_s=evals / self.pair_rate)
 
+    def _finish(self, a, t0, clock):
+        """The blocking part of a request (a worker thread; the engine is no longer stepped)."""
+        lib, h = a.grid._lib, a.grid._handle
+        try:
+            a.grid._check(lib.zo_relax_finish(h))
+            if self.measure:
+                a.grid._check(lib.zo_measure(h))
+            stats = a.grid.stats
+            q = a.grid.quaternions if self.keep_quaternions else None
+            return Result(a.request.id, a.request.arrival, a.admitted, clock() - t0, stats, q)
+        finally:
+            a.grid.close()
+
     def run(self, requests, clock=time.perf_counter):
         """Serve `requests` (arrival times in seconds from the start); returns the results
         in completion order."""
         pending = sorted(requests, key=lambda r: (r.arrival, r.id))
         budget = self.memory_budget if self.memory_budget is not None else int(0.8 * device_free_bytes())
-        active: list[_Active] = []
+        stepping: list[_Active] = []
+        finishing = {}  # future -> _Active
         t0 = clock()
         held = 0
-        while pending or active:
-            now = clock() - t0
-            while (pending and pending[0].arrival <= now and len(active) < self.max_active
-                   and (held + estimate_bytes(pending[0].count, pending[0].group, pending[0].neighbourhood) <= budget
-                        or not active)):
-                a = self._admit(pending.pop(0), now)
-                held += a.bytes
-                active.append(a)
-            progressed = False
-            for a in list(active):
-                lib, h = a.grid._lib, a.grid._handle
-                idle = lib.zo_idle(h)
-                if idle < 0:
-                    a.grid._check(-1)
-                if not idle:
-                    continue
-                if a.remaining > 0:
-                    k = max(1, min(a.remaining, int(self.chunk_seconds / max(a.per_step_s, 1e-9))))
-                    a.grid._check(lib.zo_relax_async(h, k))
-                    a.remaining -= k
-                    a.started = True
+        with ThreadPoolExecutor(max_workers=max(1, self.workers)) as pool:
+            while pending or stepping or finishing:
+                now = clock() - t0
+                resident = len(stepping) + len(finishing)
+                # One sample at a time is admitted on its estimate: the next waits until the
+                # first chunk has sized its workspace and its engine has reported its bytes.
+                if (pending and pending[0].arrival <= now and resident < self.max_active
+                        and all(a.sized for a in stepping)
+                        and (held + estimate_bytes(pending[0].count, pending[0].group, pending[0].neighbourhood)
+                             <= budget or resident == 0)):
+                    a = self._admit(pending.pop(0), now)
+                    held += a.bytes
+                    stepping.append(a)
+                progressed = False
+                for a in list(stepping):
+                    lib, h = a.grid._lib, a.grid._handle
+                    idle = lib.zo_idle(h)
+                    if idle < 0:
+                        a.grid._check(-1)
+                    if not idle:
+                        continue
+                    if a.remaining > 0:
+                        k = max(1, min(a.remaining, int(self.chunk_seconds / max(a.per_step_s, 1e-9))))
+                        a.grid._check(lib.zo_relax_async(h, k))
+                        a.remaining -= k
+                        if not a.sized:  # the first chunk sized the workspace: count real bytes
+                            real = int(lib.zo_device_bytes(h))
+                            held += real - a.bytes
+                            a.bytes, a.sized = real, True
+                        progressed = True
+                        continue
+                    stepping.remove(a)
+                    finishing[pool.submit(self._finish, a, t0, clock)] = a
                     progressed = True
-                    continue
-                a.grid._check(lib.zo_relax_finish(h))
-                stats = a.grid.stats
-                q = a.grid.quaternions if self.keep_quaternions else None
-                self.results.append(Result(a.request.id, a.request.arrival, a.admitted, clock() - t0, stats, q))
-                a.grid.close()
-                held -= a.bytes
-                active.remove(a)
-                progressed = True
-            if not progressed:
-                if not active and pending:
-                    time.sleep(max(0.0, min(0.05, pending[0].arrival - (clock() - t0))))
-                else:
-                    time.sleep(0.0002)
+                for fut in [f for f in finishing if f.done()]:
+                    a = finishing.pop(fut)
+                    held -= a.bytes
+                    self.results.append(fut.result())  # re-raises a failed request's error
+                    progressed = True
+                if not progressed:
+                    if not stepping and not finishing and pending:
+                        time.sleep(max(0.0, min(0.05, pending[0].arrival - (clock() - t0))))
+                    else:
+                        time.sleep(0.0005)
         return self.results
 
 
-def serve_one_at_a_time(requests, precision="fp64", clock=time.perf_counter, keep_quaternions=False):
+def serve_one_at_a_time(requests, precision="fp64", clock=time.perf_counter, keep_quaternions=False, measure=True):
     """The plain path: requests in arrival order, one at a time, each relaxed with zo_relax
-    (no graphs, no overlap); FP64 by default."""
+    (no graphs, no overlap) and then measured; FP64 by default."""
     pending = sorted(requests, key=lambda r: (r.arrival, r.id))
     results = []
     t0 = clock()
@@ -162,6 +191,8 @@ def serve_one_at_a_time(requests, precision="fp64", clock=time.perf_counter, kee
         try:
             g._check(g._lib.zo_graphs(g._handle, 0))
             g.relax(r.steps, neighbourhood=r.neighbourhood)
+            if measure:
+                g.measure()
             results.append(Result(r.id, r.arrival, admitted, clock() - t0, g.stats,
                                   g.quaternions if keep_quaternions else None))
         finally:
