@@ -266,7 +266,7 @@ def e2e_requests(zo, seed, requests):
     return evals * len(lat) / sum(lat), lat, stats
 
 
-def batched_section(zo, samples=256, steps=50):
+def batched_section(zo, samples=256, steps=50, dist=None):
     """Config 4: 256 samples (groups uniform over the eleven, N log-uniform in [1e3, 2e5],
     seeds 0..255, neighbourhood 20), 50 BB steps each, relaxed together by zo_batch_relax:
     each step is one CUDA graph over all samples, whose near-field gathers run in one
@@ -274,26 +274,34 @@ def batched_section(zo, samples=256, steps=50):
     the whole batch (steps plus each sample's closing force pass), wall clock."""
     from zxtalori_b200 import batch, serve
 
-    specs = batch.random_samples(samples)
+    rank, world = (dist.rank, dist.world) if dist else (0, 1)
+    specs = batch.shard(batch.random_samples(samples), rank, world)  # all of them on one GPU
     t = time.perf_counter()
     grids = batch.make_grids(specs)
     setup = time.perf_counter() - t
     evals = sum(batch.pair_evals(s.count, serve.ORDER[s.group], s.neighbourhood, steps) for s in specs)
+    sum_n = sum(s.count for s in specs)
     try:
+        if dist:
+            dist.barrier()
         t = time.perf_counter()
         batch.relax_batch(grids, steps)
         dt = time.perf_counter() - t
     finally:
         for g in grids:
             g.close()
+    if dist:  # every rank's share at once: the slowest rank's time, all ranks' work
+        dt, setup = dist.reduce(dt, "max"), dist.reduce(setup, "max")
+        evals, sum_n = dist.reduce(evals, "sum"), int(dist.reduce(sum_n, "sum"))
     lib = zo.api._library()
     out = (C.c_double * 2)()
     shapes = {}
     for sp in specs:
         lib.zo_tiles_lookup(0, zo.GROUPS.index(sp.group), sp.count, out)
         shapes[f"{int(out[0])}x{out[1]:g}"] = shapes.get(f"{int(out[0])}x{out[1]:g}", 0) + 1
-    return {"samples": samples, "steps": steps, "sum_n": sum(s.count for s in specs), "pair_evals_per_s": evals / dt,
-            "seconds": dt, "setup_seconds": setup, "tile_shapes_from_table": shapes,
+    return {"samples": samples, "steps": steps, "sum_n": sum_n, "pair_evals_per_s": evals / dt,
+            "seconds": dt, "setup_seconds": setup, "tile_shapes_from_table": shapes, "gpus": world,
+            "split": "samples over ranks, largest first to the least-loaded rank; no collective",
             "timing": "wall clock of zo_batch_relax (all steps and closing passes), samples created beforehand"}
 
 
@@ -588,10 +596,12 @@ def run_ours(args, dist):
     # End to end through the public API.
     e2e_value, lat, _ = e2e_requests(zo, seed, requests=4)
     e2e_value = dist.reduce(e2e_value, "sum")
+    extras = {}
+    if args.gpus > 1 and not args.no_extras:
+        extras["batched"] = batched_section(zo, dist=dist)  # config 4 split over the ranks
     if dist.rank != 0:
         return 0
-    # All pairs, spacing, batched and served workloads (configs 1, 3, 4, 5), one GPU only.
-    extras = {}
+    # All pairs, spacing, batched and served workloads (configs 1, 3, 4, 5) on one GPU.
     if args.gpus == 1 and not args.no_extras:
         extras["allpairs"] = allpairs_section(zo, peak)
         extras["spacing"] = spacing_section(zo, hbm_peak(), measure_count=1_000_000 if args.large else None)

@@ -189,3 +189,18 @@ def test_summary_counts_pairs_as_the_reference():
     assert info["pair_evals_per_s"] == pytest.approx(evals / 4.0)
     assert info["requests"] == 2
     assert info["latency_p50_s"] == pytest.approx(2.5)
+
+
+def test_batch_shards_cover_every_sample_once_and_balance():
+    from zxtalori_b200 import batch
+
+    specs = batch.random_samples(256)
+    work_of = {s.seed: batch.pair_evals(s.count, serve.ORDER[s.group], s.neighbourhood, 50) for s in specs}
+    for world in (1, 2, 3, 8):
+        shares = [batch.shard(specs, r, world) for r in range(world)]
+        assert sorted(s.seed for share in shares for s in share) == list(range(256))
+        work = [sum(work_of[s.seed] for s in share) for share in shares]
+        assert max(work) <= sum(work) / world + max(work_of.values())  # greedy balance bound
+        assert shares == [batch.shard(specs, r, world) for r in range(world)]  # the same split on every rank
+    with pytest.raises(ValueError):
+        batch.shard(specs, 2, 2)

@@ -1,9 +1,9 @@
-"""Many samples relaxed side by side on one GPU.
+"""Many samples relaxed together on one GPU, and split over GPUs.
 
-Each sample is an engine with its own CUDA stream and resident state; in FP32 mode a step
-replays the sample's captured CUDA graph. `relax_batch` enqueues every sample's steps
-before waiting for any, so samples of uneven sizes and different groups run concurrently,
-then closes each with its force pass and readback (zo_batch_relax).
+Each sample is an engine with its own CUDA stream and resident state. `relax_batch` runs
+zo_batch_relax: every step of the batch is one CUDA graph over all its FP32 samples, whose
+near-field gathers run in one persistent launch per tile variant, then each sample closes
+with its force pass and readback. `shard` splits a batch over ranks (one process per GPU).
 """
 from __future__ import annotations
 
@@ -63,6 +63,25 @@ def relax_batch(grids, steps):
     return [g.stats for g in grids]
 
 
+def shard(samples, rank, world, steps=50):
+    """This rank's share of `samples` when `world` GPUs relax a batch together (one process
+    per GPU, no collective: samples are independent). Samples go, largest first by pair
+    evaluations, to the rank with the least work so far (ties to the lower rank), so every
+    rank computes the same split and the ranks finish close together. Returns the rank's
+    samples in their original order."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    order = {"C2": 2, "C3": 3, "C4": 4, "C6": 6, "D2": 4, "D3": 6, "D4": 8, "D6": 12, "T": 12, "O": 24, "I": 60}
+    work = [pair_evals(s.count, order[s.group], s.neighbourhood, steps) for s in samples]
+    load = [0.0] * world
+    owner = [0] * len(samples)
+    for k in sorted(range(len(samples)), key=lambda k: (-work[k], k)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        owner[k] = r
+        load[r] += work[k]
+    return [s for s, o in zip(samples, owner) if o == rank]
+
+
 def random_samples(count, seed=0, groups=("C2", "C3", "C4", "C6", "D2", "D3", "D4", "D6", "T", "O", "I"),
                    n_min=1000, n_max=200_000, neighbourhood=20.0):
     """Batched workload: groups uniform, N log-uniform in [n_min, n_max], seeds 0..count-1."""
@@ -74,4 +93,4 @@ def random_samples(count, seed=0, groups=("C2", "C3", "C4", "C6", "D2", "D3", "D
     return out
 
 
-__all__ = ["Sample", "make_grids", "relax_batch", "random_samples", "pair_evals", "neighbours", "Grid"]
+__all__ = ["Sample", "make_grids", "relax_batch", "random_samples", "shard", "pair_evals", "neighbours", "Grid"]

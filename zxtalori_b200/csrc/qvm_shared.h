@@ -7,7 +7,10 @@ namespace zo {
 constexpr int kMaxOperatorRows = 141;   // sum of |K| over the eleven groups
 constexpr int kMaxPlaneRows = 271;      // sum of 2|K|-1 zone bisector planes
 constexpr uint32_t kIdentityBit = 0x80000000u;  // site code: the source's identity image
-constexpr int kMaxCellDim = 128;        // chart grid side (src/near.zig:135)
+// Largest chart grid side. The reference clamps it at 128 (src/near.zig:135); at ten million
+// sources that holds about six sites per cell, so the cap here is 256, which keeps the target
+// sites per cell up to about 33 million shell sites.
+constexpr int kMaxCellDim = 256;
 // Sources are ordered along a Hilbert curve over a 64^3 grid of the chart box (the
 // reference sorts them into a 32^3 Morton grid, src/near.zig:23).
 constexpr int kOrderBits = 6;
