@@ -533,8 +533,8 @@ def errors_section(zo):
     s64n, p64n, _ = run2("fp64", _nudged(start))
     s64s, p64s, _ = run2("fp64", start)
     g = zo.from_quaternions(p32, GROUP, precision="fp64")
-    g.relax(0, neighbourhood=DELTA)
-    near_same = g.stats
+    g.relax(0, neighbourhood=DELTA)  # sets the neighbourhood; measure() then uses the near field
+    near_same = g.measure()
     g.close()
     a32, a64, a64s, a64n = all_pairs(p32), all_pairs(p64), all_pairs(p64s), all_pairs(p64n)
     near = ("quey_energy", "separation_deg")
