@@ -101,7 +101,9 @@ const int32_t* zo_point_neighbours(void* h);
 /* Tuning extension, no reference counterpart: the tile shape of this engine's FP32
  * near-field gathers (relaxation and spacing), instead of the tile table's choice:
  * sources per warp 2, 4 or 8 and target shell sites per chart cell (0.5..16); applies from
- * the next pass (the workspace is sized again). sources_per_warp 0 returns to the table.
+ * the next pass (the workspace is sized again). 1 (one source per thread, no shared tiles)
+ * applies to spacing passes only; relaxation passes then keep 4. sources_per_warp 0
+ * returns to the table.
  * The reference's tiling knobs are constants (src/pairs.zig:100-128, src/near.zig:22-29). */
 int zo_near_tiles(void* h, uint32_t sources_per_warp, float sites_per_cell);
 /* The tile table's choice for a pass kind (0 relaxation, 1 spacing), group and sample size:

@@ -134,10 +134,12 @@ def test_near_relax_fp32_vs_fp64(engine):
     assert np.minimum(np.linalg.norm(q - q64, axis=1), np.linalg.norm(q + q64, axis=1)).max() < 1e-4
 
 
-@pytest.mark.parametrize("sources_per_warp,sites_per_cell", [(2, 1.5), (2, 3.0), (8, 1.5), (8, 3.0), (4, 2.0)])
+@pytest.mark.parametrize("sources_per_warp,sites_per_cell",
+                         [(2, 1.5), (2, 3.0), (8, 1.5), (8, 3.0), (4, 2.0), (1, 2.0), (1, 3.0)])
 def test_every_tile_shape_matches_the_oracle(engine, ops32, sources_per_warp, sites_per_cell):
     """Each tile shape the tuner may choose (zo_near_tiles) gives the oracle's rows (near
-    field, O 30k) and the oracle's spacing indices (I 40k)."""
+    field, O 30k) and the oracle's spacing indices (I 40k). Shape 1 (one source per thread)
+    is the spacing pass's alone; the relaxation pass then keeps 4 sources per warp."""
     with engine.haar("O", 30000, 23) as grid:
         grid._check(grid._lib.zo_near_tiles(grid._handle, sources_per_warp, sites_per_cell))
         grid.relax(0, neighbourhood=20)

@@ -146,7 +146,8 @@ const TileTable& tile_table() {
       int gid = -1;
       for (int c = 0; c < 11; ++c)
         if (std::strcmp(group, host_group_name(c)) == 0) gid = c;
-      if (k < 0 || gid < 0 || (g != 2 && g != 4 && g != 8) || !(spc >= 0.5 && spc <= 16)) continue;
+      if (k < 0 || gid < 0 || (g != 1 && g != 2 && g != 4 && g != 8) || !(spc >= 0.5 && spc <= 16)) continue;
+      if (g == 1 && k != kTilesSpacing) continue;  // one source per thread: spacing passes only
       table.entries[{k, gid, bucket}] = NearTiles{g, spc};
     }
     std::fclose(f);
@@ -179,6 +180,8 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   n_ = n;
   prec_ = prec;
   tiles_ = forced_ ? *forced_ : lookup_tiles(kind, gid_, n);
+  // One source per thread is a spacing-pass search only; relaxation passes keep the default.
+  if (tiles_.group_size == 1 && kind != kTilesSpacing) tiles_.group_size = kNearGroup;
   radius_ = std::min(1.5, delta_ * mean_r);
   s_margin_ = std::sin(radius_ + 1e-4);
   chord_ = 2.0 * std::sin(radius_ / 2.0);
@@ -941,7 +944,8 @@ void Engine::sync_neighbourhood() {
 }
 
 void Engine::force_tiles(std::optional<NearTiles> tiles) {
-  if (tiles && tiles->group_size != 2 && tiles->group_size != 4 && tiles->group_size != 8) throw Failure("InvalidTiles");
+  if (tiles && tiles->group_size != 1 && tiles->group_size != 2 && tiles->group_size != 4 && tiles->group_size != 8)
+    throw Failure("InvalidTiles");
   if (tiles && !(tiles->sites_per_cell >= 0.5 && tiles->sites_per_cell <= 16)) throw Failure("InvalidTiles");
   forced_tiles_ = tiles;
   for (RelaxState* st : {&relax_state_, &spacing_state_})

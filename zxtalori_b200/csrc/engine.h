@@ -116,8 +116,9 @@ struct RowBuffers {
   Rows rows() const { return Rows{force.as<double4>(), energy.as<double>(), nearest.as<double>(), nearest_at.as<int>()}; }
 };
 
-// Tile shape of the FP32 near-field gather: sources per warp (2, 4 or 8) and target shell
-// sites per chart cell.
+// Tile shape of the FP32 near-field gather: sources per warp (2, 4 or 8; for the spacing
+// pass also 1, one source per thread walking its own ball) and target shell sites per chart
+// cell.
 struct NearTiles {
   int group_size = kNearGroup;
   double sites_per_cell = kSitesPerCell;

@@ -931,6 +931,77 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const NearArgs A)
   near32_warp<G, TRACK, SHORT, NEAREST>(A, blockIdx.x * kNearWarps + w, blockIdx.y, tiles[w], walks[w], sums);
 }
 
+// The spacing pass's FP32 nearest-site search with one source per thread (tile shape 1):
+// each thread walks its own source's first ball, cell row by cell row, reading the sorted
+// sites straight from global memory - consecutive threads hold Hilbert-consecutive sources,
+// whose rows overlap, so the reads mostly hit in L1 - and keeps its two best chords. No
+// union of several sources' balls and no shared-memory staging: the work per site (one
+// squared chord) is too small to pay for either. The proof test, the exact-search list and
+// the rows written are those of k_near32's nearest-only variant (direct rows, one slice).
+__global__ void __launch_bounds__(256) k_nearest_lane(const NearArgs A) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= A.n) return;
+  const uint32_t i = A.src_perm[p];
+  const float4 x = A.q[i];
+  const NearGrid* __restrict__ gp = A.gp;
+  const float lower[3] = {gp->lower[0], gp->lower[1], gp->lower[2]};
+  const float per = gp->cells_per_unit;
+  const int sdim = gp->sdim;
+  const double kappa = 1.0 - 0.5 * A.cut.walk2;
+  const double den = 1.0 / ((double)x.x + kappa);
+  const float c[3] = {(float)(x.y * den), (float)(x.z * den), (float)(x.w * den)};
+  const float rho = (float)(sqrt(1.0 - kappa * kappa) * den) * 1.001f + 1e-6f;
+  int lo[3], hi[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = cell_axis(c[a] - rho, lower[a], per, sdim);
+    hi[a] = cell_axis(c[a] + rho, lower[a], per, sdim);
+  }
+  const float width = 1.0f / per;
+  const uint32_t* __restrict__ cell_off = A.cell_off;
+  const float4* __restrict__ sq = A.sq;
+  const uint32_t* __restrict__ scode = A.scode;
+  float best = 4.0f, second = 4.0f;
+  int best_at = -1;
+  for (int z = lo[2]; z <= hi[2]; ++z) {
+    const float cz = lower[2] + (float)z * width;
+    const float gz = fmaxf(0.f, fmaxf(cz - c[2], c[2] - (cz + width)));
+    for (int y = lo[1]; y <= hi[1]; ++y) {
+      const float cy = lower[1] + (float)y * width;
+      const float gy = fmaxf(0.f, fmaxf(cy - c[1], c[1] - (cy + width)));
+      const float rest = rho * rho - gy * gy - gz * gz;
+      if (rest < 0.f) continue;
+      const float span = sqrtf(rest);
+      const int row = sdim * (y + sdim * z);
+      const uint32_t end = __ldg(&cell_off[row + cell_axis(c[0] + span, lower[0], per, sdim) + 1]);
+      for (uint32_t t = __ldg(&cell_off[row + cell_axis(c[0] - span, lower[0], per, sdim)]); t < end; ++t) {
+        const float4 s = __ldg(&sq[t]);
+        const float mw = x.x - s.x, mx = x.y - s.y, my = x.z - s.z, mz = x.w - s.w;
+        float d = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
+        if (__ldg(&scode[t]) == (i | kIdentityBit)) d = 4.0f;  // the source itself
+        second = fminf(second, fmaxf(best, d));
+        if (d < best) {
+          best = d;
+          best_at = (int)t;
+        }
+      }
+    }
+  }
+  const double b = best, margin = 2.0 * chord_error32(b);
+  if ((double)second <= b + margin || b + margin > A.cut.walk2) {
+    const uint32_t slot = atomicAdd(A.exact_count, 1u);
+    A.exact_list[slot] = i;
+  }
+  if (best > (float)A.cut.cut2) {  // no site within the cutoff
+    best = 4.0f;
+    best_at = -1;
+  }
+  A.out.force[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+  A.out.energy[i] = 0.0;
+  A.out.nearest[i] = best;
+  A.out.nearest_at[i] = best_at;
+}
+
 // The exact nearest orbit neighbour of each source the FP32 spacing gather listed: every
 // site in the chart ball of the cutoff (the whole shell's reach, not the first walk's
 // smaller ball), its chord in FP64 from the float32 positions with the image formed in FP64
@@ -1447,7 +1518,13 @@ cudaError_t launch_near(const NearLaunch& L, cudaStream_t s) {
   } else {
     NearTask t = near_task(L);
     t.a.cut = cut;
-    if ((e = launch_near32(G, L.track, L.short_atan, nearest_only, grid, t.a, s))) return e;
+    if (nearest_only && G == 1) {
+      k_nearest_lane<<<(n + 255) / 256, 256, 0, s>>>(t.a);
+      e = cudaGetLastError();
+    } else {
+      e = launch_near32(G, L.track, L.short_atan, nearest_only, grid, t.a, s);
+    }
+    if (e) return e;
   }
   probe_mark(s);
   probe_count();

@@ -2,7 +2,8 @@
 
 For each group and size bucket (N from 2^b to 2^(b+1)), a Haar sample of the bucket's
 middle size is relaxed with every candidate tile shape - sources per warp (2, 4, 8) times
-target shell sites per chart cell (1.5, 2, 3) - and the device time of its BB steps is
+target shell sites per chart cell (1.5, 2, 3); the spacing pass also one source per
+thread - and the device time of its BB steps is
 taken with CUDA events (zo_bench: L2 flushed before each step). The fastest shape is
 written to the tile table, which every engine reads when it sizes a near-field workspace
 (zo_tiles_lookup shows its choice). Sizes whose cutoff takes the dense path (every image
@@ -28,6 +29,8 @@ from .api import GROUPS, haar
 
 ORDER = {"C2": 2, "C3": 3, "C4": 4, "C6": 6, "D2": 4, "D3": 6, "D4": 8, "D6": 12, "T": 12, "O": 24, "I": 60}
 SHAPES = [(g, spc) for g in (2, 4, 8) for spc in (1.5, 2.0, 3.0)]
+# The spacing pass may also search one source per thread (tile shape 1).
+SPACING_SHAPES = SHAPES + [(1, spc) for spc in (1.5, 2.0, 3.0)]
 DEFAULT_TABLE = Path(__file__).resolve().parent / "near_tiles.txt"
 FLUSH_BYTES = 256 << 20
 
@@ -91,7 +94,7 @@ def tune(groups=GROUPS, buckets=range(10, 19), spacing_groups=("I",), spacing_bu
             if n > 10_000_000 or n <= 20_000:
                 continue
             with haar(group, n, 2000 + b) as grid:
-                times = {shape: _spacing_ms(grid, shape, steps, warmup) for shape in SHAPES}
+                times = {shape: _spacing_ms(grid, shape, steps, warmup) for shape in SPACING_SHAPES}
             best = min(times, key=times.get)
             found[("spacing", group, b)] = (best, times)
             log(f"spacing {group} {b} n={n}: best {best} {times[best]:.3f} ms (default {times[(4, 2.0)]:.3f} ms)")
