@@ -206,3 +206,23 @@ def test_force_is_half_energy_gradient(engine, golden, precision, rtol):
             energy.append(qvm.pair_rows(moved, ops)["energy"].sum())
         derivative = (energy[0] - energy[1]) / (2 * h)
         assert abs(derivative + 2 * force[0, axis]) <= rtol * max(1.0, abs(derivative)), (axis, derivative, force[0])
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("group,source", [("O", "random"), ("I", "random"), ("T", "hopf"), ("O", "hopf")])
+def test_log_ratio_against_dense_fp64(engine, ops32, ops64, group, source, precision):
+    """tests/test_log_scale.py of the reference: the log ratio of about a thousand points
+    within 1e-5 (absolute) of the dense FP64 value, for random points and generated grids
+    (the reference also uses its FCC transports, which this engine does not build)."""
+    gid = GROUPS.index(group)
+    if source == "random":
+        q = np.random.default_rng(936).normal(size=(1000, 4))
+        grid = engine.from_quaternions(q / np.linalg.norm(q, axis=1, keepdims=True), group, precision=precision)
+    else:
+        grid = engine.generate(group, count=1000, precision=precision)
+    with grid:
+        actual = grid.measure()["log_ratio"]
+        q = grid.quaternions.astype(np.float64)
+    ops = ops32[group] if precision == "fp32" else ops64[group]
+    expected = qvm.full_measures(qvm.pair_rows(q, ops, full=True), len(ops))["log_ratio"]
+    assert abs(actual - expected) < 1e-5

@@ -111,3 +111,18 @@ def test_spacing_exact_search_beyond_first_ball(engine, ops32):
     q_in = q[far].astype(np.float32)
     report = _spacing_vs_oracle(engine, ops32, group, int(far.sum()), 0, q_in=q_in)
     assert report["exact_search"] >= 1
+
+
+def test_spacing_matches_all_pairs(engine):
+    """tests/test_measures.py:122-131 of the reference: above 20,000 orientations the spacing
+    pass (near field of 4 mean radii) gives the same per-point nearest angles as a measure
+    over all pairs (O 60k is above O's ratio limit, so measure() is an all-pairs quick pass)."""
+    with engine.haar("O", 60000, 3) as grid:
+        spacing = grid.spacing()
+        near = grid.point_values("separation").copy()
+        near_index = grid.point_neighbours().copy()
+        assert spacing["quey_energy"] is None and "energy not measured" in spacing["precision"]
+        grid.measure()
+        assert np.abs(near - grid.point_values("separation")).max() < 1e-5
+        assert abs(spacing["separation_deg"] - grid.stats["separation_deg"]) < 1e-5
+        assert np.array_equal(near_index, grid.point_neighbours())
