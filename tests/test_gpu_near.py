@@ -161,3 +161,40 @@ def test_tile_override_rejects_bad_shapes(engine):
         with pytest.raises(RuntimeError, match="InvalidTiles"):
             grid._check(grid._lib.zo_near_tiles(grid._handle, 4, 100.0))
         grid._check(grid._lib.zo_near_tiles(grid._handle, 0, 0.0))  # back to the table
+
+
+def test_sites_at_the_cutoff_along_the_chart_axes(engine, ops32):
+    """The walk trims each cell row's run to the balls' extent along chart x; sites just
+    inside the cutoff (at 1 - 1e-6 of it) in the six chart-axis directions of an isolated
+    source must all be found: its nearest chord and rows equal the dense oracle's."""
+    group, count = "O", 30000
+    ops = ops32[group]
+    base = qvm.fold(qvm.haar(2 * count, 19), 9, ops, f32=True).astype(np.float64)
+    r = qvm.near_radius(count, len(ops), 20)[0]  # the cutoff of the final sample of `count` points
+    # Clear the source's neighbourhood (every image within 1.2 r of the identity), then put
+    # the identity and six points at angle r (1 - 1e-6) from it, along +-x, +-y, +-z.
+    x = qvm.normalize(base)
+    keep = np.ones(len(x), bool)
+    for g in ops:
+        y = qvm.normalize(qvm.qmul(x, g))
+        keep &= np.minimum(np.linalg.norm(y - [1, 0, 0, 0], axis=1), np.linalg.norm(y + [1, 0, 0, 0], axis=1)) > \
+            2 * np.sin(0.6 * r)
+    theta = r * (1 - 1e-6)  # the S3 angle from (1, 0, 0, 0) to (cos t, sin t, 0, 0) is t
+    planted = [[1.0, 0, 0, 0]]
+    for axis in range(3):
+        for sign in (1.0, -1.0):
+            v = np.zeros(4)
+            v[0], v[1 + axis] = np.cos(theta), sign * np.sin(theta)
+            planted.append(v)
+    q = np.vstack([np.array(planted), x[keep][: count - len(planted)]]).astype(np.float32)
+    assert len(q) == count
+    with engine.from_quaternions(q, group) as grid:
+        grid.relax(0, neighbourhood=20)
+        rows = grid.debug_rows(0)
+        got = grid.quaternions.astype(np.float64)
+    dense = qvm.near_rows(got, ops, 20, sources=np.arange(7))
+    assert np.all(dense["nearest"] < dense["cut"])  # the planted sites are inside the cutoff
+    np.testing.assert_allclose(rows[:7, 5], dense["nearest"], rtol=5e-5)
+    # The isolated source's energy is a window remainder of about 1e-11 (its sites sit where
+    # the window vanishes); the planted sites' own rows are ordinary.
+    np.testing.assert_allclose(rows[1:7, 4], dense["energy"][1:], rtol=1e-5)

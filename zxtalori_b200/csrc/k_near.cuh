@@ -606,10 +606,13 @@ __device__ __forceinline__ bool walk_row(const NearWalk<G>& W, const uint32_t* c
   const int row = W.sdim * (y + W.sdim * z);
   start = cell_off[row + c0];
   end = cell_off[row + c1 + 1];
-  // Each cell's sites are sorted by chart x: drop those of the end cells outside [x0, x1].
+  // Each cell's sites are sorted by chart x: drop those of the end cells outside [x0, x1],
+  // widened by 2e-6 (chart coordinates are below 2 here, so that is many FP32 roundings of
+  // a site's x and of the span) on top of the balls' own 0.1% + 1e-6.
+  const float lo_x = x0 - 2e-6f, hi_x = x1 + 2e-6f;
   const uint32_t first_end = cell_off[row + c0 + 1], last_begin = cell_off[row + c1];
-  while (start < first_end && site_x[start] < x0) ++start;
-  while (end > last_begin && end > start && site_x[end - 1] > x1) --end;
+  while (start < first_end && site_x[start] < lo_x) ++start;
+  while (end > last_begin && end > start && site_x[end - 1] > hi_x) --end;
   return start < end;
 }
 
