@@ -553,14 +553,36 @@ struct NearShape {
 };
 
 // One tile. Slot u holds elements 2u and 2u + 1; lane (source s, sub-lane j) evaluates
-// slots j + sub m, m < slots.
+// slots j + sub m, m < slots. NORM: the arctangent form reads the sites' norms; AT: a pass
+// that tracks the nearest site reads their indices (the other variants keep one element of
+// each, to leave shared memory to the staging buffer).
+template <bool NORM, bool AT>
 struct NearTile {
-  float4 wx[kNearTile / 2];  // (w, w', x, x')
-  float4 yz[kNearTile / 2];  // (y, y', z, z')
-  float2 norm[kNearTile / 2];  // (2|y|^2, 2|y'|^2), for the arctangent form only
-  uint2 code[kNearTile / 2];   // (code, code')
-  uint32_t at[kNearTile];      // sorted-site index of each element
+  float4 wx[kNearTile / 2];              // (w, w', x, x')
+  float4 yz[kNearTile / 2];              // (y, y', z, z')
+  float2 norm[NORM ? kNearTile / 2 : 1];  // (2|y|^2, 2|y'|^2)
+  uint2 code[kNearTile / 2];             // (code, code')
+  uint32_t at[AT ? kNearTile : 1];       // sorted-site index of each element
 };
+// The next tile's sites and codes as they arrive from global memory (cp.async), in element
+// order; each lane stages and later packs only its own elements.
+struct NearStage {
+  float4 q[kNearTile];
+  uint32_t code[kNearTile];
+};
+
+// Asynchronous global-to-shared copies (cp.async): 16 bytes (cached in L2 only) or 4 bytes,
+// committed as one group per tile and awaited before the tile is packed.
+__device__ __forceinline__ void copy_async16(void* shared, const void* global) {
+  const unsigned to = (unsigned)__cvta_generic_to_shared(shared);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(to), "l"(global) : "memory");
+}
+__device__ __forceinline__ void copy_async4(void* shared, const void* global) {
+  const unsigned to = (unsigned)__cvta_generic_to_shared(shared);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(to), "l"(global) : "memory");
+}
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Per-warp data of the row walk, kept in shared memory (it is warp-uniform) so the hot
 // loop's registers go to the pair arithmetic. Stereographic projection maps spheres to
@@ -636,8 +658,8 @@ __device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], floa
 // its identity image is no neighbour); without it that test is left out. SHORT: cutoffs up
 // to 0.4 rad take the chord form (near_chord_pair32x2), wider ones the arctangent of near
 // over far. se sums energy / pi. NEAREST: only the nearest site is tracked.
-template <int G, bool TRACK, bool SHORT, bool OWN, bool NEAREST>
-__device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub, uint32_t i, float2 xw, float2 xx,
+template <int G, bool TRACK, bool SHORT, bool OWN, bool NEAREST, class Tile>
+__device__ __forceinline__ void near_slots(const Tile& T, int count, int sub, uint32_t i, float2 xw, float2 xx,
                                            float2 xy, float2 xz, float2 xn, float cut_hi, float cw, float czw,
                                            float pk, float2& sw, float2& sx, float2& sy, float2& sz, float2& sc,
                                            float2& se, float& best, int& best_at, float& second) {
@@ -717,9 +739,12 @@ __device__ __forceinline__ void near_slots(const NearTile& T, int count, int sub
 
 // One warp task of the gather: warp `warp` (G sources along the Hilbert order) and slice
 // `slice` of the sample in A; T, W and sums are the warp's shared memory.
+template <bool TRACK, bool SHORT, bool NEAREST>
+using NearTileOf = NearTile<!SHORT && !NEAREST, TRACK>;
+
 template <int G, bool TRACK, bool SHORT, bool NEAREST>
-__device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int slice, NearTile& T, NearWalk<G>& W,
-                                            double (*sums)[kNearWarps * 32]) {
+__device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int slice, NearTileOf<TRACK, SHORT, NEAREST>& T,
+                                            NearStage& S, NearWalk<G>& W, double (*sums)[kNearWarps * 32]) {
   constexpr int kSub = NearShape<G>::sub;
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -808,16 +833,13 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
     const uint32_t total = __shfl_sync(full, incl, 31);
     const uint32_t shift = start - (incl - len);  // element e of run k is site shift_k + e
     int k = 0;  // the run of this lane's next element: the first lane with incl > e
-    for (uint32_t tb = 0; tb < total; tb += kNearTile) {
+    // Stages tile tb: lane l copies elements 64h + 2l and 64h + 2l + 1 (h = 0, 1), those
+    // before the batch's end, into the staging buffer, and keeps their site indices.
+    uint32_t staged[4];
+    auto stage = [&](uint32_t tb) {
       const int count = (int)min((uint32_t)kNearTile, total - tb);
-      bool mine = false;  // this lane loaded an image of one of the warp's sources
-      __syncwarp();
 #pragma unroll
       for (int h = 0; h < kNearTile / 64; ++h) {
-        // Lane l loads elements 64h + 2l and 64h + 2l + 1 (slot 32h + l) and writes the slot
-        // whole. An element past the batch's end is a blank site: at the origin,
-        // dm2 = |x|^2 ~ 1 lies beyond every cutoff of the chart-grid path (r < 0.9 rad,
-        // cut2 < 0.76), and its code matches no source.
         const int el = 64 * h + 2 * lane;
         const uint32_t e = tb + el;
         uint32_t kin;
@@ -830,9 +852,30 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
         }
         // Element e + 1 is in run k, or starts run k + 1 (runs are nonempty).
         const int k1 = (e + 1 >= kin && k < 31) ? k + 1 : k;
-        uint32_t site[2];
-        site[0] = __shfl_sync(full, shift, k) + e;
-        site[1] = __shfl_sync(full, shift, k1) + e + 1;
+        staged[2 * h] = __shfl_sync(full, shift, k) + e;
+        staged[2 * h + 1] = __shfl_sync(full, shift, k1) + e + 1;
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+          if (el + b < count) {
+            copy_async16(&S.q[el + b], &sq[staged[2 * h + b]]);
+            copy_async4(&S.code[el + b], &scode[staged[2 * h + b]]);
+          }
+      }
+      copy_async_commit();
+    };
+    if (total > 0) stage(0);
+    for (uint32_t tb = 0; tb < total; tb += kNearTile) {
+      const int count = (int)min((uint32_t)kNearTile, total - tb);
+      bool mine = false;  // this lane loaded an image of one of the warp's sources
+      copy_async_wait();
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < kNearTile / 64; ++h) {
+        // Lane l packs its elements 64h + 2l and 64h + 2l + 1 into slot 32h + l, whole. An
+        // element past the batch's end is a blank site: at the origin, dm2 = |x|^2 ~ 1 lies
+        // beyond every cutoff of the chart-grid path (r < 0.9 rad, cut2 < 0.76), and its code
+        // matches no source.
+        const int el = 64 * h + 2 * lane;
         float4 y[2];
         uint32_t code[2];
 #pragma unroll
@@ -840,8 +883,8 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
           y[b] = make_float4(0.f, 0.f, 0.f, 0.f);
           code[b] = 0xffffffffu;
           if (el + b < count) {
-            y[b] = sq[site[b]];
-            code[b] = scode[site[b]];
+            y[b] = S.q[el + b];
+            code[b] = S.code[el + b];
           }
         }
         const int slot = 32 * h + lane;
@@ -851,7 +894,7 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
         if (!SHORT && !NEAREST)
           T.norm[slot] = make_float2(2.0f * fmaf(y[0].x, y[0].x, fmaf(y[0].y, y[0].y, fmaf(y[0].z, y[0].z, y[0].w * y[0].w))),
                                      2.0f * fmaf(y[1].x, y[1].x, fmaf(y[1].y, y[1].y, fmaf(y[1].z, y[1].z, y[1].w * y[1].w))));
-        if (TRACK) reinterpret_cast<uint2*>(T.at)[slot] = make_uint2(site[0], site[1]);
+        if (TRACK) reinterpret_cast<uint2*>(T.at)[slot] = make_uint2(staged[2 * h], staged[2 * h + 1]);
 #pragma unroll
         for (int s2 = 0; s2 < G; ++s2)
           mine |= ((code[0] & ~kIdentityBit) == W.src[s2]) | ((code[1] & ~kIdentityBit) == W.src[s2]);
@@ -860,6 +903,8 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
       // the slot loop test each site's source.
       const bool tile_own = __any_sync(full, mine);
       __syncwarp();
+      // The staging buffer is free again: the next tile's copies run under this one's pairs.
+      if (tb + kNearTile < total) stage(tb + kNearTile);
       if (live) {
         if (tile_own)
           near_slots<G, TRACK, SHORT, true, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
@@ -927,11 +972,13 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
 
 template <int G, bool TRACK, bool SHORT, bool NEAREST>
 __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const NearArgs A) {
-  __shared__ NearTile tiles[kNearWarps];
+  __shared__ NearTileOf<TRACK, SHORT, NEAREST> tiles[kNearWarps];
+  __shared__ NearStage stages[kNearWarps];
   __shared__ NearWalk<G> walks[kNearWarps];
   __shared__ double sums[6][kNearWarps * 32];  // FP64 lane sums: force differences, curvature, energy
   const int w = threadIdx.x >> 5;
-  near32_warp<G, TRACK, SHORT, NEAREST>(A, blockIdx.x * kNearWarps + w, blockIdx.y, tiles[w], walks[w], sums);
+  near32_warp<G, TRACK, SHORT, NEAREST>(A, blockIdx.x * kNearWarps + w, blockIdx.y, tiles[w], stages[w], walks[w],
+                                        sums);
 }
 
 // The spacing pass's FP32 nearest-site search with one source per thread (tile shape 1):
@@ -1554,7 +1601,8 @@ template <int G, bool SHORT>
 __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32_batch(const NearTask* __restrict__ tasks,
                                                                     const uint32_t* __restrict__ prefix, int count,
                                                                     uint32_t total, uint32_t* __restrict__ counter) {
-  __shared__ NearTile tiles[kNearWarps];
+  __shared__ NearTileOf<false, SHORT, false> tiles[kNearWarps];
+  __shared__ NearStage stages[kNearWarps];
   __shared__ NearWalk<G> walks[kNearWarps];
   __shared__ double sums[6][kNearWarps * 32];
   __shared__ NearTask mine[kNearWarps];  // the warp's current task, copied in by its lanes
@@ -1579,8 +1627,8 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32_batch(const NearT
     __syncwarp();
     const uint32_t local = t - prefix[lo];
     const uint32_t warps = (uint32_t)mine[w].warps;
-    near32_warp<G, false, SHORT, false>(mine[w].a, (int)(local % warps), (int)(local / warps), tiles[w], walks[w],
-                                        sums);
+    near32_warp<G, false, SHORT, false>(mine[w].a, (int)(local % warps), (int)(local / warps), tiles[w], stages[w],
+                                        walks[w], sums);
     __syncwarp();
   }
 }
