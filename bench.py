@@ -292,7 +292,7 @@ def batched_section(zo, samples=256, steps=50, dist=None):
         dt, setup = dist.reduce(dt, "max"), dist.reduce(setup, "max")
         evals, sum_n = dist.reduce(evals, "sum"), int(dist.reduce(sum_n, "sum"))
     lib = zo.api._library()
-    out = (C.c_double * 2)()
+    out = (C.c_double * 3)()
     shapes = {}
     for sp in specs:
         lib.zo_tiles_lookup(0, zo.GROUPS.index(sp.group), sp.count, out)

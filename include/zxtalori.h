@@ -106,10 +106,15 @@ const int32_t* zo_point_neighbours(void* h);
  * returns to the table.
  * The reference's tiling knobs are constants (src/pairs.zig:100-128, src/near.zig:22-29). */
 int zo_near_tiles(void* h, uint32_t sources_per_warp, float sites_per_cell);
+/* Tuning extension: the fraction of the spacing pass's cutoff (4 mean radii) that its first
+ * FP32 walk covers, instead of the tile table's choice (0 returns to the table); 0.3..1.
+ * Sources whose nearest neighbour the first walk cannot prove are searched again over the
+ * whole cutoff in FP64, so the spacing results do not depend on it, only the pass's time. */
+int zo_near_walk(void* h, float fraction);
 /* The tile table's choice for a pass kind (0 relaxation, 1 spacing), group and sample size:
- * out[0] sources per warp, out[1] sites per chart cell. The table (near_tiles.txt beside the
- * library's folder, or $ZXTALORI_TILES) is read once per process. Needs no GPU; -1 on a bad
- * argument. */
+ * out[0] sources per warp, out[1] sites per chart cell, out[2] the spacing pass's first-walk
+ * fraction (out must hold 3). The table (near_tiles.txt beside the library's folder, or
+ * $ZXTALORI_TILES) is read once per process. Needs no GPU; -1 on a bad argument. */
 int zo_tiles_lookup(uint32_t kind, uint32_t group, uint32_t n, double* out);
 /* Extension, no reference counterpart: the device memory the engine holds now, in bytes
  * (positions, rows, BB history, near-field workspace, measure scratch; all of it from the
@@ -174,6 +179,14 @@ double zo_fp32x2_peak(void* h);
  * the row count, -1 for an unknown group, a frequency outside 1..512 or a grid above ten
  * million rows, -2 when capacity is too small. Needs no GPU. */
 int64_t zo_hopf_points(uint32_t group, uint32_t freq, float* out, uint64_t capacity);
+/* Diagnostic extension: the group's 2|K|-1 zone bisector planes in the order the shell's rim
+ * test takes them (order[r], group-local plane index as in the reference's plane list,
+ * src/covering.zig:382-396) with each one's reach (reach[r]: a lower bound, less 1e-5, on the
+ * plane's dot product with any point of the zone, from the zone's vertices; -1 for planes
+ * that touch the zone and for groups whose zone has no vertices). The rim test of a source
+ * stops at the first plane whose reach exceeds the shell margin. Each array holds 119 at
+ * most. Returns the plane count, -1 for an unknown group. Needs no GPU. */
+int zo_zone_planes(uint32_t group, uint8_t* order, float* reach);
 
 /* No counterpart in the reference. The all-pairs force pass (FP32 pair arithmetic, FP64
  * sums) for callers that cannot allocate device memory: a framework that owns every

@@ -150,7 +150,7 @@ def test_near_relax_fp32_vs_fp64(engine, ops32):
 
 
 @pytest.mark.parametrize("sources_per_warp,sites_per_cell",
-                         [(2, 1.5), (2, 3.0), (8, 1.5), (8, 3.0), (4, 2.0), (1, 2.0), (1, 3.0)])
+                         [(2, 1.5), (2, 3.0), (8, 1.0), (8, 3.0), (4, 1.25), (4, 2.0), (1, 1.0), (1, 3.0)])
 def test_every_tile_shape_matches_the_oracle(engine, ops32, sources_per_warp, sites_per_cell):
     """Each tile shape the tuner may choose (zo_near_tiles) gives the oracle's rows (near
     field, O 30k) and the oracle's spacing indices (I 40k). Shape 1 (one source per thread)

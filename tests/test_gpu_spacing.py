@@ -126,3 +126,37 @@ def test_spacing_matches_all_pairs(engine):
         assert np.abs(near - grid.point_values("separation")).max() < 1e-5
         assert abs(spacing["separation_deg"] - grid.stats["separation_deg"]) < 1e-5
         assert np.array_equal(near_index, grid.point_neighbours())
+
+
+def test_spacing_walk_fraction_changes_no_result(engine, ops32):
+    """The first walk's fraction of the cutoff (zo_near_walk, picked per size by the tuner)
+    moves sources between the FP32 walk and the exact FP64 search, never a result: indices
+    and degrees are the same bit for bit for every fraction and tile shape, and equal the FP64
+    oracle's. A shorter walk leaves more sources to the exact search."""
+    group, count, seed = "I", 200_000, 7
+    runs = {}
+    with engine.haar(group, count, seed) as grid:
+        lib, h = grid._lib, grid._handle
+        for shape in ((1, 1.5), (4, 2.0)):
+            grid._check(lib.zo_near_tiles(h, *shape))
+            for walk in (0.3, 0.45, 0.625, 1.0):
+                grid._check(lib.zo_near_walk(h, walk))
+                grid.spacing()
+                runs[shape, walk] = (grid.point_neighbours().copy(), grid.point_values("separation").copy(),
+                                     grid.spacing_exact()["exact_search"])
+        for bad in (0.1, 1.5, -1.0):
+            with pytest.raises(RuntimeError, match="InvalidWalk"):
+                grid._check(lib.zo_near_walk(h, bad))
+        grid._check(lib.zo_near_walk(h, 0.0))
+        grid._check(lib.zo_near_tiles(h, 0, 0.0))
+        q = grid.quaternions.astype(np.float64)
+    first = runs[(1, 1.5), 0.625]
+    for key, (neighbours, degrees, _) in runs.items():
+        assert np.array_equal(neighbours, first[0]), key
+        assert np.array_equal(degrees, first[1]), key
+    for shape in ((1, 1.5), (4, 2.0)):
+        listed = [runs[shape, w][2] for w in (0.3, 0.45, 0.625, 1.0)]
+        assert listed == sorted(listed, reverse=True) and listed[0] > listed[-1], (shape, listed)
+    rows = cref.near_rows(q, ops32[group], 4)
+    assert np.array_equal(first[0], rows["nearest_source"])
+    np.testing.assert_allclose(first[1], qvm.nearest_degrees(rows), rtol=1e-6)

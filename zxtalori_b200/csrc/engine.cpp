@@ -21,10 +21,6 @@ constexpr uint32_t kMaxCount = 10000000;          // hopf.max_count (src/hopf.zi
 constexpr double kFullMeasurePairs = 5e10;        // src/engine.zig:1123
 constexpr uint32_t kSpacingAllPairs = 20000;      // src/engine.zig:1126
 constexpr double kSpacingDelta = 4;               // src/engine.zig:1127
-// The spacing pass's first walk covers 2.5 of the 4 mean radii (about 15 neighbours
-// expected, against about 60): nearly every source's nearest lies within it, and the
-// few that do not are searched again over the whole cutoff.
-constexpr double kSpacingWalk = 2.5 / 4.0;
 // Near field over every image ("dense") or over the chart grid. FP64 mode: dense from a
 // 0.5 rad cutoff on. FP32 mode (the gather walks exact chart balls): dense from 0.9 rad on,
 // or from 0.5 rad for samples of at most 1e8 image pairs, where the grid's fixed cost and
@@ -140,15 +136,17 @@ const TileTable& tile_table() {
     while (std::fgets(line, sizeof line, f)) {
       char kind[32], group[8];
       int bucket = 0, g = 0;
-      double spc = 0;
-      if (line[0] == '#' || std::sscanf(line, "%31s %7s %d %d %lf", kind, group, &bucket, &g, &spc) != 5) continue;
+      double spc = 0, walk = kSpacingWalk;
+      const int fields = line[0] == '#' ? 0 : std::sscanf(line, "%31s %7s %d %d %lf %lf", kind, group, &bucket, &g, &spc, &walk);
+      if (fields < 5) continue;
       const int k = std::strcmp(kind, "spacing") == 0 ? kTilesSpacing : std::strcmp(kind, "relax") == 0 ? kTilesRelax : -1;
       int gid = -1;
       for (int c = 0; c < 11; ++c)
         if (std::strcmp(group, host_group_name(c)) == 0) gid = c;
       if (k < 0 || gid < 0 || (g != 1 && g != 2 && g != 4 && g != 8) || !(spc >= 0.5 && spc <= 16)) continue;
       if (g == 1 && k != kTilesSpacing) continue;  // one source per thread: spacing passes only
-      table.entries[{k, gid, bucket}] = NearTiles{g, spc};
+      if (fields == 6 && !(walk >= kMinSpacingWalk && walk <= 1.0)) continue;
+      table.entries[{k, gid, bucket}] = NearTiles{g, spc, k == kTilesSpacing ? walk : kSpacingWalk};
     }
     std::fclose(f);
   });
@@ -241,6 +239,7 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   mcount_.ensure(mcells * 4);
   moff_.ensure(mcells * 4);
   src_perm_.ensure((size_t)n * 4);
+  if (kind == kTilesSpacing && prec != kFP64) self_site_.ensure((size_t)n * 4);
   grid_.ensure(sizeof(NearGrid));
   cells_.ensure(sizeof(int));
   exact_list_.ensure((size_t)n * 4);
@@ -277,7 +276,7 @@ NearLaunch NearField::make_launch(int prec, const float4* q32, const double4* q6
   L.track = track;
   L.short_atan = radius_ <= 0.4;
   L.nearest_only = nearest_only && track;
-  const double walk = 2.0 * std::sin(0.5 * kSpacingWalk * radius_);
+  const double walk = 2.0 * std::sin(0.5 * (walk_override_ > 0 ? walk_override_ : tiles_.walk) * radius_);
   L.walk_cut2 = walk * walk;
   L.exact_list = exact_list_.as<uint32_t>();
   L.exact_count = exact_count_.as<uint32_t>();
@@ -309,6 +308,7 @@ NearLaunch NearField::make_launch(int prec, const float4* q32, const double4* q6
   L.sq64 = prec == kFP64 ? sq_.as<double4>() : nullptr;
   L.scode = scode_.as<uint32_t>();
   L.sx = sx_.as<float>();
+  L.self_site = L.nearest_only && L.group_size == 1 && prec != kFP64 ? self_site_.as<uint32_t>() : nullptr;
   L.simg = simg_.as<uint32_t>();
   L.src_key = src_key_.as<uint32_t>();
   L.src_rank = src_rank_.as<uint32_t>();
@@ -367,7 +367,7 @@ size_t NearField::bytes() const {
   const DeviceBuffer* all[] = {&counts_,    &offsets_,  &scan_tmp_, &shell_mask_, &rim_list_,  &rim_q_,
                                &rim_count_, &site_q_,   &site_code_, &site_img_,  &site_cell_, &site_rank_,
                                &site_pos_,  &cell_count_, &cell_off_, &perm_,     &sq_,        &scode_,
-                               &simg_,      &sx_,       &src_key_,  &src_rank_,  &mcount_,    &moff_,
+                               &simg_,      &sx_,       &self_site_, &src_key_, &src_rank_,  &mcount_,    &moff_,
                                &src_perm_,  &grid_,     &cells_,    &exact_list_, &exact_count_};
   size_t total = partial_.bytes();
   for (const DeviceBuffer* b : all) total += b->bytes();
@@ -952,9 +952,16 @@ void Engine::force_tiles(std::optional<NearTiles> tiles) {
     if (NearField* nf = st->near_field()) nf->force_tiles(tiles);
 }
 
+void Engine::force_walk(double fraction) {
+  if (fraction != 0 && !(fraction >= kMinSpacingWalk && fraction <= 1.0)) throw Failure("InvalidWalk");
+  forced_walk_ = fraction;
+  if (NearField* nf = spacing_state_.near_field()) nf->force_walk(fraction);
+}
+
 void Engine::apply_overrides(RelaxState& state) {
   NearField* nf = state.near_field();
   if (nf) nf->force_tiles(forced_tiles_);
+  if (nf && &state == &spacing_state_) nf->force_walk(forced_walk_);
   if (!shell_override_ || !nf) return;
   nf->override_capacity(shell_override_);
   shell_override_ = 0;

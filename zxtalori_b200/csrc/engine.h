@@ -122,14 +122,19 @@ struct RowBuffers {
 struct NearTiles {
   int group_size = kNearGroup;
   double sites_per_cell = kSitesPerCell;
+  double walk = kSpacingWalk;  // spacing passes: the first walk's fraction of the cutoff
 };
+// The smallest first-walk fraction accepted (below it most sources would need the exact
+// search).
+constexpr double kMinSpacingWalk = 0.3;
 // Which near-field pass a tile choice is for.
 enum TileKind : int { kTilesRelax = 0, kTilesSpacing = 1 };
 // The tile table's choice for a group and sample size: the entry of (kind, group,
 // floor(log2 n)), else the group's entry of the nearest size bucket, else the defaults. The
 // table is read once per process from $ZXTALORI_TILES, or near_tiles.txt in the package
 // directory beside the library's _lib folder; lines "kind group bucket sources_per_warp
-// sites_per_cell" (kind relax|spacing, group by name), '#' comments.
+// sites_per_cell [walk]" (kind relax|spacing, group by name; walk, for spacing lines, the
+// first walk's fraction of the cutoff), '#' comments.
 NearTiles lookup_tiles(int kind, int gid, int n);
 
 // Near-field workspace (src/near.zig:31-196): sized by one shell pass, then reused.
@@ -190,6 +195,9 @@ class NearField {
     forced_ = tiles;
     ready_ = false;
   }
+  // The spacing pass's first-walk fraction to use instead of the tile choice's (0: none); it
+  // changes no workspace, only the next launches.
+  void force_walk(double fraction) { walk_override_ = fraction; }
   const NearTiles& tiles() const { return tiles_; }
   void reconfigure(int gid, double delta) {
     gid_ = gid;
@@ -210,13 +218,15 @@ class NearField {
   double taper_ = 0.5;
   NearTiles tiles_;
   std::optional<NearTiles> forced_;
+  double walk_override_ = 0;
   bool ready_ = false;
   int n_ = 0, prec_ = -1, capacity_ = 0, sdim_max_ = 1, slices_ = 1, slices32_ = 1;
   uint32_t next_capacity_ = 0;
   double radius_ = 0, s_margin_ = 0, chord_ = 0;
   DeviceBuffer counts_, offsets_, scan_tmp_, shell_mask_, rim_list_, rim_q_, rim_count_;
   DeviceBuffer site_q_, site_code_, site_img_, site_cell_, site_rank_, site_pos_;
-  DeviceBuffer cell_count_, cell_off_, perm_, sq_, scode_, simg_, sx_, src_key_, src_rank_, mcount_, moff_, src_perm_;
+  DeviceBuffer cell_count_, cell_off_, perm_, sq_, scode_, simg_, sx_, self_site_, src_key_, src_rank_, mcount_, moff_,
+      src_perm_;
   DeviceBuffer grid_, cells_;
   DeviceBuffer exact_list_, exact_count_;
   RowBuffers partial_;
@@ -347,6 +357,9 @@ class Engine {
   // Development: the next near-field pass (of the relaxation and of the spacing pass) sizes
   // its workspace for only `sites` shell sites, once; 0 cancels.
   void debug_shell_capacity(uint32_t sites) { shell_override_ = sites; }
+  // The spacing pass's first-walk fraction of the cutoff, instead of the tile table's (0:
+  // the table's); the result does not depend on it, only the time.
+  void force_walk(double fraction);
   // Development: one pass's raw rows to host. what 0: force pass of the relaxation
   // (8 doubles per source), 1: full measure rows (12 doubles per source).
   void debug_rows(uint32_t what, double* out);
@@ -409,6 +422,7 @@ class Engine {
   void apply_overrides(RelaxState& state);
   uint32_t shell_override_ = 0;
   std::optional<NearTiles> forced_tiles_;
+  double forced_walk_ = 0;
   void fetch();
   Measures full_measure();
   Measures relax_state_measure();

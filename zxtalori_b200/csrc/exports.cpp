@@ -157,11 +157,16 @@ int zo_near_tiles(void* h, uint32_t sources_per_warp, float sites_per_cell) {
   });
 }
 
+int zo_near_walk(void* h, float fraction) {
+  return guarded(h, "Tiles", [&](Engine& e) { e.force_walk((double)fraction); });
+}
+
 int zo_tiles_lookup(uint32_t kind, uint32_t group, uint32_t n, double* out) {
   if (group >= 11 || kind > 1 || !out) return -1;
   const zo::NearTiles t = zo::lookup_tiles((int)kind, (int)group, (int)n);
   out[0] = t.group_size;
   out[1] = t.sites_per_cell;
+  out[2] = t.walk;
   return 0;
 }
 
@@ -215,6 +220,17 @@ int64_t zo_hopf_points(uint32_t group, uint32_t freq, float* out, uint64_t capac
   } catch (const std::exception&) {
     return -1;
   }
+}
+
+int zo_zone_planes(uint32_t group, uint8_t* order, float* reach) {
+  if (group >= 11 || !order || !reach) return -1;
+  const zo::HostTables& t = zo::host_tables();
+  const int off = t.plane_offset[group], planes = 2 * t.group_order[group] - 1;
+  for (int r = 0; r < planes; ++r) {
+    order[r] = t.plane_order[off + r];
+    reach[r] = t.plane_reach[off + r];
+  }
+  return planes;
 }
 
 double zo_fp32_peak(void* h) {

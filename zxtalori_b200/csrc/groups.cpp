@@ -1,5 +1,9 @@
 // Host copies of the group tables and the zone bisector planes.
+#include <algorithm>
+#include <array>
 #include <cmath>
+#include <numeric>
+#include <vector>
 
 #include "kernels.h"
 
@@ -26,6 +30,49 @@ void planes_of(const double (*ops)[4], int order, Out out) {
   }
 }
 
+// Reach of each plane over the zone {x unit: h_k . x >= 0 for all k}. When the planes span
+// R^4 the zone is the spherical hull of its vertices (the unit points where three planes
+// meet and every half-space holds), and for any zone point x = sum l_i v_i / |sum l_i v_i|
+// (l_i >= 0) and a plane whose dot products with all vertices are >= 0,
+// h . x >= sum l_i (h . v_i) / sum l_i >= min_i h . v_i, by the triangle inequality. So
+// min over the vertices bounds the plane's dot product below over the whole zone; the 1e-5
+// taken off covers float32 planes and sources that the fold leaves within rounding of the
+// zone.
+void plane_reach(const double (*h)[4], int planes, float* reach) {
+  std::vector<std::array<double, 4>> vertices;
+  for (int a = 0; a < planes; ++a)
+    for (int b = a + 1; b < planes; ++b)
+      for (int c = b + 1; c < planes; ++c) {
+        // The line orthogonal to three normals: cofactors of the 3x4 matrix.
+        const double* r[3] = {h[a], h[b], h[c]};
+        auto minor = [&](int skip) {
+          int col[3], n = 0;
+          for (int i = 0; i < 4; ++i)
+            if (i != skip) col[n++] = i;
+          return r[0][col[0]] * (r[1][col[1]] * r[2][col[2]] - r[1][col[2]] * r[2][col[1]]) -
+                 r[0][col[1]] * (r[1][col[0]] * r[2][col[2]] - r[1][col[2]] * r[2][col[0]]) +
+                 r[0][col[2]] * (r[1][col[0]] * r[2][col[1]] - r[1][col[1]] * r[2][col[0]]);
+        };
+        std::array<double, 4> v = {minor(0), -minor(1), minor(2), -minor(3)};
+        const double len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3]);
+        if (len < 1e-9) continue;
+        for (double sign : {1.0, -1.0}) {
+          std::array<double, 4> u;
+          for (int i = 0; i < 4; ++i) u[i] = sign * v[i] / len;
+          bool inside = true;
+          for (int k = 0; k < planes && inside; ++k)
+            inside = h[k][0] * u[0] + h[k][1] * u[1] + h[k][2] * u[2] + h[k][3] * u[3] >= -1e-9;
+          if (inside) vertices.push_back(u);
+        }
+      }
+  for (int k = 0; k < planes; ++k) {
+    double least = vertices.empty() ? -1.0 : 2.0;
+    for (const auto& u : vertices)
+      least = std::min(least, h[k][0] * u[0] + h[k][1] * u[1] + h[k][2] * u[2] + h[k][3] * u[3]);
+    reach[k] = least <= 1e-9 ? -1.0f : (float)(least - 1e-5);
+  }
+}
+
 HostTables build() {
   HostTables t{};
   int plane = 0;
@@ -47,7 +94,17 @@ HostTables build() {
     planes_of(f32ops, order, [&](int r, const double* v) {
       for (int c = 0; c < 4; ++c) t.planes32[plane + r][c] = (float)v[c];
     });
-    plane += 2 * order - 1;
+    const int planes = 2 * order - 1;
+    float reach[kMaxPlaneRows];
+    plane_reach(&t.planes64[plane], planes, reach);
+    std::vector<int> sorted(planes);
+    std::iota(sorted.begin(), sorted.end(), 0);
+    std::stable_sort(sorted.begin(), sorted.end(), [&](int x, int y) { return reach[x] < reach[y]; });
+    for (int r = 0; r < planes; ++r) {
+      t.plane_order[plane + r] = (uint8_t)sorted[r];
+      t.plane_reach[plane + r] = reach[sorted[r]];
+    }
+    plane += planes;
   }
   return t;
 }

@@ -34,8 +34,13 @@ __device__ __forceinline__ bool inside_planes(double4 q, int poff, int planes, b
   }
   return true;
 }
+// Whether a zone source lies within `margin` of some bisector plane. The planes are taken in
+// order of reach and the test stops at the first that reaches no zone point within the
+// margin: every later one reaches none either.
 __device__ __forceinline__ bool on_rim(double4 orig, int poff, int planes, bool fp64, double margin) {
-  for (int k = 0; k < planes; ++k) {
+  for (int r = 0; r < planes; ++r) {
+    if ((double)c_plane_reach[poff + r] > margin) break;
+    const int k = c_plane_order[poff + r];
     const double4 h = fp64 ? c_planes64[poff + k] : to_d4(c_planes32[poff + k]);
     if (dot4(orig, h) <= margin) return true;
   }
@@ -106,8 +111,11 @@ __global__ void __launch_bounds__(256) k_shell_rim32(const float4* __restrict__ 
   if (j < n) {
     const int poff = c_plane_offset[gid], planes = 2 * c_group_order[gid] - 1;
     orig = q32[j];  // unit to 1e-7 (folded in FP64), far inside the margin's slack
-    for (int k = 0; k < planes && !rim; ++k) {
-      const float4 h = c_planes32[poff + k];
+    // Planes in order of reach, up to the first that no zone point comes within the margin
+    // of (for I at small cutoffs, the 12 faces of the zone instead of 119 planes).
+    for (int r = 0; r < planes && !rim; ++r) {
+      if (c_plane_reach[poff + r] > margin) break;
+      const float4 h = c_planes32[poff + c_plane_order[poff + r]];
       rim = fmaf(orig.x, h.x, fmaf(orig.y, h.y, fmaf(orig.z, h.z, orig.w * h.w))) <= margin;
     }
     masks[j] = make_uint4(1u, 0u, 0u, 0u);  // the identity image is always a (core) site
@@ -383,15 +391,18 @@ __global__ void k_site_gather(const uint32_t* __restrict__ perm, const NearGrid*
                               const float4* __restrict__ q32, const double4* __restrict__ q64,
                               const uint32_t* __restrict__ code, const uint32_t* __restrict__ img,
                               const float4* __restrict__ pos, float4* __restrict__ sq32, double4* __restrict__ sq64,
-                              uint32_t* __restrict__ scode, uint32_t* __restrict__ simg, float* __restrict__ sx) {
+                              uint32_t* __restrict__ scode, uint32_t* __restrict__ simg, float* __restrict__ sx,
+                              uint32_t* __restrict__ self_site) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= gp->sites) return;
   const uint32_t s = perm[p];
   if (FP64) sq64[p] = q64[s];
   else sq32[p] = q32[s];
-  scode[p] = code[s];
+  const uint32_t c = code[s];
+  scode[p] = c;
   simg[p] = img[s];
   sx[p] = pos[s].x;
+  if (self_site && (c & kIdentityBit)) self_site[c & ~kIdentityBit] = (uint32_t)p;  // one identity site per source
 }
 
 // ------------------------------------------------------------------ 3. sources in Hilbert order
@@ -555,7 +566,7 @@ struct NearShape {
 // One tile. Slot u holds elements 2u and 2u + 1; lane (source s, sub-lane j) evaluates
 // slots j + sub m, m < slots. NORM: the arctangent form reads the sites' norms; AT: a pass
 // that tracks the nearest site reads their indices (the other variants keep one element of
-// each, to leave shared memory to the staging buffer).
+// each).
 template <bool NORM, bool AT>
 struct NearTile {
   float4 wx[kNearTile / 2];              // (w, w', x, x')
@@ -564,26 +575,6 @@ struct NearTile {
   uint2 code[kNearTile / 2];             // (code, code')
   uint32_t at[AT ? kNearTile : 1];       // sorted-site index of each element
 };
-// The next tile's sites and codes as they arrive from global memory (cp.async), in element
-// order; each lane stages and later packs only its own elements.
-struct NearStage {
-  float4 q[kNearTile];
-  uint32_t code[kNearTile];
-};
-
-// Asynchronous global-to-shared copies (cp.async): 16 bytes (cached in L2 only) or 4 bytes,
-// committed as one group per tile and awaited before the tile is packed.
-__device__ __forceinline__ void copy_async16(void* shared, const void* global) {
-  const unsigned to = (unsigned)__cvta_generic_to_shared(shared);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(to), "l"(global) : "memory");
-}
-__device__ __forceinline__ void copy_async4(void* shared, const void* global) {
-  const unsigned to = (unsigned)__cvta_generic_to_shared(shared);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(to), "l"(global) : "memory");
-}
-__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // Per-warp data of the row walk, kept in shared memory (it is warp-uniform) so the hot
 // loop's registers go to the pair arithmetic. Stereographic projection maps spheres to
 // spheres: the sites within the cutoff of source x (x . y >= k, k = 1 - cut2/2) are the
@@ -744,7 +735,7 @@ using NearTileOf = NearTile<!SHORT && !NEAREST, TRACK>;
 
 template <int G, bool TRACK, bool SHORT, bool NEAREST>
 __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int slice, NearTileOf<TRACK, SHORT, NEAREST>& T,
-                                            NearStage& S, NearWalk<G>& W, double (*sums)[kNearWarps * 32]) {
+                                            NearWalk<G>& W, double (*sums)[kNearWarps * 32]) {
   constexpr int kSub = NearShape<G>::sub;
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -833,13 +824,16 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
     const uint32_t total = __shfl_sync(full, incl, 31);
     const uint32_t shift = start - (incl - len);  // element e of run k is site shift_k + e
     int k = 0;  // the run of this lane's next element: the first lane with incl > e
-    // Stages tile tb: lane l copies elements 64h + 2l and 64h + 2l + 1 (h = 0, 1), those
-    // before the batch's end, into the staging buffer, and keeps their site indices.
-    uint32_t staged[4];
-    auto stage = [&](uint32_t tb) {
+    for (uint32_t tb = 0; tb < total; tb += kNearTile) {
       const int count = (int)min((uint32_t)kNearTile, total - tb);
+      bool mine = false;  // this lane loaded an image of one of the warp's sources
+      __syncwarp();
 #pragma unroll
       for (int h = 0; h < kNearTile / 64; ++h) {
+        // Lane l loads elements 64h + 2l and 64h + 2l + 1 (slot 32h + l) and writes the slot
+        // whole. An element past the batch's end is a blank site: at the origin,
+        // dm2 = |x|^2 ~ 1 lies beyond every cutoff of the chart-grid path (r < 0.9 rad,
+        // cut2 < 0.76), and its code matches no source.
         const int el = 64 * h + 2 * lane;
         const uint32_t e = tb + el;
         uint32_t kin;
@@ -852,30 +846,9 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
         }
         // Element e + 1 is in run k, or starts run k + 1 (runs are nonempty).
         const int k1 = (e + 1 >= kin && k < 31) ? k + 1 : k;
-        staged[2 * h] = __shfl_sync(full, shift, k) + e;
-        staged[2 * h + 1] = __shfl_sync(full, shift, k1) + e + 1;
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-          if (el + b < count) {
-            copy_async16(&S.q[el + b], &sq[staged[2 * h + b]]);
-            copy_async4(&S.code[el + b], &scode[staged[2 * h + b]]);
-          }
-      }
-      copy_async_commit();
-    };
-    if (total > 0) stage(0);
-    for (uint32_t tb = 0; tb < total; tb += kNearTile) {
-      const int count = (int)min((uint32_t)kNearTile, total - tb);
-      bool mine = false;  // this lane loaded an image of one of the warp's sources
-      copy_async_wait();
-      __syncwarp();
-#pragma unroll
-      for (int h = 0; h < kNearTile / 64; ++h) {
-        // Lane l packs its elements 64h + 2l and 64h + 2l + 1 into slot 32h + l, whole. An
-        // element past the batch's end is a blank site: at the origin, dm2 = |x|^2 ~ 1 lies
-        // beyond every cutoff of the chart-grid path (r < 0.9 rad, cut2 < 0.76), and its code
-        // matches no source.
-        const int el = 64 * h + 2 * lane;
+        uint32_t site[2];
+        site[0] = __shfl_sync(full, shift, k) + e;
+        site[1] = __shfl_sync(full, shift, k1) + e + 1;
         float4 y[2];
         uint32_t code[2];
 #pragma unroll
@@ -883,8 +856,8 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
           y[b] = make_float4(0.f, 0.f, 0.f, 0.f);
           code[b] = 0xffffffffu;
           if (el + b < count) {
-            y[b] = S.q[el + b];
-            code[b] = S.code[el + b];
+            y[b] = sq[site[b]];
+            code[b] = scode[site[b]];
           }
         }
         const int slot = 32 * h + lane;
@@ -894,7 +867,7 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
         if (!SHORT && !NEAREST)
           T.norm[slot] = make_float2(2.0f * fmaf(y[0].x, y[0].x, fmaf(y[0].y, y[0].y, fmaf(y[0].z, y[0].z, y[0].w * y[0].w))),
                                      2.0f * fmaf(y[1].x, y[1].x, fmaf(y[1].y, y[1].y, fmaf(y[1].z, y[1].z, y[1].w * y[1].w))));
-        if (TRACK) reinterpret_cast<uint2*>(T.at)[slot] = make_uint2(staged[2 * h], staged[2 * h + 1]);
+        if (TRACK) reinterpret_cast<uint2*>(T.at)[slot] = make_uint2(site[0], site[1]);
 #pragma unroll
         for (int s2 = 0; s2 < G; ++s2)
           mine |= ((code[0] & ~kIdentityBit) == W.src[s2]) | ((code[1] & ~kIdentityBit) == W.src[s2]);
@@ -903,8 +876,6 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
       // the slot loop test each site's source.
       const bool tile_own = __any_sync(full, mine);
       __syncwarp();
-      // The staging buffer is free again: the next tile's copies run under this one's pairs.
-      if (tb + kNearTile < total) stage(tb + kNearTile);
       if (live) {
         if (tile_own)
           near_slots<G, TRACK, SHORT, true, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
@@ -973,12 +944,10 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
 template <int G, bool TRACK, bool SHORT, bool NEAREST>
 __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const NearArgs A) {
   __shared__ NearTileOf<TRACK, SHORT, NEAREST> tiles[kNearWarps];
-  __shared__ NearStage stages[kNearWarps];
   __shared__ NearWalk<G> walks[kNearWarps];
   __shared__ double sums[6][kNearWarps * 32];  // FP64 lane sums: force differences, curvature, energy
   const int w = threadIdx.x >> 5;
-  near32_warp<G, TRACK, SHORT, NEAREST>(A, blockIdx.x * kNearWarps + w, blockIdx.y, tiles[w], stages[w], walks[w],
-                                        sums);
+  near32_warp<G, TRACK, SHORT, NEAREST>(A, blockIdx.x * kNearWarps + w, blockIdx.y, tiles[w], walks[w], sums);
 }
 
 // The spacing pass's FP32 nearest-site search with one source per thread (tile shape 1):
@@ -1010,7 +979,7 @@ __global__ void __launch_bounds__(256) k_nearest_lane(const NearArgs A) {
   const float width = 1.0f / per;
   const uint32_t* __restrict__ cell_off = A.cell_off;
   const float4* __restrict__ sq = A.sq;
-  const uint32_t* __restrict__ scode = A.scode;
+  const uint32_t self = A.self_site[i];  // the source's own site, which is no neighbour
   float best = 4.0f, second = 4.0f;
   int best_at = -1;
   for (int z = lo[2]; z <= hi[2]; ++z) {
@@ -1028,7 +997,7 @@ __global__ void __launch_bounds__(256) k_nearest_lane(const NearArgs A) {
         const float4 s = __ldg(&sq[t]);
         const float mw = x.x - s.x, mx = x.y - s.y, my = x.z - s.z, mz = x.w - s.w;
         float d = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
-        if (__ldg(&scode[t]) == (i | kIdentityBit)) d = 4.0f;  // the source itself
+        if (t == self) d = 4.0f;
         second = fminf(second, fmaxf(best, d));
         if (d < best) {
           best = d;
@@ -1068,10 +1037,15 @@ __global__ void __launch_bounds__(128) k_nearest_exact(const float4* __restrict_
                                                        const uint32_t* __restrict__ list,
                                                        const uint32_t* __restrict__ listed, Rows out,
                                                        unsigned int* __restrict__ ties) {
+  __shared__ double4 ops[kMaxGroupOrder];  // the group's rows: each lane reads its own site's
+  {
+    const int off = c_group_offset[gid], order = c_group_order[gid];
+    for (int k = threadIdx.x; k < order; k += blockDim.x) ops[k] = c_ops32[off + k];
+  }
+  __syncthreads();
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const uint32_t count = *listed;
-  const int off = c_group_offset[gid];
   const NearGrid g = *gp;
   const uint32_t stride = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < count; w += stride) {
@@ -1099,7 +1073,7 @@ __global__ void __launch_bounds__(128) k_nearest_exact(const float4* __restrict_
         if (code == (i | kIdentityBit)) continue;  // the source itself
         const uint32_t j = code & ~kIdentityBit, im = simg[t];
         const int op = (int)(im >> 1);
-        double4 y = normalize4(op == 0 ? to_d4(q[j]) : qmul(to_d4(q[j]), c_ops32[off + op]));
+        double4 y = normalize4(op == 0 ? to_d4(q[j]) : qmul(to_d4(q[j]), ops[op]));
         if (im & 1u) y = neg4(y);
         const double mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
         const double d = mw * mw + mx * mx + my * my + mz * mz;
@@ -1492,11 +1466,11 @@ cudaError_t launch_near_structure(const NearLaunch& L, cudaStream_t s, int* laun
   if (fp64)
     k_site_gather<true><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_code,
                                                                   L.site_img, L.site_pos, L.sq32, L.sq64, L.scode,
-                                                                  L.simg, L.sx);
+                                                                  L.simg, L.sx, nullptr);
   else
     k_site_gather<false><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_code,
                                                                    L.site_img, L.site_pos, L.sq32, L.sq64, L.scode,
-                                                                   L.simg, L.sx);
+                                                                   L.simg, L.sx, L.self_site);
   // 3. sources in Hilbert order
   const int mcells = kOrderDim * kOrderDim * kOrderDim;
   if ((e = cudaMemsetAsync(L.mcount, 0, sizeof(uint32_t) * (mcells + 1), s))) return e;
@@ -1506,10 +1480,14 @@ cudaError_t launch_near_structure(const NearLaunch& L, cudaStream_t s, int* laun
     k_source_count<false><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.grid, L.src_key, L.src_rank, L.mcount);
   if ((e = launch_scan(L.mcount, L.moff, mcells, nullptr, L.scan_tmp, s))) return e;
   k_scatter<<<(n + tb - 1) / tb, tb, 0, s>>>(L.src_key, L.src_rank, L.moff, n, nullptr, L.src_perm);
-  k_bucket_sort<<<(mcells + tb - 1) / tb, tb, 0, s>>>(L.moff, mcells, nullptr, L.src_perm);
+  // Sources within a Hilbert cell in index order, so that a warp's sources (and with them the
+  // order of its sums) are the same every pass. The one-source-per-thread spacing search
+  // computes each source's row alone, in any order, and keeps the arrival order.
+  const bool any_order = !fp64 && L.nearest_only && L.group_size == 1;
+  if (!any_order) k_bucket_sort<<<(mcells + tb - 1) / tb, tb, 0, s>>>(L.moff, mcells, nullptr, L.src_perm);
   // shell masks (1 or 3), shell write, grid, cell count, scatter, bucket sort, site gather,
   // source count, scatter, bucket sort (scans counted by launch_scan; memsets aside)
-  *launches = 9 + shell_launches;
+  *launches = (any_order ? 8 : 9) + shell_launches;
   return cudaGetLastError();
 }
 
@@ -1525,7 +1503,7 @@ NearTask near_task(const NearLaunch& L) {
   NearTask t{};
   t.a = NearArgs{L.q32, L.n, L.src_perm, L.sq32, L.scode, L.cell_off, L.sx, L.grid,
                  near_cut(L.cut2, L.chord, L.cut_z, L.cut_w), slices, direct ? L.out : L.partial, L.n, direct,
-                 L.exact_list, L.exact_count};
+                 L.exact_list, L.exact_count, L.self_site};
   t.group_size = L.group_size;
   t.short_atan = L.short_atan ? 1 : 0;
   t.warps = (L.n + L.group_size - 1) / L.group_size;
@@ -1602,7 +1580,6 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32_batch(const NearT
                                                                     const uint32_t* __restrict__ prefix, int count,
                                                                     uint32_t total, uint32_t* __restrict__ counter) {
   __shared__ NearTileOf<false, SHORT, false> tiles[kNearWarps];
-  __shared__ NearStage stages[kNearWarps];
   __shared__ NearWalk<G> walks[kNearWarps];
   __shared__ double sums[6][kNearWarps * 32];
   __shared__ NearTask mine[kNearWarps];  // the warp's current task, copied in by its lanes
@@ -1627,8 +1604,8 @@ __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32_batch(const NearT
     __syncwarp();
     const uint32_t local = t - prefix[lo];
     const uint32_t warps = (uint32_t)mine[w].warps;
-    near32_warp<G, false, SHORT, false>(mine[w].a, (int)(local % warps), (int)(local / warps), tiles[w], stages[w],
-                                        walks[w], sums);
+    near32_warp<G, false, SHORT, false>(mine[w].a, (int)(local % warps), (int)(local / warps), tiles[w], walks[w],
+                                        sums);
     __syncwarp();
   }
 }

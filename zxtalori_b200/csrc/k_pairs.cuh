@@ -31,6 +31,8 @@ cudaError_t upload_tables(const HostTables& t) {
   if ((e = cudaMemcpyToSymbol(c_ops32, ops32, sizeof(ops32)))) return e;
   if ((e = cudaMemcpyToSymbol(c_planes64, planes64, sizeof(planes64)))) return e;
   if ((e = cudaMemcpyToSymbol(c_planes32, planes32, sizeof(planes32)))) return e;
+  if ((e = cudaMemcpyToSymbol(c_plane_order, t.plane_order, sizeof(t.plane_order)))) return e;
+  if ((e = cudaMemcpyToSymbol(c_plane_reach, t.plane_reach, sizeof(t.plane_reach)))) return e;
   if ((e = cudaMemcpyToSymbol(c_group_offset, t.group_offset, sizeof(int) * 11))) return e;
   if ((e = cudaMemcpyToSymbol(c_group_order, t.group_order, sizeof(int) * 11))) return e;
   return cudaMemcpyToSymbol(c_plane_offset, t.plane_offset, sizeof(int) * 11);
@@ -203,7 +205,9 @@ __device__ __forceinline__ PairTile pair_tile(int tile, int jtiles, int n) {
 //
 // A block holds 128 sources, one per thread, and walks tiles of 128 images of one operator
 // built in shared memory; each thread evaluates two images per iteration with packed FP32
-// arithmetic. The tile stores the images as pairs, component by component (w, w', x, x')
+// arithmetic. The next tile's 128 points (2 KB, contiguous) are copied into shared memory by
+// cp.async while the current tile's pairs run, one point per thread into a double buffer,
+// so a tile starts without waiting on global memory. The tile stores the images as pairs, component by component (w, w', x, x')
 // and (y, y', z, z'), plus 2|y|^2 of each, so one broadcast load gives a component of both.
 // The near twin of an image is chosen by the sign of x . y; its difference d = x - y~
 // gives the near chord |d|^2 directly and the far chord by the parallelogram law
@@ -272,6 +276,7 @@ template <bool TRACK>
 __global__ void __launch_bounds__(kPairBlock, 8) k_pairs32(const float4* __restrict__ q, int n, int op_off, int jtiles,
                                                            int total_tiles, int tiles_per_chunk, Rows out, int stride) {
   __shared__ PairSlots S;
+  __shared__ float4 raw[2][kPairBlock];   // tile points as they arrive; thread t copies and reads point t
   __shared__ double sums[6][kPairBlock];  // FP64 row sums (shared: registers go to the pairs)
   const int i0 = blockIdx.x * kPairBlock;
   const int i = i0 + threadIdx.x;
@@ -283,11 +288,27 @@ __global__ void __launch_bounds__(kPairBlock, 8) k_pairs32(const float4* __restr
   int best_at = -1;
   const int t0 = blockIdx.y * tiles_per_chunk, t1 = min(total_tiles, t0 + tiles_per_chunk);
   const int slot = threadIdx.x >> 1, half = threadIdx.x & 1;
+  // Copies this thread's point of tile `tile` into raw[buffer] (none past the tile's end);
+  // one commit group per tile, empty or not, so the waits count tiles.
+  auto stage = [&](int tile, int buffer) {
+    const PairTile nt = pair_tile(tile, jtiles, n);
+    if ((int)threadIdx.x < nt.count) copy_async16(&raw[buffer][threadIdx.x], &q[nt.j0 + threadIdx.x]);
+    copy_async_commit();
+  };
+  if (t0 < t1) stage(t0, 0);
   for (int tid = t0; tid < t1; ++tid) {
     const PairTile pt = pair_tile(tid, jtiles, n);
+    const int buffer = (tid - t0) & 1;
+    // The other buffer was last read for the previous tile, before this thread went on.
+    if (tid + 1 < t1) {
+      stage(tid + 1, buffer ^ 1);
+      copy_async_wait<1>();  // this tile's copy has landed; the next one may be in flight
+    } else {
+      copy_async_wait<0>();
+    }
     __syncthreads();
     {
-      const float4 y = (int)threadIdx.x < pt.count ? image32(q[pt.j0 + threadIdx.x], op_off + pt.k, pt.k == 0)
+      const float4 y = (int)threadIdx.x < pt.count ? image32(raw[buffer][threadIdx.x], op_off + pt.k, pt.k == 0)
                                                    : make_float4(1.f, 0.f, 0.f, 0.f);
       float* wx = reinterpret_cast<float*>(&S.wx[slot]);
       float* yz = reinterpret_cast<float*>(&S.yz[slot]);

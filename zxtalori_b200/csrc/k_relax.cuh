@@ -318,9 +318,19 @@ __global__ void k_nearest_degrees(const double* __restrict__ nearest, int n, flo
 // the float32 positions (images formed in FP64), so separations carry FP64 accuracy.
 // `near_sites` selects the near-field encoding of `nearest_at` (a sorted site) over the
 // all-pairs one (image index k*n+j). Also writes each source's neighbour source index.
-__global__ void k_refine_nearest(const float4* __restrict__ q32, int n, int gid, Rows rows, int near_sites,
-                                 const uint32_t* __restrict__ scode, const uint32_t* __restrict__ simg,
-                                 int* __restrict__ neighbour) {
+// The group's operator rows are copied into shared memory first: each thread reads the row
+// of its own neighbour's image, and constant memory would serve a warp's distinct rows one
+// after another.
+__global__ void __launch_bounds__(256) k_refine_nearest(const float4* __restrict__ q32, int n, int gid, Rows rows,
+                                                        int near_sites, const uint32_t* __restrict__ scode,
+                                                        const uint32_t* __restrict__ simg,
+                                                        int* __restrict__ neighbour) {
+  __shared__ double4 ops[kMaxGroupOrder];
+  {
+    const int off = c_group_offset[gid], order = c_group_order[gid];
+    for (int k = threadIdx.x; k < order; k += blockDim.x) ops[k] = c_ops32[off + k];
+  }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int at = rows.nearest_at[i];
@@ -328,7 +338,6 @@ __global__ void k_refine_nearest(const float4* __restrict__ q32, int n, int gid,
     neighbour[i] = -1;
     return;
   }
-  const int off = c_group_offset[gid];
   int j, op;
   bool neg = false, any_sign = false;
   if (near_sites) {
@@ -342,7 +351,7 @@ __global__ void k_refine_nearest(const float4* __restrict__ q32, int n, int gid,
     any_sign = true;
   }
   const double4 x = normalize4(to_d4(q32[i]));
-  double4 y = normalize4(op == 0 ? to_d4(q32[j]) : qmul(to_d4(q32[j]), c_ops32[off + op]));
+  double4 y = normalize4(op == 0 ? to_d4(q32[j]) : qmul(to_d4(q32[j]), ops[op]));
   if (neg) y = neg4(y);
   const double mw = x.x - y.x, mx = x.y - y.y, my = x.z - y.z, mz = x.w - y.w;
   double c = mw * mw + mx * mx + my * my + mz * mz;

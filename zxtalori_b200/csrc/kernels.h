@@ -12,6 +12,12 @@ struct HostTables {
   float ops32[kMaxOperatorRows][4];
   double planes64[kMaxPlaneRows][4];
   float planes32[kMaxPlaneRows][4];
+  // Each group's planes sorted by their reach, the least dot product of the plane's normal
+  // with any point of the zone (from the zone's vertices), less 1e-5; -1 for groups whose
+  // zone has no vertices (cyclic groups) and for planes that touch the zone. plane_order holds
+  // the group-local plane index of each sorted row, plane_reach its reach.
+  uint8_t plane_order[kMaxPlaneRows];
+  float plane_reach[kMaxPlaneRows];
   int group_offset[11];
   int group_order[11];
   int plane_offset[11];
@@ -76,6 +82,7 @@ struct NearArgs {
   int direct;  // one slice: rows written in place by source (else partial rows by slice)
   uint32_t* exact_list;   // spacing pass: the sources left to the exact search
   uint32_t* exact_count;
+  const uint32_t* self_site;  // one-source-per-thread spacing search: each source's own sorted site
 };
 
 // One sample's FP32 gather as a task of a shared launch: its arguments, tile shape (sources
@@ -117,6 +124,7 @@ struct NearLaunch {
   double4* sq64;
   uint32_t *scode, *simg;
   float* sx;  // chart x of each sorted site (sites are sorted by x within each cell)
+  uint32_t* self_site;  // per source, its identity image's sorted site (spacing search, tile shape 1)
   uint32_t *src_key, *src_rank, *mcount, *moff, *src_perm;
   NearGrid* grid;
   int* cells;

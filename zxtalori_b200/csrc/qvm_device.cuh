@@ -25,6 +25,11 @@ __constant__ double4 c_planes64[kMaxPlaneRows];
 __constant__ int c_group_offset[11];
 __constant__ int c_group_order[11];
 __constant__ int c_plane_offset[11];
+// Each group's planes sorted by reach (the least dot product of the plane with any zone
+// point, less a margin for rounding): the group-local index of each sorted row and its
+// reach. A source in the zone can be within `margin` of a plane only if its reach <= margin.
+__constant__ uint8_t c_plane_order[kMaxPlaneRows];
+__constant__ float c_plane_reach[kMaxPlaneRows];
 
 // ------------------------------------------------------------------ quaternion helpers
 __device__ __forceinline__ double4 qmul(double4 a, double4 b) {
@@ -135,6 +140,20 @@ __device__ __forceinline__ PairF quey_pair32(float dm2, float dp2) {
   p.a = a;
   p.inv_sine = onept2 * a2b2 * r1;
   return p;
+}
+
+// ------------------------------------------------------------------ asynchronous copies
+// cp.async: a 16-byte global-to-shared copy that bypasses the registers (cached in L2
+// only), committed as a group and awaited with wait_group; both addresses 16-byte aligned.
+__device__ __forceinline__ void copy_async16(void* shared, const void* global) {
+  const unsigned to = (unsigned)__cvta_generic_to_shared(shared);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(to), "l"(global) : "memory");
+}
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// Waits until at most `pending` of this thread's committed groups are still in flight.
+template <int pending>
+__device__ __forceinline__ void copy_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(pending) : "memory");
 }
 
 // ------------------------------------------------------------------ packed FP32 (two pairs)

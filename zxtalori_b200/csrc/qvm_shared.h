@@ -5,6 +5,7 @@
 namespace zo {
 
 constexpr int kMaxOperatorRows = 141;   // sum of |K| over the eleven groups
+constexpr int kMaxGroupOrder = 60;      // |K| of the largest group (I)
 constexpr int kMaxPlaneRows = 271;      // sum of 2|K|-1 zone bisector planes
 constexpr uint32_t kIdentityBit = 0x80000000u;  // site code: the source's identity image
 // Largest chart grid side. The reference clamps it at 128 (src/near.zig:135); at ten million
@@ -21,6 +22,11 @@ constexpr int kOrderDim = 1 << kOrderBits;
 // the union of the sources' neighbourhoods close to each one's).
 constexpr double kSitesPerCell = 2.0;
 constexpr int kNearGroup = 4;
+// The spacing pass's first walk covers this fraction of its cutoff (the 4 mean radii) unless
+// the tile table names another: 2.5 of the 4 radii, about a quarter of the cutoff ball's
+// volume, so nearly every source's nearest lies within it; the few whose nearest may not
+// are searched again over the whole cutoff in FP64.
+constexpr double kSpacingWalk = 2.5 / 4.0;
 
 // Precision of one sample's arithmetic.
 //  kFP32: FP32 pair arithmetic (approximate SFU reciprocals, own atan), FP64 row sums,

@@ -2,13 +2,15 @@
 
 For each group and size bucket (N from 2^b to 2^(b+1)), a Haar sample of the bucket's
 middle size is relaxed with every candidate tile shape - sources per warp (2, 4, 8) times
-target shell sites per chart cell (1.5, 2, 3); the spacing pass also one source per
+target shell sites per chart cell (1 to 3); the spacing pass also one source per
 thread - and the device time of its BB steps is
 taken with CUDA events (zo_bench: L2 flushed before each step). The fastest shape is
 written to the tile table, which every engine reads when it sizes a near-field workspace
 (zo_tiles_lookup shows its choice). Sizes whose cutoff takes the dense path (every image
 tested, no tiles) are skipped. The spacing pass (nearest neighbour only, neighbourhood 4)
-is tuned the same way for the groups asked, with zo_bench_spacing.
+is tuned the same way for the groups asked, with zo_bench_spacing, and then, with its
+fastest shape, the fraction of the cutoff that its first FP32 walk covers (WALKS): a
+shorter walk tests fewer sites but leaves more sources to the exact FP64 search.
 
     python -m zxtalori_b200.tune [--out near_tiles.txt] [--groups O I ...] [--spacing-groups I]
 
@@ -28,9 +30,12 @@ import numpy as np
 from .api import GROUPS, haar
 
 ORDER = {"C2": 2, "C3": 3, "C4": 4, "C6": 6, "D2": 4, "D3": 6, "D4": 8, "D6": 12, "T": 12, "O": 24, "I": 60}
-SHAPES = [(g, spc) for g in (2, 4, 8) for spc in (1.5, 2.0, 3.0)]
+CELLS = (1.0, 1.25, 1.5, 2.0, 3.0)  # target shell sites per chart cell
+SHAPES = [(g, spc) for g in (2, 4, 8) for spc in CELLS]
 # The spacing pass may also search one source per thread (tile shape 1).
-SPACING_SHAPES = SHAPES + [(1, spc) for spc in (1.5, 2.0, 3.0)]
+SPACING_SHAPES = SHAPES + [(1, spc) for spc in CELLS]
+WALKS = (0.45, 0.5, 0.55, 0.625, 0.75)
+DEFAULT_WALK = 0.625
 DEFAULT_TABLE = Path(__file__).resolve().parent / "near_tiles.txt"
 FLUSH_BYTES = 256 << 20
 
@@ -64,9 +69,10 @@ def _relax_step_ms(grid, shape, steps, warmup):
     return float(np.median(out[4:4 + steps]))
 
 
-def _spacing_ms(grid, shape, passes, warmup):
+def _spacing_ms(grid, shape, passes, warmup, walk=0.0):
     lib, h = grid._lib, grid._handle
     grid._check(lib.zo_near_tiles(h, shape[0], shape[1]))
+    grid._check(lib.zo_near_walk(h, walk))
     out = np.zeros(6)
     grid._check(lib.zo_bench_spacing(h, passes, warmup, float(FLUSH_BYTES), out.ctypes.data_as(C.POINTER(C.c_double)),
                                      len(out)))
@@ -95,9 +101,14 @@ def tune(groups=GROUPS, buckets=range(10, 19), spacing_groups=("I",), spacing_bu
                 continue
             with haar(group, n, 2000 + b) as grid:
                 times = {shape: _spacing_ms(grid, shape, steps, warmup) for shape in SPACING_SHAPES}
-            best = min(times, key=times.get)
+                shape = min(times, key=times.get)
+                walks = {w: _spacing_ms(grid, shape, steps, warmup, w) for w in WALKS}
+            walk = min(walks, key=walks.get)
+            best = shape + (walk,)
+            times[best] = walks[walk]
             found[("spacing", group, b)] = (best, times)
-            log(f"spacing {group} {b} n={n}: best {best} {times[best]:.3f} ms (default {times[(4, 2.0)]:.3f} ms)")
+            log(f"spacing {group} {b} n={n}: best {best} {times[best]:.3f} ms (default {times[(4, 2.0)]:.3f} ms, "
+                f"walk {DEFAULT_WALK} {walks[DEFAULT_WALK]:.3f} ms)")
     return found
 
 
@@ -105,10 +116,12 @@ def write_table(found, path=DEFAULT_TABLE, device=""):
     lines = ["# FP32 near-field gather tile table, written by python -m zxtalori_b200.tune",
              f"# measured {time.strftime('%Y-%m-%d')} on {device or 'one GPU'}; device ms per BB step (relax) or",
              "# per spacing pass, L2 flushed; columns: kind group log2-size-bucket sources-per-warp sites-per-cell",
-             "# then the best time and the default shape's (4 sources per warp, 2 sites per cell)"]
+             "# (spacing lines: then the first walk's fraction of the cutoff), then the best time and the",
+             "# default shape's (4 sources per warp, 2 sites per cell, walk 0.625)"]
     for (kind, group, b), (best, times) in sorted(found.items(), key=lambda kv: (kv[0][0], GROUPS.index(kv[0][1]),
                                                                                   kv[0][2])):
-        lines.append(f"{kind} {group} {b} {best[0]} {best[1]:g}  # {times[best]:.4f} ms, default "
+        walk = f" {best[2]:g}" if len(best) > 2 else ""
+        lines.append(f"{kind} {group} {b} {best[0]} {best[1]:g}{walk}  # {times[best]:.4f} ms, default "
                      f"{times[(4, 2.0)]:.4f} ms")
     Path(path).write_text("\n".join(lines) + "\n")
     return path
