@@ -413,20 +413,31 @@ def spacing_section(zo, peak, count=10_000_000, seed=7, measure_count=None):
                                      len(out)))
     g.close()
     n_pairs = count * neighbours_of(count, 60, 4.0)
+    tiles = (C.c_double * 3)()
+    zo.api._library().zo_tiles_lookup(1, zo.GROUPS.index("I"), count, tiles)
+    lane = int(tiles[0]) == 1
     # Algorithmic bytes of one gather launch: every source read once (16 B), every shell
-    # site read once (16 B position + 4 B code + 4 B chart x), the nearest chord (8 B) and
-    # site (4 B) written per source.
+    # site read once (its 16 B position; the warp-tiled search also reads a 4 B code and a
+    # 4 B chart x), the chosen site written per source (4 B; the tiled search also writes
+    # the 8 B chord).
     sites = out[3]
-    algorithmic = count * 16 + sites * 24 + count * 12
+    algorithmic = count * 16 + sites * (16 if lane else 24) + count * (4 if lane else 12)
     achieved = algorithmic / (out[1] * 1e-3) / 1e9
     result = {"workload": f"I, N={count} Haar (seed {seed}), spacing with neighbourhood 4",
               "seconds": dt, "first_call_seconds": first, "pair_evals_per_s": n_pairs / dt,
               "device_ms_per_pass": out[0], "separation_deg": sep, "median_nearest_deg": float(np.median(degrees)),
               "exact_search_points": exact["exact_search"], "exact_ties": exact["exact_ties"],
-              "roofline": {"bound": "hbm", "kernel": "k_near32<nearest only> (spacing gather)",
+              "roofline": {"bound": "hbm",
+                           "kernel": ("k_nearest_lane (one source per thread" if lane else
+                                      "k_near32<nearest only> (") + f"; tile shape {int(tiles[0])}, "
+                                     f"{tiles[1]:g} sites per cell, first walk {tiles[2]:g} of the cutoff)",
                            "kernel_ms_avg": out[1], "launches": int(out[2]), "shell_sites": int(sites),
                            "algorithmic_bytes": algorithmic, "achieved": achieved, "peak": peak[0],
-                           "peak_source": peak[1], "unit": "GB/s", "frac": achieved / peak[0]}}
+                           "peak_source": peak[1], "unit": "GB/s", "frac": achieved / peak[0],
+                           "limiter": "not HBM: each source reads every site of its first ball's cell rows (tens "
+                                      "per source) from L1/L2; ncu on the 1M launch shows L1 throughput at "
+                                      "about 70 % of peak and long-scoreboard stalls first "
+                                      "(profiles/spacing_pass_i10m.md)"}}
     # The same float32 sample through the FP64 method: indices must agree except exact ties.
     g64 = zo.from_quaternions(q, "I", precision="fp64")
     g64.spacing()
@@ -603,6 +614,10 @@ def run_ours(args, dist):
     kernel_ms, kernel_launches, launches_per_step = out[1], out[2], out[3]
     peak = grid._lib.zo_fp32_peak(grid._handle)
     separation = grid.measure()["separation_deg"]
+    # Pairs the gather evaluates and those inside the cutoff, from one counting pass (outside
+    # the timed steps), beside the metric's nominal count.
+    counted = (C.c_double * 2)()
+    grid._check(grid._lib.zo_debug_pair_counts(grid._handle, counted))
     grid.close()
     dist.barrier()
     t_max = dist.reduce(total_ms, "max")
@@ -643,6 +658,11 @@ def run_ours(args, dist):
         "fp64_plain": {"value": fp64_value, "ms_per_step": t64 / k64, "steps": k64,
                        "ratio_fp32_refined_over_fp64": value / fp64_value},
         "separation_deg": separation,
+        "pairs_per_pass": {"nominal": EVALS_PER_PASS, "in_cutoff": counted[1], "candidates": counted[0],
+                           "note": "nominal: the reference's metric count, N min(N|K|, 0.94 delta^3 + 64); "
+                                   "in_cutoff: orbit pairs within the cutoff that exert a force; candidates: "
+                                   "sites the gather evaluates (the union of its warp's four sources' balls, "
+                                   "cell row by cell row); the metric and the roofline use nominal"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "k_near32 (near-field rows)",
                      "peak_source": "FP32 FMA probe on this GPU (zo_fp32_peak); MEASURED_PEAKS.json has no FP32 figure",

@@ -96,7 +96,8 @@ size_t zo_profile_report(void* h, uint8_t* output, size_t capacity);
 int zo_precision(void* h, uint32_t mode);
 uint32_t zo_get_precision(void* h);
 /* Extension: the nearest orbit neighbour's source index of every point (same pass as
- * zo_point_values kind 0), or NULL before such a pass. */
+ * zo_point_values kind 0), or NULL before such a pass (or on a CUDA error, with the message
+ * in zo_error). After zo_spacing the indices are copied to the host on this call. */
 const int32_t* zo_point_neighbours(void* h);
 /* Tuning extension, no reference counterpart: the tile shape of this engine's FP32
  * near-field gathers (relaxation and spacing), instead of the tile table's choice:
@@ -135,6 +136,13 @@ int zo_spacing_exact(void* h, uint32_t* out);
  *   Riesz 1, 2, 3, Green, log sums (the self pair's antipode not yet added), degenerate
  *   flag (width 12). */
 int zo_debug_rows(void* h, uint32_t what, double* out);
+/* Diagnostic extension: one relaxation force pass that counts its pairs (the rows are the
+ * ordinary pass's). out[0]: candidate sites the FP32 near-field gather evaluated (each
+ * source against every site of its warp's cell-row runs), out[1]: pairs inside the cutoff
+ * that exert a force (the own source's images excluded); both -1 when the pass has no FP32
+ * grid gather (all pairs, a dense cutoff, FP64 mode). The reference's metric counts
+ * N min(N|K|, 0.94 delta^3 + 64) pairs per pass (src/engine.zig:905-907). */
+int zo_debug_pair_counts(void* h, double* out);
 /* Development hook (no reference counterpart): the next near-field pass, of the relaxation
  * or of the spacing pass, sizes its shell workspace for only `sites` sites, once (0
  * cancels). A pass that then produces more sites than that overflows, and the engine's

@@ -213,3 +213,36 @@ def test_sites_at_the_cutoff_along_the_chart_axes(engine, ops32):
     # The isolated source's energy is a window remainder of about 1e-11 (its sites sit where
     # the window vanishes); the planted sites' own rows are ordinary.
     np.testing.assert_allclose(rows[1:7, 4], dense["energy"][1:], rtol=1e-5)
+
+
+def test_pair_counts_of_the_gather(engine, ops32):
+    """zo_debug_pair_counts: the in-cutoff pairs the FP32 gather counts equal a k-d tree's
+    count of orbit images within the cutoff chord (own images excluded), up to FP32 rounding at
+    the boundary; the candidates it evaluates include all of them. The rows of the counting
+    pass are the ordinary pass's."""
+    import ctypes as C
+    from scipy.spatial import cKDTree
+
+    group, count, delta = "O", 20000, 20
+    ops = ops32[group]
+    with engine.haar(group, count, 41) as grid:
+        grid.relax(0, neighbourhood=delta)
+        before = grid.debug_rows(0)
+        out = (C.c_double * 2)()
+        grid._check(grid._lib.zo_debug_pair_counts(grid._handle, out))
+        after = grid.debug_rows(0)
+        q = grid.quaternions.astype(np.float64)
+    np.testing.assert_array_equal(before, after)
+    candidates, inside = out[0], out[1]
+    x = qvm.normalize(q)
+    images = qvm.normalize(qvm.images(x, ops))  # (|K|, n, 4)
+    _, cut2 = qvm.near_radius(count, len(ops), delta)
+    chord = np.sqrt(cut2)
+    tree = cKDTree(np.concatenate([images, -images]).reshape(-1, 4))
+    every = int(tree.query_ball_point(x, chord, return_length=True).sum())
+    own = sum(int(np.count_nonzero(np.linalg.norm(s * images[k] - x, axis=1) <= chord))
+              for k in range(len(ops)) for s in (1.0, -1.0))  # the identity image, and any other own image
+    expected = every - own
+    assert abs(inside - expected) <= 1e-5 * expected + 10, (inside, expected)
+    assert candidates >= inside
+    assert candidates < 3 * inside  # the walk stays near the sources' balls

@@ -221,8 +221,7 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   const size_t cells = (size_t)sdim_max_ * sdim_max_ * sdim_max_ + 1;
   const size_t qsize = prec == kFP64 ? sizeof(double4) : sizeof(float4);
   site_q_.ensure(capacity_ * qsize);
-  site_code_.ensure(capacity_ * 4ull);
-  site_img_.ensure(capacity_ * 4ull);
+  site_meta_.ensure(capacity_ * sizeof(uint4));
   site_cell_.ensure(capacity_ * 4ull);
   site_rank_.ensure(capacity_ * 4ull);
   site_pos_.ensure(capacity_ * sizeof(float4));
@@ -239,7 +238,6 @@ void NearField::setup(cudaStream_t s, int prec, const float4* q32, const double4
   mcount_.ensure(mcells * 4);
   moff_.ensure(mcells * 4);
   src_perm_.ensure((size_t)n * 4);
-  if (kind == kTilesSpacing && prec != kFP64) self_site_.ensure((size_t)n * 4);
   grid_.ensure(sizeof(NearGrid));
   cells_.ensure(sizeof(int));
   exact_list_.ensure((size_t)n * 4);
@@ -280,6 +278,7 @@ NearLaunch NearField::make_launch(int prec, const float4* q32, const double4* q6
   L.walk_cut2 = walk * walk;
   L.exact_list = exact_list_.as<uint32_t>();
   L.exact_count = exact_count_.as<uint32_t>();
+  L.pair_counts = counting_ ? pair_counts_.as<unsigned long long>() : nullptr;
   L.s_margin = s_margin_;
   L.cut2 = chord_ * chord_;
   L.chord = chord_;
@@ -296,8 +295,7 @@ NearLaunch NearField::make_launch(int prec, const float4* q32, const double4* q6
   L.rim_count = rim_count_.as<uint32_t>();
   L.site_q32 = prec == kFP64 ? nullptr : site_q_.as<float4>();
   L.site_q64 = prec == kFP64 ? site_q_.as<double4>() : nullptr;
-  L.site_code = site_code_.as<uint32_t>();
-  L.site_img = site_img_.as<uint32_t>();
+  L.site_meta = site_meta_.as<uint4>();
   L.site_cell = site_cell_.as<uint32_t>();
   L.site_rank = site_rank_.as<uint32_t>();
   L.site_pos = site_pos_.as<float4>();
@@ -308,7 +306,6 @@ NearLaunch NearField::make_launch(int prec, const float4* q32, const double4* q6
   L.sq64 = prec == kFP64 ? sq_.as<double4>() : nullptr;
   L.scode = scode_.as<uint32_t>();
   L.sx = sx_.as<float>();
-  L.self_site = L.nearest_only && L.group_size == 1 && prec != kFP64 ? self_site_.as<uint32_t>() : nullptr;
   L.simg = simg_.as<uint32_t>();
   L.src_key = src_key_.as<uint32_t>();
   L.src_rank = src_rank_.as<uint32_t>();
@@ -365,9 +362,9 @@ void NearField::exact_report(cudaStream_t s, uint32_t* listed, uint32_t* ties) {
 
 size_t NearField::bytes() const {
   const DeviceBuffer* all[] = {&counts_,    &offsets_,  &scan_tmp_, &shell_mask_, &rim_list_,  &rim_q_,
-                               &rim_count_, &site_q_,   &site_code_, &site_img_,  &site_cell_, &site_rank_,
+                               &rim_count_, &site_q_,   &site_meta_, &site_cell_, &site_rank_,
                                &site_pos_,  &cell_count_, &cell_off_, &perm_,     &sq_,        &scode_,
-                               &simg_,      &sx_,       &self_site_, &src_key_, &src_rank_,  &mcount_,    &moff_,
+                               &simg_,      &sx_,       &src_key_,  &src_rank_,  &mcount_,    &moff_,
                                &src_perm_,  &grid_,     &cells_,    &exact_list_, &exact_count_};
   size_t total = partial_.bytes();
   for (const DeviceBuffer* b : all) total += b->bytes();
@@ -537,7 +534,7 @@ void RelaxState::summarize_async(cudaStream_t s, int n, int order, RowSummary* s
   if (prec == kFP32) ZO_CUDA(launch_refine_nearest(q32, n, gid, r, near_sites, scode, simg, neighbours_.as<int>(), s));
   else ZO_CUDA(launch_neighbour_index(r, n, near_sites, scode, neighbours_.as<int>(), s));
   ZO_CUDA(launch_row_summary(r, n, summary_partials_.as<double>(), near_partials_.as<double>(), near_rows_.as<int>(),
-                             summary_.as<RowSummary>(), s));
+                             summary_.as<RowSummary>(), s, nearest_only));
   ZO_CUDA(launch_nearest_degrees(r.nearest, n, degrees_.as<float>(), s));
   ZO_CUDA(cudaMemcpyAsync(summary, summary_.as<RowSummary>(), sizeof(RowSummary), cudaMemcpyDeviceToHost, s));
   if (degrees) ZO_CUDA(cudaMemcpyAsync(degrees, degrees_.as<float>(), (size_t)n * 4, cudaMemcpyDeviceToHost, s));
@@ -762,6 +759,7 @@ void Engine::finish_async() {
   if (flag) ZO_CUDA(cudaMemcpyAsync(stage_.overflow, flag, 4, cudaMemcpyDeviceToHost, stream_));
   point_separation_.resize(n_);
   point_neighbours_.resize(n_);
+  neighbours_on_device_ = false;
   relax_state_.summarize_async(stream_, n, (int)order(), stage_.summary, point_separation_.data(),
                                point_neighbours_.data(), prec_, q32(), group_);
   ZO_CUDA(cudaMemcpyAsync(stage_.positions, q32(), (size_t)n * 16, cudaMemcpyDeviceToHost, stream_));
@@ -976,6 +974,7 @@ Measures Engine::relax_state_measure() {
     if (relax_state_.near_overflowed(stream_)) continue;
     point_separation_.resize(n_);
     point_neighbours_.resize(n_);
+    neighbours_on_device_ = false;
     point_separation_iteration_ = iteration_;
     Measures m = relax_state_.summarize(stream_, (int)n_, (int)order(), point_separation_.data(),
                                         point_neighbours_.data(), prec_, q32(), group_);
@@ -1076,8 +1075,8 @@ void Engine::spacing() {
   apply_overrides(spacing_state_);
   spacing_state_.prepare(stream_, (int)n_, prec_);
   point_separation_.resize(n_);
-  point_neighbours_.resize(n_);
   point_separation_iteration_ = iteration_;
+  neighbours_on_device_ = false;
   for (int attempt = 0;; ++attempt) {
     if (attempt == 4) throw Failure("NearShellTooLarge");
     spacing_state_.record_forces(stream_, prec_, q32(), q64(), (int)n_, group_, true, budget_scale_, sms_);
@@ -1085,8 +1084,11 @@ void Engine::spacing() {
     if (!spacing_state_.near_overflowed(stream_)) break;
   }
   try {
-    spacing_state_.summarize(stream_, (int)n_, (int)order(), point_separation_.data(), point_neighbours_.data(), prec_,
-                             q32(), group_);
+    // The per-point degrees come to the host with the pass (the reference's spacing makes
+    // them); the neighbour indices stay on the device until point_neighbours() asks.
+    spacing_state_.summarize(stream_, (int)n_, (int)order(), point_separation_.data(), nullptr, prec_, q32(),
+                             group_);
+    neighbours_on_device_ = true;
   } catch (const Failure& x) {
     // A duplicate shows as a zero separation below.
     if (std::strcmp(x.what(), "DuplicateOrientations") != 0) throw;
@@ -1169,6 +1171,37 @@ void Engine::identity(bool add, bool fixed) {
     ZO_CUDA(cudaStreamSynchronize(stream_));
     relax_state_.current = false;
   }
+}
+
+void Engine::debug_pair_counts(double* out) {
+  if (n_ == 0) throw Failure("NoOrientations");
+  ZO_CUDA(cudaSetDevice(device_));
+  const int n = (int)n_;
+  sync_neighbourhood();
+  relax_state_.prepare(stream_, n, prec_);
+  out[0] = out[1] = -1;
+  // Size the workspace with an ordinary pass first, then count one pass.
+  relax_state_.current = false;
+  relax_state_.record_forces(stream_, prec_, q32(), q64(), n, group_, false, budget_scale_, sms_);
+  NearField* nf = relax_state_.near_field();
+  if (prec_ == kFP64 || !nf || nf->dense()) return;
+  unsigned long long* counts = nf->pair_counts();
+  ZO_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), stream_));
+  nf->count_pairs(true);
+  try {
+    relax_state_.current = false;
+    relax_state_.record_forces(stream_, prec_, q32(), q64(), n, group_, false, budget_scale_, sms_);
+  } catch (...) {
+    nf->count_pairs(false);
+    throw;
+  }
+  nf->count_pairs(false);
+  unsigned long long host[2];
+  ZO_CUDA(cudaMemcpyAsync(host, counts, sizeof host, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  relax_state_.current = false;
+  out[0] = (double)host[0];
+  out[1] = (double)host[1];
 }
 
 void Engine::debug_rows(uint32_t what, double* out) {
@@ -1328,8 +1361,8 @@ void Engine::bench_spacing(uint32_t passes, uint32_t warmup, double flush_bytes,
       if (fbytes) ZO_CUDA(cudaMemsetAsync(flush.as<void>(), (int)(k & 0xff), fbytes, stream_));
       ZO_CUDA(cudaEventRecord(ev[2 * k], stream_));
       spacing_state_.record_forces(stream_, prec_, q32(), q64(), (int)n_, group_, true, budget_scale_, sms_);
-      spacing_state_.summarize_async(stream_, (int)n_, (int)order(), &summary, point_separation_.data(),
-                                     point_neighbours_.data(), prec_, q32(), group_);
+      spacing_state_.summarize_async(stream_, (int)n_, (int)order(), &summary, point_separation_.data(), nullptr,
+                                     prec_, q32(), group_);
       ZO_CUDA(cudaEventRecord(ev[2 * k + 1], stream_));
     }
   } catch (...) {
@@ -1365,8 +1398,17 @@ const float* Engine::point_values(uint32_t kind) const {
   if (kind != 0 || !point_separation_iteration_ || point_separation_.size() != n_) return nullptr;
   return point_separation_.data();
 }
-const int* Engine::point_neighbours() const {
-  if (!point_separation_iteration_ || point_neighbours_.size() != n_) return nullptr;
+const int* Engine::point_neighbours() {
+  if (!point_separation_iteration_) return nullptr;
+  if (neighbours_on_device_) {
+    point_neighbours_.resize(n_);
+    ZO_CUDA(cudaSetDevice(device_));
+    ZO_CUDA(cudaMemcpyAsync(point_neighbours_.data(), spacing_state_.neighbours_device(), (size_t)n_ * sizeof(int),
+                            cudaMemcpyDeviceToHost, stream_));
+    ZO_CUDA(cudaStreamSynchronize(stream_));
+    neighbours_on_device_ = false;
+  }
+  if (point_neighbours_.size() != n_) return nullptr;
   return point_neighbours_.data();
 }
 

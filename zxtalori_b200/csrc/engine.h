@@ -180,6 +180,13 @@ class NearField {
   // The next pass sizes the workspace again (after an observed overflow, or for a new
   // sample); allocations large enough are reused.
   void invalidate() { ready_ = false; }
+  // Diagnostic: while on, each FP32 grid gather of a force pass adds its candidate sites and
+  // in-cutoff pairs to two device counters (pair_counts()).
+  void count_pairs(bool on) { counting_ = on; }
+  unsigned long long* pair_counts() {
+    pair_counts_.ensure(2 * sizeof(unsigned long long));
+    return pair_counts_.as<unsigned long long>();
+  }
   // Development: the next sizing of the workspace holds only `sites` shell sites (once), so
   // a pass overflows and the resize-and-redo path runs without a GPU fault.
   void override_capacity(uint32_t sites) {
@@ -219,14 +226,15 @@ class NearField {
   NearTiles tiles_;
   std::optional<NearTiles> forced_;
   double walk_override_ = 0;
+  bool counting_ = false;
+  DeviceBuffer pair_counts_;
   bool ready_ = false;
   int n_ = 0, prec_ = -1, capacity_ = 0, sdim_max_ = 1, slices_ = 1, slices32_ = 1;
   uint32_t next_capacity_ = 0;
   double radius_ = 0, s_margin_ = 0, chord_ = 0;
   DeviceBuffer counts_, offsets_, scan_tmp_, shell_mask_, rim_list_, rim_q_, rim_count_;
-  DeviceBuffer site_q_, site_code_, site_img_, site_cell_, site_rank_, site_pos_;
-  DeviceBuffer cell_count_, cell_off_, perm_, sq_, scode_, simg_, sx_, self_site_, src_key_, src_rank_, mcount_, moff_,
-      src_perm_;
+  DeviceBuffer site_q_, site_meta_, site_cell_, site_rank_, site_pos_;
+  DeviceBuffer cell_count_, cell_off_, perm_, sq_, scode_, simg_, sx_, src_key_, src_rank_, mcount_, moff_, src_perm_;
   DeviceBuffer grid_, cells_;
   DeviceBuffer exact_list_, exact_count_;
   RowBuffers partial_;
@@ -271,6 +279,8 @@ class RelaxState {
                        int prec, const float4* q32, int gid);
   Measures measures_of(const RowSummary& sum, int n, int order) const;
   const RelaxDev* state_device() const { return state_.as<RelaxDev>(); }
+  // Each source's nearest neighbour's source index from the last summarize (device).
+  const int* neighbours_device() const { return neighbours_.as<int>(); }
   StepResult result_of(const RelaxDev& st) const { return step_result(st); }
   bool near_overflowed(cudaStream_t s) { return near_ && near_->overflowed(s); }
   NearField* near_field() { return near_.get(); }
@@ -308,7 +318,9 @@ class Engine {
   void identity(bool add, bool fixed);
   const char* stats();
   const float* point_values(uint32_t kind) const;
-  const int* point_neighbours() const;
+  // The neighbour indices of the last pass that made point values; after a spacing pass they
+  // are copied to the host here, on the first request.
+  const int* point_neighbours();
   // Device memory this engine holds now (every buffer it sized, from the pool).
   size_t device_bytes() const;
   // Of the last spacing pass: sources settled by the exact FP64 search instead of the FP32
@@ -363,6 +375,10 @@ class Engine {
   // Development: one pass's raw rows to host. what 0: force pass of the relaxation
   // (8 doubles per source), 1: full measure rows (12 doubles per source).
   void debug_rows(uint32_t what, double* out);
+  // One force pass of the relaxation counting its pairs: out[0] candidate sites evaluated,
+  // out[1] pairs inside the cutoff that exert a force; -1 for both when the pass has no FP32
+  // grid gather (all pairs, a dense cutoff, FP64 mode).
+  void debug_pair_counts(double* out);
   // Measurement: `steps` relaxation steps after `warmup`, each bracketed by CUDA events on
   // the engine's stream with an L2 flush (a memset of flush_bytes) before it, outside the
   // events. out[0] total step ms, out[1] dominant-kernel ms, out[2] its launches, out[3]
@@ -467,6 +483,7 @@ class Engine {
   double neighbourhood_ = 0, measure_neighbourhood_ = 0;
   PinnedArray<float> point_separation_;
   PinnedArray<int> point_neighbours_;
+  bool neighbours_on_device_ = false;  // the last spacing pass's indices are still on the device
   std::optional<uint32_t> point_separation_iteration_;
   double step_deg_ = 0, force_rms_ = 0;
   std::atomic<bool> cancelled_{false};

@@ -148,7 +148,15 @@ int zo_precision(void* h, uint32_t mode) {
   return guarded(h, "Precision", [&](Engine& e) { e.set_precision((int)mode); });
 }
 uint32_t zo_get_precision(void* h) { return (uint32_t) static_cast<Engine*>(h)->precision(); }
-const int32_t* zo_point_neighbours(void* h) { return static_cast<Engine*>(h)->point_neighbours(); }
+const int32_t* zo_point_neighbours(void* h) {
+  Engine* e = static_cast<Engine*>(h);
+  try {
+    return e->point_neighbours();
+  } catch (const std::exception& x) {
+    std::snprintf(e->err, sizeof e->err, "Neighbours: %s", x.what());
+    return nullptr;
+  }
+}
 
 int zo_near_tiles(void* h, uint32_t sources_per_warp, float sites_per_cell) {
   return guarded(h, "Tiles", [&](Engine& e) {
@@ -178,6 +186,10 @@ int zo_spacing_exact(void* h, uint32_t* out) {
 
 int zo_debug_shell_capacity(void* h, uint32_t sites) {
   return guarded(h, "Rows", [&](Engine& e) { e.debug_shell_capacity(sites); });
+}
+
+int zo_debug_pair_counts(void* h, double* out) {
+  return guarded(h, "Rows", [&](Engine& e) { e.debug_pair_counts(out); });
 }
 
 int zo_debug_rows(void* h, uint32_t what, double* out) {

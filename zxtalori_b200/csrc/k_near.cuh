@@ -223,8 +223,8 @@ __global__ void __launch_bounds__(256) k_shell_write(const float4* __restrict__ 
                                                      int n, int gid, const uint4* __restrict__ masks,
                                                      const uint32_t* __restrict__ offsets, int capacity,
                                                      float4* __restrict__ site_q32, double4* __restrict__ site_q64,
-                                                     uint32_t* __restrict__ site_code, uint32_t* __restrict__ site_img,
-                                                     float4* __restrict__ site_pos, NearGrid* grid) {
+                                                     uint4* __restrict__ site_meta, float4* __restrict__ site_pos,
+                                                     NearGrid* grid) {
   __shared__ double4 g[60];
   const int off = c_group_offset[gid], order = c_group_order[gid];
   unit_operators(g, off, order, FP64);
@@ -250,8 +250,8 @@ __global__ void __launch_bounds__(256) k_shell_write(const float4* __restrict__ 
         if (img & 1) y = make_float4(-y.x, -y.y, -y.z, -y.w);
         site_q32[at] = y;
       }
-      site_code[at] = (uint32_t)j | (identity ? kIdentityBit : 0u);
-      site_img[at] = (uint32_t)img;
+      // What the sorted copy needs of the site in one 16-byte record (one random read there).
+      site_meta[at] = make_uint4((uint32_t)j | (identity ? kIdentityBit : 0u), (uint32_t)img, __float_as_uint(p.x), 0u);
       site_pos[at] = make_float4(p.x, p.y, p.z, 0.f);
       lo[0] = fminf(lo[0], p.x);
       lo[1] = fminf(lo[1], p.y);
@@ -386,23 +386,22 @@ __global__ void k_bucket_sort(const uint32_t* __restrict__ offsets, int max_buck
   }
 }
 
+// The sites in sorted order: position, code, image number and chart x of sorted site p from
+// unsorted site perm[p] (two random reads: the position and the 16-byte record).
 template <bool FP64>
 __global__ void k_site_gather(const uint32_t* __restrict__ perm, const NearGrid* __restrict__ gp,
                               const float4* __restrict__ q32, const double4* __restrict__ q64,
-                              const uint32_t* __restrict__ code, const uint32_t* __restrict__ img,
-                              const float4* __restrict__ pos, float4* __restrict__ sq32, double4* __restrict__ sq64,
-                              uint32_t* __restrict__ scode, uint32_t* __restrict__ simg, float* __restrict__ sx,
-                              uint32_t* __restrict__ self_site) {
+                              const uint4* __restrict__ meta, float4* __restrict__ sq32, double4* __restrict__ sq64,
+                              uint32_t* __restrict__ scode, uint32_t* __restrict__ simg, float* __restrict__ sx) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= gp->sites) return;
   const uint32_t s = perm[p];
   if (FP64) sq64[p] = q64[s];
   else sq32[p] = q32[s];
-  const uint32_t c = code[s];
-  scode[p] = c;
-  simg[p] = img[s];
-  sx[p] = pos[s].x;
-  if (self_site && (c & kIdentityBit)) self_site[c & ~kIdentityBit] = (uint32_t)p;  // one identity site per source
+  const uint4 m = meta[s];
+  scode[p] = m.x;
+  simg[p] = m.y;
+  sx[p] = __uint_as_float(m.z);
 }
 
 // ------------------------------------------------------------------ 3. sources in Hilbert order
@@ -649,11 +648,14 @@ __device__ __forceinline__ void merge_sums(double (*sums)[kNearWarps * 32], floa
 // its identity image is no neighbour); without it that test is left out. SHORT: cutoffs up
 // to 0.4 rad take the chord form (near_chord_pair32x2), wider ones the arctangent of near
 // over far. se sums energy / pi. NEAREST: only the nearest site is tracked.
-template <int G, bool TRACK, bool SHORT, bool OWN, bool NEAREST, class Tile>
+// COUNT (a diagnostic pass only): the lane also counts the sites it evaluates (candidates)
+// and those inside the cutoff that exert a force (in).
+template <int G, bool TRACK, bool SHORT, bool OWN, bool NEAREST, bool COUNT, class Tile>
 __device__ __forceinline__ void near_slots(const Tile& T, int count, int sub, uint32_t i, float2 xw, float2 xx,
                                            float2 xy, float2 xz, float2 xn, float cut_hi, float cw, float czw,
                                            float pk, float2& sw, float2& sx, float2& sy, float2& sz, float2& sc,
-                                           float2& se, float& best, int& best_at, float& second) {
+                                           float2& se, float& best, int& best_at, float& second, float cut2,
+                                           uint32_t& candidates, uint32_t& in) {
   constexpr int kSub = NearShape<G>::sub;
 #pragma unroll
   for (int m = 0; m < NearShape<G>::slots; ++m) {
@@ -677,6 +679,10 @@ __device__ __forceinline__ void near_slots(const Tile& T, int count, int sub, ui
       own1 = ((c.y ^ i) & ~kIdentityBit) == 0;
       if (own0 && c.x != i) n0 = 4.0f;
       if (own1 && c.y != i) n1 = 4.0f;
+    }
+    if (COUNT) {
+      candidates += (first < count) + (first + 1 < count);
+      in += (n0 <= cut2 && !own0) + (n1 <= cut2 && !own1);
     }
     if (NEAREST) {
       // The two smallest chords (of distinct sites) and where the smallest is.
@@ -733,7 +739,7 @@ __device__ __forceinline__ void near_slots(const Tile& T, int count, int sub, ui
 template <bool TRACK, bool SHORT, bool NEAREST>
 using NearTileOf = NearTile<!SHORT && !NEAREST, TRACK>;
 
-template <int G, bool TRACK, bool SHORT, bool NEAREST>
+template <int G, bool TRACK, bool SHORT, bool NEAREST, bool COUNT = false>
 __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int slice, NearTileOf<TRACK, SHORT, NEAREST>& T,
                                             NearWalk<G>& W, double (*sums)[kNearWarps * 32]) {
   constexpr int kSub = NearShape<G>::sub;
@@ -788,6 +794,7 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
   const float2 xw = splat(x.x), xx = splat(x.y), xy = splat(x.z), xz = splat(x.w), xn = splat(nx2);
   float best = 4.0f, second = 4.0f;
   int best_at = -1;
+  uint32_t candidates = 0, in = 0;  // COUNT only
   float2 sw = splat(0.f), sx = splat(0.f), sy = splat(0.f), sz = splat(0.f), sc = splat(0.f), se = splat(0.f);
   int since = 0;  // tiles since the last FP64 merge
   const int rows = (W.chi[1] - W.clo[1] + 1) * (W.chi[2] - W.clo[2] + 1);
@@ -878,11 +885,13 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
       __syncwarp();
       if (live) {
         if (tile_own)
-          near_slots<G, TRACK, SHORT, true, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
-                                                  sz, sc, se, best, best_at, second);
+          near_slots<G, TRACK, SHORT, true, NEAREST, COUNT>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw,
+                                                         sx, sy, sz, sc, se, best, best_at, second, cut2, candidates,
+                                                         in);
         else
-          near_slots<G, TRACK, SHORT, false, NEAREST>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw, sx, sy,
-                                                   sz, sc, se, best, best_at, second);
+          near_slots<G, TRACK, SHORT, false, NEAREST, COUNT>(T, count, sub, i, xw, xx, xy, xz, xn, cut_hi, cw, czw, pk, sw,
+                                                          sx, sy, sz, sc, se, best, best_at, second, cut2, candidates,
+                                                          in);
       }
       if (!NEAREST && ++since == NearShape<G>::merge) {
         merge_sums(sums, sw, sx, sy, sz, sc, se);
@@ -891,6 +900,18 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
     }
   }
   merge_sums(sums, sw, sx, sy, sz, sc, se);
+  if (COUNT) {
+    unsigned long long c = live ? candidates : 0u, v = live ? in : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      c += __shfl_xor_sync(full, c, o);
+      v += __shfl_xor_sync(full, v, o);
+    }
+    if (lane == 0) {
+      atomicAdd(&A.pair_counts[0], c);
+      atomicAdd(&A.pair_counts[1], v);
+    }
+  }
   // The nearest over the source's lanes: smallest chord, then smallest sorted-site index
   // (the first such site in the walk's order).
 #pragma unroll
@@ -941,13 +962,13 @@ __device__ __forceinline__ void near32_warp(const NearArgs& A, int warp, int sli
   if (TRACK) A.out.nearest_at[at] = best_at;
 }
 
-template <int G, bool TRACK, bool SHORT, bool NEAREST>
+template <int G, bool TRACK, bool SHORT, bool NEAREST, bool COUNT = false>
 __global__ void __launch_bounds__(kNearWarps * 32, 7) k_near32(const NearArgs A) {
   __shared__ NearTileOf<TRACK, SHORT, NEAREST> tiles[kNearWarps];
   __shared__ NearWalk<G> walks[kNearWarps];
   __shared__ double sums[6][kNearWarps * 32];  // FP64 lane sums: force differences, curvature, energy
   const int w = threadIdx.x >> 5;
-  near32_warp<G, TRACK, SHORT, NEAREST>(A, blockIdx.x * kNearWarps + w, blockIdx.y, tiles[w], walks[w], sums);
+  near32_warp<G, TRACK, SHORT, NEAREST, COUNT>(A, blockIdx.x * kNearWarps + w, blockIdx.y, tiles[w], walks[w], sums);
 }
 
 // The spacing pass's FP32 nearest-site search with one source per thread (tile shape 1):
@@ -979,7 +1000,10 @@ __global__ void __launch_bounds__(256) k_nearest_lane(const NearArgs A) {
   const float width = 1.0f / per;
   const uint32_t* __restrict__ cell_off = A.cell_off;
   const float4* __restrict__ sq = A.sq;
-  const uint32_t self = A.self_site[i];  // the source's own site, which is no neighbour
+  // The source's own (identity) site holds x itself, bit for bit, and is no neighbour: the
+  // first site equal to x is taken for it. Any further site equal to x (a duplicate of the
+  // source, or an image of it that rounds onto it) is a neighbour at distance 0.
+  bool self_seen = false;
   float best = 4.0f, second = 4.0f;
   int best_at = -1;
   for (int z = lo[2]; z <= hi[2]; ++z) {
@@ -997,7 +1021,10 @@ __global__ void __launch_bounds__(256) k_nearest_lane(const NearArgs A) {
         const float4 s = __ldg(&sq[t]);
         const float mw = x.x - s.x, mx = x.y - s.y, my = x.z - s.z, mz = x.w - s.w;
         float d = fmaf(mw, mw, fmaf(mx, mx, fmaf(my, my, mz * mz)));
-        if (t == self) d = 4.0f;
+        if (d == 0.0f && !self_seen && s.x == x.x && s.y == x.y && s.z == x.z && s.w == x.w) {
+          self_seen = true;  // (an equal site has d = 0: the rare branch)
+          d = 4.0f;
+        }
         second = fminf(second, fmaxf(best, d));
         if (d < best) {
           best = d;
@@ -1011,14 +1038,9 @@ __global__ void __launch_bounds__(256) k_nearest_lane(const NearArgs A) {
     const uint32_t slot = atomicAdd(A.exact_count, 1u);
     A.exact_list[slot] = i;
   }
-  if (best > (float)A.cut.cut2) {  // no site within the cutoff
-    best = 4.0f;
-    best_at = -1;
-  }
-  A.out.force[i] = make_double4(0.0, 0.0, 0.0, 0.0);
-  A.out.energy[i] = 0.0;
-  A.out.nearest[i] = best;
-  A.out.nearest_at[i] = best_at;
+  // Only the chosen site: the refinement that follows computes its FP64 chord (4 when there
+  // is none within the cutoff), and a nearest-only pass has no forces or energies.
+  A.out.nearest_at[i] = best > (float)A.cut.cut2 ? -1 : best_at;
 }
 
 // The exact nearest orbit neighbour of each source the FP32 spacing gather listed: every
@@ -1410,6 +1432,9 @@ cudaError_t launch_near32_shape(bool track, bool short_atan, bool nearest, dim3 
   auto kernel = nearest ? k_near32<G, true, false, true>
                         : track ? (short_atan ? k_near32<G, true, true, false> : k_near32<G, true, false, false>)
                                 : (short_atan ? k_near32<G, false, true, false> : k_near32<G, false, false, false>);
+  // A diagnostic pass that counts its pairs (a relaxation's force pass only).
+  if (A.pair_counts && !nearest && !track)
+    kernel = short_atan ? k_near32<G, false, true, false, true> : k_near32<G, false, false, false, true>;
   kernel<<<grid, kNearWarps * 32, 0, s>>>(A);
   return cudaGetLastError();
 }
@@ -1448,11 +1473,11 @@ cudaError_t launch_near_structure(const NearLaunch& L, cudaStream_t s, int* laun
   if (e) return e;
   if (fp64)
     k_shell_write<true><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.shell_mask, L.offsets, L.capacity,
-                                                         L.site_q32, L.site_q64, L.site_code, L.site_img, L.site_pos,
+                                                         L.site_q32, L.site_q64, L.site_meta, L.site_pos,
                                                          L.grid);
   else
     k_shell_write<false><<<(n + tb - 1) / tb, tb, 0, s>>>(L.q32, L.q64, n, L.gid, L.shell_mask, L.offsets, L.capacity,
-                                                          L.site_q32, L.site_q64, L.site_code, L.site_img, L.site_pos,
+                                                          L.site_q32, L.site_q64, L.site_meta, L.site_pos,
                                                           L.grid);
   // 2. grid and the site sort
   k_grid_setup<<<1, 1, 0, s>>>(L.grid, L.offsets + n, L.capacity, L.sdim_max, (float)L.sites_per_cell, L.cells);
@@ -1464,13 +1489,11 @@ cudaError_t launch_near_structure(const NearLaunch& L, cudaStream_t s, int* laun
                                                       &L.grid->sites, L.perm);
   k_bucket_sort<<<(max_cells + tb - 1) / tb, tb, 0, s>>>(L.cell_off, max_cells, L.cells, L.perm, L.site_pos);
   if (fp64)
-    k_site_gather<true><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_code,
-                                                                  L.site_img, L.site_pos, L.sq32, L.sq64, L.scode,
-                                                                  L.simg, L.sx, nullptr);
+    k_site_gather<true><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_meta,
+                                                                  L.sq32, L.sq64, L.scode, L.simg, L.sx);
   else
-    k_site_gather<false><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64, L.site_code,
-                                                                   L.site_img, L.site_pos, L.sq32, L.sq64, L.scode,
-                                                                   L.simg, L.sx, L.self_site);
+    k_site_gather<false><<<(L.capacity + tb - 1) / tb, tb, 0, s>>>(L.perm, L.grid, L.site_q32, L.site_q64,
+                                                                   L.site_meta, L.sq32, L.sq64, L.scode, L.simg, L.sx);
   // 3. sources in Hilbert order
   const int mcells = kOrderDim * kOrderDim * kOrderDim;
   if ((e = cudaMemsetAsync(L.mcount, 0, sizeof(uint32_t) * (mcells + 1), s))) return e;
@@ -1503,7 +1526,7 @@ NearTask near_task(const NearLaunch& L) {
   NearTask t{};
   t.a = NearArgs{L.q32, L.n, L.src_perm, L.sq32, L.scode, L.cell_off, L.sx, L.grid,
                  near_cut(L.cut2, L.chord, L.cut_z, L.cut_w), slices, direct ? L.out : L.partial, L.n, direct,
-                 L.exact_list, L.exact_count, L.self_site};
+                 L.exact_list, L.exact_count, L.pair_counts};
   t.group_size = L.group_size;
   t.short_atan = L.short_atan ? 1 : 0;
   t.warps = (L.n + L.group_size - 1) / L.group_size;

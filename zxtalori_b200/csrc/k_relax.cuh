@@ -221,18 +221,22 @@ __device__ __forceinline__ float nearest_degrees_of(double chord2) {
 }
 
 // Quick measures of a force pass (src/pairs.zig:130-140, 182-199): energy sum, force^2 sum
-// and the smallest nearest chord with its source, deterministic.
+// and the smallest nearest chord with its source, deterministic. A nearest-only pass (the
+// spacing pass) writes no forces or energies, and its sums are left 0.
 __global__ void __launch_bounds__(kRelaxBlock) k_row_summary(Rows rows, int n, double* __restrict__ partials,
                                                              double* __restrict__ near_partials,
-                                                             int* __restrict__ near_rows, RowSummary* out) {
+                                                             int* __restrict__ near_rows, RowSummary* out,
+                                                             int nearest_only) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0, 0};
   double best = 4.0;
   int at = -1;
   if (i < n) {
-    const double4 f = rows.force[i];
-    v[0] = rows.energy[i];
-    v[1] = f.x * f.x + f.y * f.y + f.z * f.z;
+    if (!nearest_only) {
+      const double4 f = rows.force[i];
+      v[0] = rows.energy[i];
+      v[1] = f.x * f.x + f.y * f.y + f.z * f.z;
+    }
     best = rows.nearest[i];
     at = i;
   }
@@ -334,7 +338,8 @@ __global__ void __launch_bounds__(256) k_refine_nearest(const float4* __restrict
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int at = rows.nearest_at[i];
-  if (at < 0) {
+  if (at < 0) {  // no orbit neighbour within the cutoff
+    rows.nearest[i] = 4.0;
     neighbour[i] = -1;
     return;
   }

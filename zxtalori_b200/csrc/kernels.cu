@@ -46,8 +46,9 @@ cudaError_t launch_move_fold(float4* q32, double4* q64, int n, int gid, int prec
 }
 
 cudaError_t launch_row_summary(Rows rows, int n, double* partials, double* near_partials, int* near_rows,
-                               RowSummary* out, cudaStream_t s) {
-  k_row_summary<<<reduce_blocks(n), kRelaxBlock, 0, s>>>(rows, n, partials, near_partials, near_rows, out);
+                               RowSummary* out, cudaStream_t s, bool nearest_only) {
+  k_row_summary<<<reduce_blocks(n), kRelaxBlock, 0, s>>>(rows, n, partials, near_partials, near_rows, out,
+                                                          nearest_only ? 1 : 0);
   return cudaGetLastError();
 }
 

@@ -82,7 +82,9 @@ struct NearArgs {
   int direct;  // one slice: rows written in place by source (else partial rows by slice)
   uint32_t* exact_list;   // spacing pass: the sources left to the exact search
   uint32_t* exact_count;
-  const uint32_t* self_site;  // one-source-per-thread spacing search: each source's own sorted site
+  // A diagnostic force pass only (else null): adds the candidate sites evaluated and the
+  // pairs inside the cutoff that exert a force.
+  unsigned long long* pair_counts;
 };
 
 // One sample's FP32 gather as a task of a shared launch: its arguments, tile shape (sources
@@ -108,6 +110,7 @@ struct NearLaunch {
   double walk_cut2;
   uint32_t* exact_list;
   uint32_t* exact_count;
+  unsigned long long* pair_counts;  // diagnostic force pass: candidates and in-cutoff pairs (else null)
   const float4* q32;
   const double4* q64;
   uint32_t *counts, *offsets, *scan_tmp;
@@ -117,14 +120,14 @@ struct NearLaunch {
   uint32_t* rim_count;
   float4* site_q32;
   double4* site_q64;
-  uint32_t *site_code, *site_img, *site_cell, *site_rank;
+  uint4* site_meta;  // per unsorted site: code, image number, chart x (bits), 0
+  uint32_t *site_cell, *site_rank;
   float4* site_pos;
   uint32_t *cell_count, *cell_off, *perm;
   float4* sq32;
   double4* sq64;
   uint32_t *scode, *simg;
   float* sx;  // chart x of each sorted site (sites are sorted by x within each cell)
-  uint32_t* self_site;  // per source, its identity image's sorted site (spacing search, tile shape 1)
   uint32_t *src_key, *src_rank, *mcount, *moff, *src_perm;
   NearGrid* grid;
   int* cells;
@@ -162,7 +165,7 @@ cudaError_t launch_median(int prec, Rows rows, int n, RelaxDev* st, unsigned int
 cudaError_t launch_move_fold(float4* q32, double4* q64, int n, int gid, int prec, Rows rows, double4* prev_f,
                              double4* prev_d, RelaxDev* st, int fixed, double radius, double step_scale, cudaStream_t s);
 cudaError_t launch_row_summary(Rows rows, int n, double* partials, double* near_partials, int* near_rows,
-                               RowSummary* out, cudaStream_t s);
+                               RowSummary* out, cudaStream_t s, bool nearest_only = false);
 cudaError_t launch_nearest_degrees(const double* nearest, int n, float* out, cudaStream_t s);
 cudaError_t launch_refine_nearest(const float4* q32, int n, int gid, Rows rows, bool near_sites, const uint32_t* scode,
                                   const uint32_t* simg, int* neighbour, cudaStream_t s);
