@@ -303,14 +303,14 @@ def batched_section(zo, samples=256, steps=50, dist=None):
             "timing": "wall clock of zo_batch_relax (all steps and closing passes), samples created beforehand"}
 
 
-def served_section(zo, device_rate, factors=(0.6, 1.0, 1.4), per_rate=200, plain_requests=20):
+def served_section(zo, device_rate, factors=(0.7, 1.4), per_rate=150, plain_requests=20):
     """Config 5: Poisson arrivals of relax+measure requests (group uniform, N log-uniform in
     [500, 1e6], steps uniform in [10, 200], all pairs below 5,000 orientations else
     neighbourhood 20), served by the continuous-batching loop in FP32-refined mode, at
-    rates below, near and above the GPU's capacity: capacity = the headline's device
+    rates below and above the GPU's capacity: capacity = the headline's device
     pair-evals/s over the mean pair evaluations of a request. `per_rate` requests per rate
     (p50 and p99 from that many latencies). The plain FP64 path serves a fixed subsample
-    (every k-th request of the capacity-rate stream) one at a time; both throughputs count
+    (every k-th request of the higher-rate stream) one at a time; both throughputs count
     pair evaluations as the reference does (relax steps and closing pass)."""
     from zxtalori_b200 import serve
 
