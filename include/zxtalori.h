@@ -68,9 +68,16 @@ const float* zo_point_values(void* h, uint32_t kind);
 /* src/exports.zig:69. bit 0 add the identity, bit 1 hold it fixed. */
 int zo_identity(void* h, uint32_t flags);
 
-/* src/exports.zig:45,88-120. Covering radius, meshes and covering optimisation are not part
- * of this engine: these return -1 (or NULL / 0) with an explanatory message. */
+/* src/exports.zig:45-48 (Engine.checkCovering, src/engine.zig:377-399): the covering
+ * radius, the largest empty cap of the sample's full orbit {+-q_j g_k} on S3, in SO(3)
+ * degrees, into stats (covering_radius_deg, covering_excess, mesh_ratio, covering_witness,
+ * covering_*), and point values kind 1 (each orientation's largest Delaunay cap, degrees)
+ * and kind 2 (its Voronoi cell's faces). Measured again only when the group, the float32
+ * orientations or the iteration changed since the last call (stats covering_cached).
+ * Fewer than 4 orientations: -1 ("Covering radius: TooFewOrientations"). */
 int zo_cover(void* h);
+/* src/exports.zig:88-120. The triangulation display and covering optimisation are not part
+ * of this engine: these return -1 (or NULL / 0) with an explanatory message. */
 int zo_cover_optimize(void* h, uint32_t steps, uint32_t mode, uint32_t finish, float floor_deg);
 int zo_cover_kicks(void* h, uint32_t patience, float progress, float size, float trust);
 int zo_mesh(void* h);
@@ -148,6 +155,11 @@ int zo_debug_pair_counts(void* h, double* out);
  * cancels). A pass that then produces more sites than that overflows, and the engine's
  * resize-and-redo path runs as after a real overflow (src/pairs.zig:391-394, near.zig:191-195). */
 int zo_debug_shell_capacity(void* h, uint32_t sites);
+/* Development hook (no reference counterpart): where zo_cover collects each orientation's
+ * neighbours: 0 by the sample's size (every image for small samples, else the chart grid),
+ * 1 every image, 2 the chart grid (when the grid's reach is narrow enough to build one).
+ * The result does not depend on it. */
+int zo_debug_cover_mode(void* h, uint32_t mode);
 /* Measurement hook (no reference counterpart): `steps` relaxation steps of the current
  * sample after `warmup`, each timed with CUDA events on the engine's stream and preceded,
  * outside its events, by a memset of flush_bytes (an L2 flush when larger than L2).

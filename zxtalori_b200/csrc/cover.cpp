@@ -1,0 +1,210 @@
+// The covering radius of a sample (src/engine.zig:377-399 checkCovering/measureCovering, the
+// stats keys of src/engine.zig:959-975): each source's star in the spherical Delaunay
+// triangulation of its orbit, built on the GPU (k_cover.cuh), and the largest empty cap over
+// all stars. Rounds: every source collects the orbit points within a reach expected to hold
+// kCoverTarget of them; a source whose star is not proven within its reach runs again with
+// the reach it reported, from the chart grid while the grid holds that reach, else from
+// every image.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.h"
+
+namespace zo {
+namespace {
+
+constexpr double kPiH = 3.14159265358979323846;
+constexpr double kCoverTarget = 48;         // expected orbit points within the first reach
+constexpr double kCoverDensePairs = 4e9;    // n * n * |K| up to which every image is scanned
+constexpr double kCoverGridRadius = 0.9;    // widest chart-grid reach (S3 angle)
+constexpr int kCoverRounds = 8;
+
+// The S3 angle of a cap holding `fraction` of the sphere: (phi - sin phi cos phi) / pi.
+double cap_angle(double fraction) {
+  double lo = 0, hi = kPiH;
+  for (int k = 0; k < 80; ++k) {
+    const double m = 0.5 * (lo + hi);
+    if ((m - std::sin(m) * std::cos(m)) / kPiH < fraction) lo = m;
+    else hi = m;
+  }
+  return 0.5 * (lo + hi);
+}
+double chord2_of(double angle) {
+  const double c = 2.0 * std::sin(0.5 * std::min(angle, kPiH));
+  return c * c;
+}
+double angle_of(double chord2) { return 2.0 * std::asin(std::min(1.0, 0.5 * std::sqrt(std::max(0.0, chord2)))); }
+
+}  // namespace
+
+double simplex_degrees(double count) {
+  static const double c[] = {1.889832101454757, 0.573930763512449, 0.581069217539205, 0.859789414116394,
+                             1.490131881944242, 2.791922498626376, 5.481645765756282, 11.12163594341394};
+  const double t = std::cbrt(1.0 / count);
+  double v = 0;
+  for (int i = 7; i >= 0; --i) v = c[i] + t * t * v;
+  return t * v * 360.0 / kPiH;
+}
+
+// FNV-1a over the group and the float32 orientations.
+uint64_t Engine::sample_key() const {
+  uint64_t h = 1469598103934665603ull ^ (uint64_t)group_;
+  const unsigned char* p = reinterpret_cast<const unsigned char*>(host_.data());
+  for (size_t k = 0, size = host_.size() * sizeof(float); k < size; ++k) h = (h ^ p[k]) * 1099511628211ull;
+  return h;
+}
+
+void Engine::cover() {
+  if (n_ < 4) throw Failure("TooFewOrientations");
+  ZO_CUDA(cudaSetDevice(device_));
+  cancelled_.store(false);
+  const uint64_t key = sample_key();
+  cover_cached_ = cover_ && cover_key_ == key && cover_iteration_ == iteration_ && point_covering_iteration_ &&
+                  *point_covering_iteration_ == iteration_;
+  if (cover_cached_) return;
+  measure_covering();
+  cover_key_ = key;
+}
+
+void Engine::measure_covering() {
+  const int n = (int)n_;
+  if (n >= (1 << 24)) throw Failure("TooManyOrientationsForCovering");
+  const int order = (int)this->order();
+  const double count_ext = 2.0 * order * n;
+  const double phi = cap_angle(std::min(0.5, kCoverTarget / count_ext));
+  const double reach2 = chord2_of(phi);
+  cover_alpha_.ensure((size_t)n * sizeof(double));
+  cover_centre_.ensure((size_t)n * sizeof(double4));
+  cover_faces_.ensure((size_t)n * 4);
+  cover_facets_.ensure((size_t)n * 4);
+  cover_status_.ensure((size_t)n * 4);
+  cover_need_.ensure((size_t)n * sizeof(double));
+  cover_list_.ensure((size_t)n * 4);
+  cover_probes_.ensure(sizeof(unsigned long long));
+  ZO_CUDA(cudaMemsetAsync(cover_probes_.as<void>(), 0, sizeof(unsigned long long), stream_));
+
+  CoverArgs A{};
+  A.q = q32();
+  A.n = n;
+  A.gid = group_;
+  A.alpha = cover_alpha_.as<double>();
+  A.centre = cover_centre_.as<double4>();
+  A.faces = cover_faces_.as<uint32_t>();
+  A.facets = cover_facets_.as<uint32_t>();
+  A.status = cover_status_.as<uint32_t>();
+  A.need2 = cover_need_.as<double>();
+  A.probes = cover_probes_.as<unsigned long long>();
+
+  // The chart grid, complete to a reach well past the first one (most second runs stay in it).
+  CoverResult r;
+  // Forced to the chart grid (a development mode), the grid's reach stays below the widths
+  // that the near field sums over every image for small samples.
+  const bool dense_first = cover_mode_ == 1 ||
+                           (cover_mode_ == 0 && ((double)n * n * order <= kCoverDensePairs || phi >= 0.3));
+  double grid_reach2 = 0;
+  if (!dense_first) {
+    const double radius = std::min(cover_mode_ == 2 ? 0.45 : kCoverGridRadius, 3.0 * phi);
+    const double d_r = mean_radius((double)n * order);
+    if (!cover_near_) cover_near_ = std::make_unique<NearField>(group_, radius / d_r);
+    else cover_near_->reconfigure(group_, radius / d_r);
+    if (cover_near_->structure(stream_, q32(), q64(), n, d_r, sms_)) {
+      grid_reach2 = chord2_of(cover_near_->radius());
+      A.scode = cover_near_->sorted_codes();
+      A.simg = cover_near_->sorted_images();
+      A.cell_off = cover_near_->cell_offsets();
+      A.grid = cover_near_->grid_device();
+      A.grid_reach2 = grid_reach2;
+      r.shell_points = (uint32_t)cover_near_->site_count(stream_);
+      if (cover_near_->overflowed(stream_)) throw Failure("NearShellTooLarge");
+    }
+  }
+  const NearGrid* grid = A.grid;
+
+  // Round 0: every source at the first reach.
+  A.reach2 = reach2;
+  A.reach2_of = nullptr;
+  A.list = nullptr;
+  A.count = n;
+  ZO_CUDA(launch_cover(A, sms_, stream_));
+  r.rounds = 1;
+  std::vector<uint32_t> status(n);
+  std::vector<double> need(n);
+  std::vector<double> used(n, reach2);  // the reach each source's star was built in
+  std::vector<uint32_t> again, grid_list, dense_list;
+  for (int round = 1;; ++round) {
+    ZO_CUDA(cudaMemcpyAsync(status.data(), A.status, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
+    ZO_CUDA(cudaMemcpyAsync(need.data(), A.need2, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    ZO_CUDA(cudaStreamSynchronize(stream_));
+    if (cancelled_.load()) throw Failure("Cancelled");
+    grid_list.clear();
+    dense_list.clear();
+    for (int i = 0; i < n; ++i) {
+      if (status[i] != kCoverShort && status[i] != kCoverSparse) continue;
+      const bool fits = grid && need[i] <= grid_reach2;
+      (fits ? grid_list : dense_list).push_back((uint32_t)i);
+      used[i] = need[i];
+    }
+    if ((grid_list.empty() && dense_list.empty()) || round == kCoverRounds) break;
+    // need2 holds each listed source's next reach: the kernel reads it before it writes.
+    A.reach2_of = A.need2;
+    const size_t g = grid_list.size();
+    std::vector<uint32_t>& all = again;
+    all.assign(grid_list.begin(), grid_list.end());
+    all.insert(all.end(), dense_list.begin(), dense_list.end());
+    ZO_CUDA(cudaMemcpyAsync(cover_list_.as<uint32_t>(), all.data(), all.size() * 4, cudaMemcpyHostToDevice, stream_));
+    if (g > 0) {
+      A.grid = grid;
+      A.list = cover_list_.as<uint32_t>();
+      A.count = (int)g;
+      ZO_CUDA(launch_cover(A, sms_, stream_));
+    }
+    if (!dense_list.empty()) {
+      A.grid = nullptr;
+      A.list = cover_list_.as<uint32_t>() + g;
+      A.count = (int)dense_list.size();
+      ZO_CUDA(launch_cover(A, sms_, stream_));
+    }
+    ++r.rounds;
+  }
+
+  // Results to the host: each source's largest cap and faces, the largest over all.
+  std::vector<double> alpha(n);
+  std::vector<uint32_t> faces(n), facets(n);
+  ZO_CUDA(cudaMemcpyAsync(alpha.data(), A.alpha, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaMemcpyAsync(faces.data(), A.faces, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaMemcpyAsync(facets.data(), A.facets, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
+  unsigned long long probes = 0;
+  ZO_CUDA(cudaMemcpyAsync(&probes, A.probes, sizeof probes, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  point_covering_.resize(n_);
+  point_faces_.resize(n_);
+  int top = 0;
+  double widest = 0;
+  for (int i = 0; i < n; ++i) {
+    if (status[i] != kCoverOk) ++r.unresolved;
+    else widest = std::max(widest, used[i]);
+    if (alpha[i] > alpha[top]) top = i;
+    point_covering_.data()[i] = (float)(2.0 * alpha[i] * 180.0 / kPiH);
+    point_faces_.data()[i] = (float)faces[i];
+    r.facets += facets[i];
+  }
+  double4 centre;
+  ZO_CUDA(cudaMemcpyAsync(&centre, A.centre + top, sizeof centre, cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+  r.radius_deg = 2.0 * alpha[top] * 180.0 / kPiH;
+  r.witness[0] = centre.x;
+  r.witness[1] = centre.y;
+  r.witness[2] = centre.z;
+  r.witness[3] = centre.w;
+  // A proven star's caps lie within its reach of its source: 2 a <= reach (S3), so every
+  // empty cap is at most the widest such reach, in SO(3) degrees (twice the S3 angle of a).
+  r.domain_bound_deg = std::max(r.radius_deg, angle_of(widest) * 180.0 / kPiH);
+  r.probes = probes;
+  cover_ = r;
+  cover_iteration_ = iteration_;
+  point_covering_iteration_ = iteration_;
+}
+
+}  // namespace zo

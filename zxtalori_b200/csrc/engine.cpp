@@ -332,6 +332,15 @@ void NearField::pass(cudaStream_t s, int prec, const float4* q32, const double4*
   ZO_CUDA(launch_near(make_launch(prec, q32, q64, n, track, out, nearest_only), s));
 }
 
+bool NearField::structure(cudaStream_t s, const float4* q32, const double4* q64, int n, double mean_r, int sms) {
+  if (!ready_ || n != n_ || prec_ != kFP32) setup(s, kFP32, q32, q64, n, mean_r, sms, kTilesRelax);
+  if (dense_) return false;
+  int launches = 0;
+  ZO_CUDA(launch_near_structure(make_launch(kFP32, q32, q64, n, false, Rows{}, false), s, &launches));
+  probe_count(launches);
+  return true;
+}
+
 bool NearField::pass_structure(cudaStream_t s, int prec, const float4* q32, const double4* q64, int n,
                                double mean_r, Rows out, int sms, NearTask* task) {
   if (prec != kFP32 || !ready_ || n != n_ || prec != prec_ || dense_) {
@@ -828,6 +837,9 @@ void Engine::fetch() {
 
 void Engine::reset_run() {
   point_separation_iteration_.reset();
+  point_covering_iteration_.reset();
+  cover_.reset();
+  cover_cached_ = false;
   relax_state_.reset();
   iteration_ = 0;
   step_deg_ = 0;
@@ -1395,6 +1407,11 @@ void Engine::bench_spacing(uint32_t passes, uint32_t warmup, double flush_bytes,
 }
 
 const float* Engine::point_values(uint32_t kind) const {
+  if (kind == 1 || kind == 2) {
+    const PinnedArray<float>& v = kind == 1 ? point_covering_ : point_faces_;
+    if (!point_covering_iteration_ || v.size() != n_) return nullptr;
+    return v.data();
+  }
   if (kind != 0 || !point_separation_iteration_ || point_separation_.size() != n_) return nullptr;
   return point_separation_.data();
 }
@@ -1483,11 +1500,40 @@ const char* Engine::stats() {
   else j.null("identity_index");
   j.integer("base_count", base_count_);
   j.integer("inserted_count", 0);
-  j.str("triangulation_backend", "none");
-  j.null("covering_radius_deg");
-  j.boolean("covering_current", false);
-  j.null("mesh_ratio");
-  j.null("covering_excess");
+  j.str("triangulation_backend", "cuda");
+  const double count_ext = 2.0 * order() * n_;
+  const std::optional<double> bound = n_ > 0 ? std::optional<double>(simplex_degrees(count_ext)) : std::nullopt;
+  const bool covering_current = cover_ && cover_iteration_ == iteration_;
+  j.opt("simplex_bound_deg", bound);
+  j.opt("covering_excess", cover_ && bound ? finite(cover_->radius_deg / *bound - 1.0) : std::nullopt);
+  j.opt("mesh_ratio", covering_current && current && m->separation_deg > 0
+                          ? finite(cover_->radius_deg / m->separation_deg)
+                          : std::nullopt);
+  j.opt("covering_radius_deg", cover_ ? finite(cover_->radius_deg) : std::nullopt);
+  j.boolean("covering_current", covering_current);
+  j.boolean("covering_cached", cover_cached_);
+  if (cover_) {
+    j.integer("covering_unresolved_caps", cover_->unresolved);
+    j.integer("covering_iteration", cover_iteration_);
+    j.key("covering_witness");
+    char b[160];
+    std::snprintf(b, sizeof b, "[%.9g,%.9g,%.9g,%.9g]", cover_->witness[0], cover_->witness[1], cover_->witness[2],
+                  cover_->witness[3]);
+    j.s += b;
+    j.opt("covering_domain_bound_deg", finite(cover_->domain_bound_deg));
+    j.integer("covering_shell_points", cover_->shell_points);
+    j.null("covering_fence_points");
+    j.integer("covering_tetrahedra", (long long)(cover_->facets / 4));
+    j.integer("covering_certificate_probes", (long long)cover_->probes);
+    j.null("covering_exact_predicates");
+    j.integer("covering_rounds", cover_->rounds);
+  } else {
+    for (const char* k : {"covering_unresolved_caps", "covering_iteration", "covering_witness",
+                          "covering_domain_bound_deg", "covering_shell_points", "covering_fence_points",
+                          "covering_tetrahedra", "covering_certificate_probes", "covering_exact_predicates",
+                          "covering_rounds"})
+      j.null(k);
+  }
   j.boolean("measured", m.has_value());
   j.boolean("measures_current", current);
   if (m) j.integer("measures_iteration", measure_iteration_);
@@ -1497,7 +1543,8 @@ const char* Engine::stats() {
   else j.null("relax_neighbourhood");
   if (point_separation_iteration_) j.integer("point_separation_iteration", *point_separation_iteration_);
   else j.null("point_separation_iteration");
-  j.null("point_covering_iteration");
+  if (point_covering_iteration_) j.integer("point_covering_iteration", *point_covering_iteration_);
+  else j.null("point_covering_iteration");
   if (m && measure_neighbourhood_ > 0) j.num("energy_neighbourhood", measure_neighbourhood_);
   else j.null("energy_neighbourhood");
   j.integer("ratio_limit", ratio_limit());

@@ -104,6 +104,18 @@ struct Measures {
   double quey_energy = NAN, separation_deg = NAN, force_rms = NAN;
 };
 
+// A covering pass's result (the reference's covering.Result, src/covering.zig).
+struct CoverResult {
+  double radius_deg = NAN;         // largest empty cap of the orbit, SO(3) degrees
+  double witness[4] = {1, 0, 0, 0};  // its centre (a unit quaternion of the orbit's image space)
+  double domain_bound_deg = NAN;   // every empty cap is at most this: the widest reach a star was proven in
+  uint32_t unresolved = 0;         // sources whose star could not be proven exact
+  uint64_t facets = 0;             // star facets over all sources
+  uint64_t probes = 0;             // pivots evaluated
+  uint32_t rounds = 0;             // collection rounds (sources with a short reach run again)
+  uint32_t shell_points = 0;       // shell sites of the chart grid the stars were collected from (0: every image)
+};
+
 struct StepResult {
   double max_step_deg = 0, force_rms = 0, energy = 0;
 };
@@ -157,6 +169,12 @@ class NearField {
   // Whether the last pass produced more sites than the workspace holds (after a sync);
   // the next pass sizes it again.
   bool overflowed(cudaStream_t s);
+  // The shell, chart grid and site order of the float32 positions q32 without a gather (the
+  // covering pass walks them itself); false when the cutoff takes the dense path (no grid).
+  // Sizes the workspace first when it is not ready for n FP32 sources.
+  bool structure(cudaStream_t s, const float4* q32, const double4* q64, int n, double mean_radius, int sms);
+  const uint32_t* cell_offsets() const { return cell_off_.as<uint32_t>(); }
+  const NearGrid* grid_device() const { return grid_.as<NearGrid>(); }
   const uint32_t* sorted_codes() const { return scode_.as<uint32_t>(); }
   const uint32_t* sorted_images() const { return simg_.as<uint32_t>(); }
   int capacity() const { return capacity_; }
@@ -313,6 +331,9 @@ class Engine {
   void generate_grid(int gid, uint32_t freq, uint32_t target, uint32_t seed, uint32_t kind);
   void measure();
   void spacing();
+  // The covering radius on request (src/engine.zig:377-399): measured again only when the
+  // sample (group and float32 orientations) or the iteration has changed since the last one.
+  void cover();
   void relax(uint32_t steps);
   void set_neighbourhood(double delta);
   void identity(bool add, bool fixed);
@@ -369,6 +390,13 @@ class Engine {
   // Development: the next near-field pass (of the relaxation and of the spacing pass) sizes
   // its workspace for only `sites` shell sites, once; 0 cancels.
   void debug_shell_capacity(uint32_t sites) { shell_override_ = sites; }
+  // Development: where the covering pass collects neighbours (0 by size, 1 every image, 2
+  // the chart grid); the result does not depend on it.
+  void debug_cover_mode(uint32_t mode) {
+    if (mode > 2) throw Failure("UnknownCoverMode");
+    cover_mode_ = (int)mode;
+    cover_.reset();
+  }
   // The spacing pass's first-walk fraction of the cutoff, instead of the tile table's (0:
   // the table's); the result does not depend on it, only the time.
   void force_walk(double fraction);
@@ -490,6 +518,19 @@ class Engine {
   bool fix_identity_ = false;
   std::optional<uint32_t> fixed_index_;
   double budget_scale_ = 1.0;
+  // Covering.
+  std::optional<CoverResult> cover_;
+  int cover_mode_ = 0;
+  uint32_t cover_iteration_ = 0;
+  uint64_t cover_key_ = 0;
+  bool cover_cached_ = false;
+  uint64_t sample_key() const;
+  void measure_covering();
+  PinnedArray<float> point_covering_, point_faces_;
+  std::optional<uint32_t> point_covering_iteration_;
+  DeviceBuffer cover_alpha_, cover_centre_, cover_faces_, cover_facets_, cover_status_, cover_need_, cover_list_,
+      cover_probes_;
+  std::unique_ptr<NearField> cover_near_;
   // Full-measure scratch.
   RowBuffers full_rows_, full_partial_;
   DeviceBuffer full_extra_, full_pextra_, full_degen_, full_pdegen_;
@@ -497,5 +538,8 @@ class Engine {
 };
 
 double mean_radius(double count);
+// Simplex bound on the covering radius of `count` points on S3 (images and antipodes
+// included), SO(3) degrees (src/covering_reference.zig:4-15).
+double simplex_degrees(double count);
 
 }  // namespace zo

@@ -34,8 +34,9 @@ int fail(void* h, const char* message) {
   return -1;
 }
 
-// Covering, meshes and exact-count generation are outside this engine.
-const char* kNoCovering = "covering radius, triangulation and covering optimisation are not part of this engine";
+// Covering optimisation, the triangulation display and exact-count generation are outside
+// this engine (the covering radius is in it).
+const char* kNoCovering = "the triangulation display and covering optimisation are not part of this engine";
 }  // namespace
 
 extern "C" {
@@ -101,7 +102,7 @@ int zo_identity(void* h, uint32_t flags) {
   return guarded(h, "Identity constraint", [&](Engine& e) { e.identity((flags & 1u) != 0, (flags & 2u) != 0); });
 }
 
-int zo_cover(void* h) { return fail(h, (std::string("Covering radius: ") + kNoCovering).c_str()); }
+int zo_cover(void* h) { return guarded(h, "Covering radius", [](Engine& e) { e.cover(); }); }
 int zo_cover_optimize(void* h, uint32_t steps, uint32_t mode, uint32_t finish, float floor_deg) {
   (void)steps, (void)mode, (void)finish, (void)floor_deg;
   return fail(h, (std::string("Covering optimization: ") + kNoCovering).c_str());
@@ -186,6 +187,10 @@ int zo_spacing_exact(void* h, uint32_t* out) {
 
 int zo_debug_shell_capacity(void* h, uint32_t sites) {
   return guarded(h, "Rows", [&](Engine& e) { e.debug_shell_capacity(sites); });
+}
+
+int zo_debug_cover_mode(void* h, uint32_t mode) {
+  return guarded(h, "Covering radius", [&](Engine& e) { e.debug_cover_mode(mode); });
 }
 
 int zo_debug_pair_counts(void* h, double* out) {

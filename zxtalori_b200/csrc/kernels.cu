@@ -4,6 +4,7 @@
 //   k_full.cuh   full pair measures (Riesz, Green, log)
 //   k_near.cuh   near-field shell, chart-grid sorts and gather
 //   k_relax.cuh  BB step, median, move+fold, row summaries
+//   k_cover.cuh  covering radius: per-source Delaunay stars
 #include <cuda_runtime.h>
 
 #include "qvm_shared.h"
@@ -12,6 +13,7 @@
 #include "k_full.cuh"
 #include "k_near.cuh"
 #include "k_relax.cuh"
+#include "k_cover.cuh"
 
 namespace zo {
 
@@ -60,6 +62,20 @@ cudaError_t launch_nearest_degrees(const double* nearest, int n, float* out, cud
 cudaError_t launch_refine_nearest(const float4* q32, int n, int gid, Rows rows, bool near_sites, const uint32_t* scode,
                                   const uint32_t* simg, int* neighbour, cudaStream_t s) {
   k_refine_nearest<<<(n + 255) / 256, 256, 0, s>>>(q32, n, gid, rows, near_sites ? 1 : 0, scode, simg, neighbour);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s) {
+  const int count = A.list ? A.count : A.n;
+  if (count <= 0) return cudaSuccess;
+  if (A.n >= (1 << 24)) return cudaErrorInvalidValue;  // point keys hold the source in 24 bits
+  const size_t smem = kCoverWarps * sizeof(CoverWarp);
+  cudaError_t e = cudaFuncSetAttribute(k_cover_star, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // Warps loop over the sources: a few resident blocks per SM.
+  const int blocks = std::max(1, std::min((count + kCoverWarps - 1) / kCoverWarps, 4 * sms));
+  k_cover_star<<<blocks, kCoverWarps * 32, smem, s>>>(A);
+  probe_count();
   return cudaGetLastError();
 }
 

@@ -157,6 +157,39 @@ cudaError_t launch_shell_count(int prec, const float4* q32, const double4* q64, 
                                uint32_t* counts, uint32_t* offsets, uint32_t* scan_tmp, uint4* masks,
                                uint32_t* rim_list, float4* rim_q, uint32_t* rim_count, cudaStream_t s);
 
+// Covering pass (k_cover.cuh): each listed source's star in the spherical Delaunay
+// triangulation of the orbit, gift-wrapped in FP64 over the orbit points within a reach.
+enum CoverStatus : uint32_t {
+  kCoverOk = 0,        // the star is exact (every cap within the reach)
+  kCoverShort = 1,     // some cap reaches past the reach: run again with need2
+  kCoverCrowded = 2,   // more points than a star holds even after shrinking the reach
+  kCoverStarFull = 3,  // more facets than a star holds
+  kCoverSparse = 4,    // too few points to close a star: run again with need2 (wider)
+};
+struct CoverArgs {
+  const float4* q;  // the float32 sample
+  int n, gid;
+  // Grid collection: the near-field structure's sorted sites and chart grid, complete to
+  // the squared chord grid_reach2; grid == null: every image (dense).
+  const uint32_t* scode;
+  const uint32_t* simg;
+  const uint32_t* cell_off;
+  const NearGrid* grid;
+  double grid_reach2;
+  double reach2;            // squared chord of the reach, or per source:
+  const double* reach2_of;  // (null: reach2 for all)
+  const uint32_t* list;     // the sources to build (null: 0 .. n-1)
+  int count;                // listed sources
+  double* alpha;            // per source: largest cap of its star (S3 angle, rad)
+  double4* centre;          // that cap's centre
+  uint32_t* faces;          // distinct neighbours its star touches
+  uint32_t* facets;         // facets of its star
+  uint32_t* status;         // CoverStatus
+  double* need2;            // squared chord of the reach a second run needs (else 0)
+  unsigned long long* probes;  // pivots evaluated (added to; may be null)
+};
+cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s);
+
 // Relaxation step pieces.
 cudaError_t launch_relax_stats(Rows rows, const double4* prev_f, const double4* prev_d, int n, int fixed,
                                double* partials, RelaxDev* st, cudaStream_t s);
