@@ -76,10 +76,16 @@ int zo_identity(void* h, uint32_t flags);
  * orientations or the iteration changed since the last call (stats covering_cached).
  * Fewer than 4 orientations: -1 ("Covering radius: TooFewOrientations"). */
 int zo_cover(void* h);
-/* src/exports.zig:88-120. The triangulation display and covering optimisation are not part
- * of this engine: these return -1 (or NULL / 0) with an explanatory message. */
+/* src/exports.zig:104-120. Covering optimisation is not part of this engine: these return
+ * -1 with an explanatory message. */
 int zo_cover_optimize(void* h, uint32_t steps, uint32_t mode, uint32_t finish, float floor_deg);
 int zo_cover_kicks(void* h, uint32_t patience, float progress, float size, float trust);
+/* src/exports.zig:88-103 (the triangulation display): zo_mesh brings the covering up to date
+ * (zo_cover) and assembles every orientation's Delaunay star into one mesh; the vertices are
+ * 4 floats each, stereographic (x, y, z) / (1 + w) of the orbit points and 0, the
+ * orientations first (vertex i is orientation i), then every other orbit point a star
+ * touches; the tetrahedra are 4 vertex indices each, every hull facet that touches an
+ * orientation once. Engine-owned, valid until the next zo_mesh (NULL / 0 before one). */
 int zo_mesh(void* h);
 const float* zo_mesh_vertices(void* h);
 const uint32_t* zo_mesh_tets(void* h);

@@ -156,3 +156,39 @@ def test_covering_at_the_headline_size(engine):
     assert np.array_equal(near_cov, dense_cov) and np.array_equal(near_faces, dense_faces)
     assert 13 < near_faces.mean() < 17
     assert near["covering_domain_bound_deg"] >= near["covering_radius_deg"] > near["simplex_bound_deg"]
+
+
+def test_actual_shell_mesh_export(engine):
+    """The reference's tests/test_explorer.py:17-23, mirrored (Hopf grid instead of the FCC
+    transport, which this engine does not build)."""
+    with engine.generate("O", h=2) as grid:
+        mesh = grid.triangulation()
+        assert len(mesh["stereographic"]) >= len(grid)
+        assert len(mesh["tetrahedra"]) > 0
+        assert mesh["tetrahedra"].max() < len(mesh["stereographic"])
+        assert grid.stats["covering_current"]
+
+
+@pytest.mark.parametrize("group,count", [("O", 300), ("D6", 250)])
+def test_mesh_is_the_hull_around_the_zone(engine, group, count):
+    """Every tetrahedron of the exported mesh is a facet of the orbit's convex hull that
+    touches an orientation's identity image, and every such facet is exported once; the
+    vertices are the orbit points' stereographic coordinates, the orientations first."""
+    from scipy.spatial import ConvexHull, cKDTree
+
+    with engine.haar(group, count, 5) as grid:
+        grid.relax(30)
+        mesh = grid.triangulation()
+        q = grid.quaternions.astype(np.float64)
+        ops = grid.operations.astype(np.float64)
+    points, _ = cov.orbit(q, ops)
+    chart = points[:, 1:] / (1 + points[:, :1])
+    tree = cKDTree(chart)
+    distance, index = tree.query(mesh["stereographic"].astype(np.float64))
+    assert distance.max() < 1e-5
+    assert np.array_equal(index[:count], np.arange(count))
+    exported = {tuple(sorted(index[t])) for t in mesh["tetrahedra"]}
+    assert len(exported) == len(mesh["tetrahedra"])
+    hull = ConvexHull(points)
+    around = {tuple(sorted(s)) for s in hull.simplices if (s < count).any()}
+    assert exported == around

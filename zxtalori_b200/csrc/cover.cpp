@@ -8,6 +8,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "engine.h"
@@ -205,6 +207,131 @@ void Engine::measure_covering() {
   cover_ = r;
   cover_iteration_ = iteration_;
   point_covering_iteration_ = iteration_;
+  cover_reach_ = std::move(used);
+  cover_facet_counts_ = std::move(facets);
+  cover_grid_reach2_ = grid ? grid_reach2 : 0.0;
+}
+
+// The triangulation display (src/exports.zig:88-103, Engine.buildMesh): the stars of every
+// source as one mesh. The covering is brought up to date first; each source's star is built
+// again, in the reach that proved it, and written out as tetrahedra of point keys; the host
+// numbers the points (the sources first, as their own vertices 0 .. n-1, then every other
+// orbit point a star touches) and keeps each tetrahedron once. Vertices are stereographic
+// (x, y, z) / (1 + w) of the unit orbit point, fourth component 0.
+void Engine::build_mesh() {
+  cover();
+  const int n = (int)n_;
+  if (cover_reach_.size() != (size_t)n || cover_facet_counts_.size() != (size_t)n) throw Failure("CoveringNotMeasured");
+  std::vector<uint32_t> offset(n + 1, 0);
+  uint64_t total = 0;
+  for (int i = 0; i < n; ++i) {
+    offset[i] = (uint32_t)total;
+    total += cover_facet_counts_[i];
+    if (total > (1ull << 31)) throw Failure("MeshTooLarge");
+  }
+  offset[n] = (uint32_t)total;
+  cover_mesh_.ensure(std::max<uint64_t>(total, 1) * sizeof(uint4));
+  cover_mesh_offset_.ensure((size_t)(n + 1) * 4);
+  cover_need_.ensure((size_t)n * sizeof(double));
+  ZO_CUDA(cudaMemcpyAsync(cover_mesh_offset_.as<uint32_t>(), offset.data(), (size_t)(n + 1) * 4,
+                          cudaMemcpyHostToDevice, stream_));
+  ZO_CUDA(cudaMemcpyAsync(cover_need_.as<double>(), cover_reach_.data(), (size_t)n * sizeof(double),
+                          cudaMemcpyHostToDevice, stream_));
+  ZO_CUDA(cudaMemsetAsync(cover_mesh_.as<void>(), 0xff, std::max<uint64_t>(total, 1) * sizeof(uint4), stream_));
+  CoverArgs A{};
+  A.q = q32();
+  A.n = n;
+  A.gid = group_;
+  A.alpha = cover_alpha_.as<double>();
+  A.centre = cover_centre_.as<double4>();
+  A.faces = cover_faces_.as<uint32_t>();
+  A.facets = cover_facets_.as<uint32_t>();
+  A.status = cover_status_.as<uint32_t>();
+  A.need2 = cover_need_.as<double>();
+  A.reach2_of = cover_need_.as<double>();
+  A.mesh = cover_mesh_.as<uint4>();
+  A.mesh_offset = cover_mesh_offset_.as<uint32_t>();
+  // Each source from the chart grid when its reach is within the grid's (the grid of the
+  // covering pass, built for these positions), else from every image.
+  std::vector<uint32_t> grid_list, dense_list;
+  for (int i = 0; i < n; ++i)
+    (cover_grid_reach2_ > 0 && cover_reach_[i] <= cover_grid_reach2_ ? grid_list : dense_list).push_back((uint32_t)i);
+  std::vector<uint32_t> all(grid_list);
+  all.insert(all.end(), dense_list.begin(), dense_list.end());
+  cover_list_.ensure((size_t)n * 4);
+  ZO_CUDA(cudaMemcpyAsync(cover_list_.as<uint32_t>(), all.data(), all.size() * 4, cudaMemcpyHostToDevice, stream_));
+  if (!grid_list.empty()) {
+    A.scode = cover_near_->sorted_codes();
+    A.simg = cover_near_->sorted_images();
+    A.cell_off = cover_near_->cell_offsets();
+    A.grid = cover_near_->grid_device();
+    A.grid_reach2 = cover_grid_reach2_;
+    A.list = cover_list_.as<uint32_t>();
+    A.count = (int)grid_list.size();
+    ZO_CUDA(launch_cover(A, sms_, stream_));
+  }
+  if (!dense_list.empty()) {
+    A.grid = nullptr;
+    A.list = cover_list_.as<uint32_t>() + grid_list.size();
+    A.count = (int)dense_list.size();
+    ZO_CUDA(launch_cover(A, sms_, stream_));
+  }
+  std::vector<uint4> tets(total);
+  if (total)
+    ZO_CUDA(cudaMemcpyAsync(tets.data(), A.mesh, total * sizeof(uint4), cudaMemcpyDeviceToHost, stream_));
+  ZO_CUDA(cudaStreamSynchronize(stream_));
+
+  // Points: the sources first, then the other keys in order of first use.
+  std::unordered_map<uint32_t, uint32_t> index;
+  std::vector<uint32_t> keys;
+  keys.reserve((size_t)n * 2);
+  for (int i = 0; i < n; ++i) {
+    index.emplace((uint32_t)i << 8, (uint32_t)i);
+    keys.push_back((uint32_t)i << 8);
+  }
+  auto vertex = [&](uint32_t key) {
+    auto it = index.find(key);
+    if (it != index.end()) return it->second;
+    const uint32_t v = (uint32_t)keys.size();
+    index.emplace(key, v);
+    keys.push_back(key);
+    return v;
+  };
+  // Each tetrahedron once: its sorted vertex numbers as two 64-bit words.
+  struct PairHash {
+    size_t operator()(const std::pair<uint64_t, uint64_t>& k) const {
+      return (size_t)(k.first * 0x9E3779B97F4A7C15ull ^ (k.second + 0x632BE59BD9B4E019ull) * 0xC2B2AE3D27D4EB4Full);
+    }
+  };
+  std::unordered_set<std::pair<uint64_t, uint64_t>, PairHash> seen;
+  mesh_tets_.clear();
+  for (const uint4& t : tets) {
+    if (t.x == 0xffffffffu || t.y == 0xffffffffu) continue;  // a star the export did not reproduce
+    uint32_t v[4] = {vertex(t.x), vertex(t.y), vertex(t.z), vertex(t.w)};
+    std::sort(v, v + 4);
+    if (!seen.insert({((uint64_t)v[0] << 32) | v[1], ((uint64_t)v[2] << 32) | v[3]}).second) continue;
+    mesh_tets_.insert(mesh_tets_.end(), v, v + 4);
+  }
+  const float* ops = host_ops32(group_);
+  mesh_vertices_.assign(keys.size() * 4, 0.f);
+  for (size_t k = 0; k < keys.size(); ++k) {
+    const uint32_t j = keys[k] >> 8, im = keys[k] & 0xffu;
+    const float* p = &host_[(size_t)j * 4];
+    double a[4] = {p[0], p[1], p[2], p[3]};
+    if (im >> 1) {
+      const float* g = ops + 4 * (im >> 1);
+      const double b[4] = {g[0], g[1], g[2], g[3]};
+      const double w = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+      const double x = a[0] * b[1] + b[0] * a[1] + a[2] * b[3] - a[3] * b[2];
+      const double y = a[0] * b[2] + b[0] * a[2] + a[3] * b[1] - a[1] * b[3];
+      const double z = a[0] * b[3] + b[0] * a[3] + a[1] * b[2] - a[2] * b[1];
+      a[0] = w, a[1] = x, a[2] = y, a[3] = z;
+    }
+    const double norm = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
+    const double sign = (im & 1u) ? -1.0 : 1.0;
+    const double s = 1.0 / (1.0 + sign * a[0] / norm);
+    for (int c = 0; c < 3; ++c) mesh_vertices_[k * 4 + c] = (float)(sign * a[c + 1] / norm * s);
+  }
 }
 
 }  // namespace zo

@@ -334,6 +334,11 @@ class Engine {
   // The covering radius on request (src/engine.zig:377-399): measured again only when the
   // sample (group and float32 orientations) or the iteration has changed since the last one.
   void cover();
+  // The triangulation display (src/engine.zig buildMesh): every source's star as one mesh of
+  // stereographic vertices (4 floats each, the sources first) and tetrahedra (4 indices).
+  void build_mesh();
+  const std::vector<float>& mesh_vertices() const { return mesh_vertices_; }
+  const std::vector<uint32_t>& mesh_tets() const { return mesh_tets_; }
   void relax(uint32_t steps);
   void set_neighbourhood(double delta);
   void identity(bool add, bool fixed);
@@ -531,6 +536,14 @@ class Engine {
   DeviceBuffer cover_alpha_, cover_centre_, cover_faces_, cover_facets_, cover_status_, cover_need_, cover_list_,
       cover_probes_;
   std::unique_ptr<NearField> cover_near_;
+  // Of the last covering pass: the reach each source's star was proven in, its facet count,
+  // and the reach its chart grid holds (0: no grid).
+  std::vector<double> cover_reach_;
+  std::vector<uint32_t> cover_facet_counts_;
+  double cover_grid_reach2_ = 0;
+  DeviceBuffer cover_mesh_, cover_mesh_offset_;
+  std::vector<float> mesh_vertices_;
+  std::vector<uint32_t> mesh_tets_;
   // Full-measure scratch.
   RowBuffers full_rows_, full_partial_;
   DeviceBuffer full_extra_, full_pextra_, full_degen_, full_pdegen_;

@@ -34,9 +34,9 @@ int fail(void* h, const char* message) {
   return -1;
 }
 
-// Covering optimisation, the triangulation display and exact-count generation are outside
-// this engine (the covering radius is in it).
-const char* kNoCovering = "the triangulation display and covering optimisation are not part of this engine";
+// Covering optimisation and exact-count generation are outside this engine (the covering
+// radius and the triangulation display are in it).
+const char* kNoCovering = "covering optimisation is not part of this engine";
 }  // namespace
 
 extern "C" {
@@ -111,23 +111,17 @@ int zo_cover_kicks(void* h, uint32_t patience, float progress, float size, float
   (void)patience, (void)progress, (void)size, (void)trust;
   return fail(h, (std::string("Covering kicks: ") + kNoCovering).c_str());
 }
-int zo_mesh(void* h) { return fail(h, (std::string("DT display: ") + kNoCovering).c_str()); }
+int zo_mesh(void* h) { return guarded(h, "DT display", [](Engine& e) { e.build_mesh(); }); }
 const float* zo_mesh_vertices(void* h) {
-  (void)h;
-  return nullptr;
+  const auto& v = static_cast<Engine*>(h)->mesh_vertices();
+  return v.empty() ? nullptr : v.data();
 }
 const uint32_t* zo_mesh_tets(void* h) {
-  (void)h;
-  return nullptr;
+  const auto& t = static_cast<Engine*>(h)->mesh_tets();
+  return t.empty() ? nullptr : t.data();
 }
-uint32_t zo_mesh_vertex_count(void* h) {
-  (void)h;
-  return 0;
-}
-uint32_t zo_mesh_tet_count(void* h) {
-  (void)h;
-  return 0;
-}
+uint32_t zo_mesh_vertex_count(void* h) { return (uint32_t)(static_cast<Engine*>(h)->mesh_vertices().size() / 4); }
+uint32_t zo_mesh_tet_count(void* h) { return (uint32_t)(static_cast<Engine*>(h)->mesh_tets().size() / 4); }
 
 const char* zo_stats(void* h) { return static_cast<Engine*>(h)->stats(); }
 const char* zo_error(void* h) { return static_cast<Engine*>(h)->err; }

@@ -255,7 +255,10 @@ __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs
       }
       __syncwarp();
       for (int u = 0; u < kCoverMax / 32; ++u)
-        if (lane + 32 * u < count) W.d[rank[u]] = sub4d(cover_point(A.q, ops, mine[u]), x);
+        if (lane + 32 * u < count) {
+          W.d[rank[u]] = sub4d(cover_point(A.q, ops, mine[u]), x);
+          if (A.mesh) W.key[rank[u]] = mine[u];  // every lane has read the keys (the sync above)
+        }
       if (lane < kCoverMax / 32) W.used[lane] = 0u;
       __syncwarp();
       // 2. A first facet: from the tangent hyperplane (n = x) pivot towards the nearest
@@ -367,6 +370,15 @@ __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs
       }
       nfacets = tail;
       __syncwarp();
+      // Export (zo_mesh): each facet as the tetrahedron (x, y_a, y_b, y_c) of point keys, in
+      // the slots the host set aside for this source (its facet count from the covering pass).
+      if (A.mesh && status == kCoverOk) {
+        const uint32_t first = A.mesh_offset[i], room = A.mesh_offset[i + 1] - first;
+        for (int t = lane; t < tail && t < (int)room; t += 32) {
+          const uint32_t f = W.facet[t];
+          A.mesh[first + t] = make_uint4(i << 8, W.key[f & 0xffu], W.key[(f >> 8) & 0xffu], W.key[(f >> 16) & 0xffu]);
+        }
+      }
       if (lane < kCoverMax / 32) faces = __popc(W.used[lane]);
       for (int o = 4; o; o >>= 1) faces += __shfl_xor_sync(full, faces, o);
       faces = __shfl_sync(full, faces, 0);

@@ -187,6 +187,10 @@ struct CoverArgs {
   uint32_t* status;         // CoverStatus
   double* need2;            // squared chord of the reach a second run needs (else 0)
   unsigned long long* probes;  // pivots evaluated (added to; may be null)
+  // Export of the stars (null: none): source i writes its facets as (x, y_a, y_b, y_c) point
+  // keys ((source << 8) | image) into mesh[mesh_offset[i] .. mesh_offset[i + 1]).
+  uint4* mesh;
+  const uint32_t* mesh_offset;
 };
 cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s);
 
