@@ -41,7 +41,10 @@ void zo_destroy(void* h);
 
 /* src/exports.zig:9. Inverse Hopf product grids (kind 0/1); transports (kind 2). */
 int zo_generate(void* h, uint32_t group, uint32_t freq, uint32_t target, uint32_t seed, uint32_t kind);
-/* src/exports.zig:16. Exact-count insertion needs the covering triangulation: returns -1. */
+/* src/exports.zig:16-22 (Engine.generateExact): exactly `target` (32 .. 1,000,000)
+ * orientations: the inverse-Hopf grid with the largest count within the target, then points
+ * at the centres of the largest empty Delaunay caps. flags bit 0 adds the identity; bits
+ * 8-15 the grid kind (2, transport: -1, "TransportNotAvailable"). */
 int zo_generate_exact(void* h, uint32_t group, uint32_t target, uint32_t flags);
 /* src/exports.zig:83. Seeded Haar-uniform sample folded into the zone (shaders/haar.wgsl). */
 int zo_random(void* h, uint32_t group, uint32_t count, uint32_t seed);

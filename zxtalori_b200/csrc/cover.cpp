@@ -212,13 +212,10 @@ void Engine::measure_covering() {
   cover_grid_reach2_ = grid ? grid_reach2 : 0.0;
 }
 
-// The triangulation display (src/exports.zig:88-103, Engine.buildMesh): the stars of every
-// source as one mesh. The covering is brought up to date first; each source's star is built
-// again, in the reach that proved it, and written out as tetrahedra of point keys; the host
-// numbers the points (the sources first, as their own vertices 0 .. n-1, then every other
-// orbit point a star touches) and keeps each tetrahedron once. Vertices are stereographic
-// (x, y, z) / (1 + w) of the unit orbit point, fourth component 0.
-void Engine::build_mesh() {
+// Every source's star again, in the reach that proved it, written out as tetrahedra of point
+// keys ((source << 8) | image; the source first) with each facet's unit normal (its cap's
+// centre). The covering is brought up to date first.
+void Engine::export_stars(std::vector<uint4>& tets, std::vector<double4>& normals) {
   cover();
   const int n = (int)n_;
   if (cover_reach_.size() != (size_t)n || cover_facet_counts_.size() != (size_t)n) throw Failure("CoveringNotMeasured");
@@ -230,14 +227,16 @@ void Engine::build_mesh() {
     if (total > (1ull << 31)) throw Failure("MeshTooLarge");
   }
   offset[n] = (uint32_t)total;
-  cover_mesh_.ensure(std::max<uint64_t>(total, 1) * sizeof(uint4));
+  const uint64_t slots = std::max<uint64_t>(total, 1);
+  cover_mesh_.ensure(slots * sizeof(uint4));
+  cover_mesh_normal_.ensure(slots * sizeof(double4));
   cover_mesh_offset_.ensure((size_t)(n + 1) * 4);
   cover_need_.ensure((size_t)n * sizeof(double));
   ZO_CUDA(cudaMemcpyAsync(cover_mesh_offset_.as<uint32_t>(), offset.data(), (size_t)(n + 1) * 4,
                           cudaMemcpyHostToDevice, stream_));
   ZO_CUDA(cudaMemcpyAsync(cover_need_.as<double>(), cover_reach_.data(), (size_t)n * sizeof(double),
                           cudaMemcpyHostToDevice, stream_));
-  ZO_CUDA(cudaMemsetAsync(cover_mesh_.as<void>(), 0xff, std::max<uint64_t>(total, 1) * sizeof(uint4), stream_));
+  ZO_CUDA(cudaMemsetAsync(cover_mesh_.as<void>(), 0xff, slots * sizeof(uint4), stream_));
   CoverArgs A{};
   A.q = q32();
   A.n = n;
@@ -251,6 +250,7 @@ void Engine::build_mesh() {
   A.reach2_of = cover_need_.as<double>();
   A.mesh = cover_mesh_.as<uint4>();
   A.mesh_offset = cover_mesh_offset_.as<uint32_t>();
+  A.mesh_normal = cover_mesh_normal_.as<double4>();
   // Each source from the chart grid when its reach is within the grid's (the grid of the
   // covering pass, built for these positions), else from every image.
   std::vector<uint32_t> grid_list, dense_list;
@@ -276,11 +276,44 @@ void Engine::build_mesh() {
     A.count = (int)dense_list.size();
     ZO_CUDA(launch_cover(A, sms_, stream_));
   }
-  std::vector<uint4> tets(total);
-  if (total)
+  tets.resize(total);
+  normals.resize(total);
+  if (total) {
     ZO_CUDA(cudaMemcpyAsync(tets.data(), A.mesh, total * sizeof(uint4), cudaMemcpyDeviceToHost, stream_));
+    ZO_CUDA(cudaMemcpyAsync(normals.data(), A.mesh_normal, total * sizeof(double4), cudaMemcpyDeviceToHost, stream_));
+  }
   ZO_CUDA(cudaStreamSynchronize(stream_));
+}
 
+// The orbit point of `key` ((source << 8) | 2 operator + sign), unit, FP64, from the float32
+// sample and the float32 operator table (the kernels' definition).
+void Engine::orbit_point(uint32_t key, double out[4]) const {
+  const uint32_t j = key >> 8, im = key & 0xffu;
+  const float* p = &host_[(size_t)j * 4];
+  double a[4] = {p[0], p[1], p[2], p[3]};
+  if (im >> 1) {
+    const float* g = host_ops32(group_) + 4 * (im >> 1);
+    const double b[4] = {g[0], g[1], g[2], g[3]};
+    const double w = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+    const double x = a[0] * b[1] + b[0] * a[1] + a[2] * b[3] - a[3] * b[2];
+    const double y = a[0] * b[2] + b[0] * a[2] + a[3] * b[1] - a[1] * b[3];
+    const double z = a[0] * b[3] + b[0] * a[3] + a[1] * b[2] - a[2] * b[1];
+    a[0] = w, a[1] = x, a[2] = y, a[3] = z;
+  }
+  const double norm = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
+  const double sign = (im & 1u) ? -1.0 : 1.0;
+  for (int c = 0; c < 4; ++c) out[c] = sign * a[c] / norm;
+}
+
+// The triangulation display (src/exports.zig:88-103, Engine.buildMesh): the stars of every
+// source as one mesh. The host numbers the points (the sources first, as their own vertices
+// 0 .. n-1, then every other orbit point a star touches) and keeps each tetrahedron once.
+// Vertices are stereographic (x, y, z) / (1 + w) of the unit orbit point, fourth component 0.
+void Engine::build_mesh() {
+  std::vector<uint4> tets;
+  std::vector<double4> normals;
+  export_stars(tets, normals);
+  const int n = (int)n_;
   // Points: the sources first, then the other keys in order of first use.
   std::unordered_map<uint32_t, uint32_t> index;
   std::vector<uint32_t> keys;
@@ -312,25 +345,12 @@ void Engine::build_mesh() {
     if (!seen.insert({((uint64_t)v[0] << 32) | v[1], ((uint64_t)v[2] << 32) | v[3]}).second) continue;
     mesh_tets_.insert(mesh_tets_.end(), v, v + 4);
   }
-  const float* ops = host_ops32(group_);
   mesh_vertices_.assign(keys.size() * 4, 0.f);
   for (size_t k = 0; k < keys.size(); ++k) {
-    const uint32_t j = keys[k] >> 8, im = keys[k] & 0xffu;
-    const float* p = &host_[(size_t)j * 4];
-    double a[4] = {p[0], p[1], p[2], p[3]};
-    if (im >> 1) {
-      const float* g = ops + 4 * (im >> 1);
-      const double b[4] = {g[0], g[1], g[2], g[3]};
-      const double w = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
-      const double x = a[0] * b[1] + b[0] * a[1] + a[2] * b[3] - a[3] * b[2];
-      const double y = a[0] * b[2] + b[0] * a[2] + a[3] * b[1] - a[1] * b[3];
-      const double z = a[0] * b[3] + b[0] * a[3] + a[1] * b[2] - a[2] * b[1];
-      a[0] = w, a[1] = x, a[2] = y, a[3] = z;
-    }
-    const double norm = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3]);
-    const double sign = (im & 1u) ? -1.0 : 1.0;
-    const double s = 1.0 / (1.0 + sign * a[0] / norm);
-    for (int c = 0; c < 3; ++c) mesh_vertices_[k * 4 + c] = (float)(sign * a[c + 1] / norm * s);
+    double p[4];
+    orbit_point(keys[k], p);
+    const double s = 1.0 / (1.0 + p[0]);
+    for (int c = 0; c < 3; ++c) mesh_vertices_[k * 4 + c] = (float)(p[c + 1] * s);
   }
 }
 

@@ -836,6 +836,7 @@ void Engine::fetch() {
 }
 
 void Engine::reset_run() {
+  inserted_count_ = 0;
   point_separation_iteration_.reset();
   point_covering_iteration_.reset();
   cover_.reset();
@@ -1499,7 +1500,7 @@ const char* Engine::stats() {
   if (auto idx = identity_index()) j.integer("identity_index", *idx);
   else j.null("identity_index");
   j.integer("base_count", base_count_);
-  j.integer("inserted_count", 0);
+  j.integer("inserted_count", inserted_count_);
   j.str("triangulation_backend", "cuda");
   const double count_ext = 2.0 * order() * n_;
   const std::optional<double> bound = n_ > 0 ? std::optional<double>(simplex_degrees(count_ext)) : std::nullopt;

@@ -329,6 +329,10 @@ class Engine {
   void set(int gid, const float* values, size_t count);
   void generate_random(int gid, uint32_t count, uint32_t seed);
   void generate_grid(int gid, uint32_t freq, uint32_t target, uint32_t seed, uint32_t kind);
+  // Exact-count generation (src/engine.zig:199-231): the largest inverse-Hopf grid within
+  // the target, then points at the centres of the largest empty Delaunay caps until the
+  // sample holds exactly `target` orientations (insert.cpp).
+  void generate_exact(int gid, uint32_t target, bool add_identity, uint32_t kind);
   void measure();
   void spacing();
   // The covering radius on request (src/engine.zig:377-399): measured again only when the
@@ -541,7 +545,12 @@ class Engine {
   std::vector<double> cover_reach_;
   std::vector<uint32_t> cover_facet_counts_;
   double cover_grid_reach2_ = 0;
-  DeviceBuffer cover_mesh_, cover_mesh_offset_;
+  DeviceBuffer cover_mesh_, cover_mesh_offset_, cover_mesh_normal_;
+  void export_stars(std::vector<uint4>& tets, std::vector<double4>& normals);
+  std::vector<float> insertion_centres(uint32_t wanted);
+  uint32_t distinct_rows(std::vector<float>& values, uint32_t unique) const;
+  uint32_t inserted_count_ = 0;
+  void orbit_point(uint32_t key, double out[4]) const;
   std::vector<float> mesh_vertices_;
   std::vector<uint32_t> mesh_tets_;
   // Full-measure scratch.

@@ -34,8 +34,8 @@ int fail(void* h, const char* message) {
   return -1;
 }
 
-// Covering optimisation and exact-count generation are outside this engine (the covering
-// radius and the triangulation display are in it).
+// Covering optimisation is outside this engine (the covering radius, the triangulation
+// display and exact-count generation are in it).
 const char* kNoCovering = "covering optimisation is not part of this engine";
 }  // namespace
 
@@ -64,10 +64,12 @@ int zo_generate(void* h, uint32_t group, uint32_t freq, uint32_t target, uint32_
 }
 
 int zo_generate_exact(void* h, uint32_t group, uint32_t target, uint32_t flags) {
-  (void)target;
-  (void)flags;
   if (group >= 11) return fail(h, "Unknown group");
-  return fail(h, "Exact-count generation: InsertionNotAvailable");
+  // flags: bit 0 adds the identity; bits 8-15 are the grid kind, as in zo_generate.
+  if (((flags >> 8) & 0xffu) > 2) return fail(h, "Unknown grid kind");
+  return guarded(h, "Exact-count generation", [&](Engine& e) {
+    e.generate_exact((int)group, target, (flags & 1u) != 0, (flags >> 8) & 0xffu);
+  });
 }
 
 int zo_random(void* h, uint32_t group, uint32_t count, uint32_t seed) {

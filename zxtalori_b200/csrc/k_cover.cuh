@@ -377,6 +377,7 @@ __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs
         for (int t = lane; t < tail && t < (int)room; t += 32) {
           const uint32_t f = W.facet[t];
           A.mesh[first + t] = make_uint4(i << 8, W.key[f & 0xffu], W.key[(f >> 8) & 0xffu], W.key[(f >> 16) & 0xffu]);
+          if (A.mesh_normal) A.mesh_normal[first + t] = W.normal[t];
         }
       }
       if (lane < kCoverMax / 32) faces = __popc(W.used[lane]);

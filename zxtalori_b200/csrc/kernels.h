@@ -191,6 +191,7 @@ struct CoverArgs {
   // keys ((source << 8) | image) into mesh[mesh_offset[i] .. mesh_offset[i + 1]).
   uint4* mesh;
   const uint32_t* mesh_offset;
+  double4* mesh_normal;  // with mesh (may be null): each facet's unit normal, its cap's centre
 };
 cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s);
 
