@@ -79,8 +79,13 @@ int zo_identity(void* h, uint32_t flags);
  * orientations or the iteration changed since the last call (stats covering_cached).
  * Fewer than 4 orientations: -1 ("Covering radius: TooFewOrientations"). */
 int zo_cover(void* h);
-/* src/exports.zig:104-120. Covering optimisation is not part of this engine: these return
- * -1 with an explanatory message. */
+/* src/exports.zig:104-120 (Engine.optimizeCovering, setKicks): covering optimisation.
+ * zo_cover_optimize runs `steps` steps that lower the covering radius (mode bit 0: "face", a
+ * wider band of caps moves, else "tet"; other bits of the reference's mode word are accepted
+ * and ignored); a run continues while the sample is the one the last call ended on; `finish`
+ * restores the best sample seen and measures it; floor_deg (SO(3) degrees, 0: none) keeps
+ * the closest pair from being brought below it. zo_cover_kicks sets the plateau kicks
+ * (patience 1..1e6 steps, progress in [0,1), size in [0,1], trust in (0,1]). */
 int zo_cover_optimize(void* h, uint32_t steps, uint32_t mode, uint32_t finish, float floor_deg);
 int zo_cover_kicks(void* h, uint32_t patience, float progress, float size, float trust);
 /* src/exports.zig:88-103 (the triangulation display): zo_mesh brings the covering up to date

@@ -1566,6 +1566,21 @@ const char* Engine::stats() {
   j.opt("separation_deg", m ? finite(m->separation_deg) : std::nullopt);
   j.num("step_deg", step_deg_);
   j.opt("force_rms", m ? finite(m->force_rms) : finite(force_rms_));
+  j.integer("covering_optimizer_steps", opt_.steps);
+  j.integer("covering_optimizer_kicks", opt_.kicks);
+  j.opt("covering_optimizer_best_deg", opt_.active ? finite(opt_.best_radius) : std::nullopt);
+  j.integer("covering_optimizer_jobs", opt_.jobs);
+  j.integer("covering_optimizer_improved", opt_.improved);
+  j.integer("covering_optimizer_skipped", opt_.skipped);
+  j.integer("covering_optimizer_full_steps", opt_.full_steps);
+  j.integer("covering_optimizer_mismatches", 0);
+  j.key("covering_kick_settings");
+  {
+    char b[192];
+    std::snprintf(b, sizeof b, "{\"patience\":%u,\"progress\":%.9g,\"size\":%.9g,\"trust\":%.9g}", kicks_.patience,
+                  kicks_.progress, kicks_.size, kicks_.trust);
+    j.s += b;
+  }
   j.str("arithmetic", prec_ == kFP64 ? "fp64" : "fp32-refined");
   j.str("adapter", adapter_);
   j.s += "}";

@@ -9,6 +9,7 @@
 #include <limits>
 #include <memory>
 #include <optional>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -114,6 +115,22 @@ struct CoverResult {
   uint64_t probes = 0;             // pivots evaluated
   uint32_t rounds = 0;             // collection rounds (sources with a short reach run again)
   uint32_t shell_points = 0;       // shell sites of the chart grid the stars were collected from (0: every image)
+};
+
+// Plateau kicks of the covering optimiser (src/engine.zig:407-413 setKicks).
+struct KickSettings {
+  uint32_t patience = 150;
+  double progress = 5e-4, size = 0.04, trust = 0.03;
+};
+// A covering-optimiser run: the best and current samples (host rows), their radii, the trust
+// angle of a move (S3 radians) and the counts the stats report.
+struct CoverOptimizer {
+  bool active = false;
+  uint64_t key = 0;  // the sample the last batch ended on
+  std::vector<float> best, current;
+  double best_radius = NAN, current_radius = NAN, gain_ref = NAN, trust = 0, separation = 0;
+  uint32_t steps = 0, kicks = 0, jobs = 0, improved = 0, skipped = 0, full_steps = 0, since_gain = 0;
+  std::mt19937_64 rng;
 };
 
 struct StepResult {
@@ -338,6 +355,12 @@ class Engine {
   // The covering radius on request (src/engine.zig:377-399): measured again only when the
   // sample (group and float32 orientations) or the iteration has changed since the last one.
   void cover();
+  // Covering optimisation (optimize.cpp; src/engine.zig:407-534): `steps` steps that lower
+  // the covering radius, continuing the run while the sample is the one the last batch ended
+  // on; `finish` restores the best sample and measures it. mode bit 0: face (a wider band of
+  // caps moves) else tet; floor_deg: separation floor (SO(3) degrees, 0: none).
+  void set_kicks(uint32_t patience, double progress, double size, double trust);
+  void optimize_covering(uint32_t steps, uint32_t mode, bool finish, double floor_deg);
   // The triangulation display (src/engine.zig buildMesh): every source's star as one mesh of
   // stereographic vertices (4 floats each, the sources first) and tetrahedra (4 indices).
   void build_mesh();
@@ -550,6 +573,10 @@ class Engine {
   std::vector<float> insertion_centres(uint32_t wanted);
   uint32_t distinct_rows(std::vector<float>& values, uint32_t unique) const;
   uint32_t inserted_count_ = 0;
+  CoverOptimizer opt_;
+  KickSettings kicks_;
+  void move_to(const std::vector<float>& values);
+  double least_separation();
   void orbit_point(uint32_t key, double out[4]) const;
   std::vector<float> mesh_vertices_;
   std::vector<uint32_t> mesh_tets_;

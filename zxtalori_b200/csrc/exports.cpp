@@ -34,9 +34,6 @@ int fail(void* h, const char* message) {
   return -1;
 }
 
-// Covering optimisation is outside this engine (the covering radius, the triangulation
-// display and exact-count generation are in it).
-const char* kNoCovering = "covering optimisation is not part of this engine";
 }  // namespace
 
 extern "C" {
@@ -106,12 +103,11 @@ int zo_identity(void* h, uint32_t flags) {
 
 int zo_cover(void* h) { return guarded(h, "Covering radius", [](Engine& e) { e.cover(); }); }
 int zo_cover_optimize(void* h, uint32_t steps, uint32_t mode, uint32_t finish, float floor_deg) {
-  (void)steps, (void)mode, (void)finish, (void)floor_deg;
-  return fail(h, (std::string("Covering optimization: ") + kNoCovering).c_str());
+  return guarded(h, "Covering optimization",
+                 [&](Engine& e) { e.optimize_covering(steps, mode, finish != 0, (double)floor_deg); });
 }
 int zo_cover_kicks(void* h, uint32_t patience, float progress, float size, float trust) {
-  (void)patience, (void)progress, (void)size, (void)trust;
-  return fail(h, (std::string("Covering kicks: ") + kNoCovering).c_str());
+  return guarded(h, "Covering kicks", [&](Engine& e) { e.set_kicks(patience, progress, size, trust); });
 }
 int zo_mesh(void* h) { return guarded(h, "DT display", [](Engine& e) { e.build_mesh(); }); }
 const float* zo_mesh_vertices(void* h) {
