@@ -246,3 +246,41 @@ def test_pair_counts_of_the_gather(engine, ops32):
     assert abs(inside - expected) <= 1e-5 * expected + 10, (inside, expected)
     assert candidates >= inside
     assert candidates < 3 * inside  # the walk stays near the sources' balls
+
+
+def test_headline_rows_against_c_oracle(engine, ops32):
+    """The headline workload (O, N = 100,000, seed 193, neighbourhood 20): the first force
+    pass's rows of 3,000 sources (random ones and the nearest a zone boundary) against the
+    FP64 C oracle, at the FP32 tolerances above."""
+    with engine.haar("O", 100_000, 193) as grid:
+        grid.relax(0, neighbourhood=20)
+        rows = grid.debug_rows(0)
+        q = grid.quaternions.astype(np.float64)
+    ops = ops32["O"]
+    rng = np.random.default_rng(0)
+    margin = np.max(np.abs(q @ ops[1:].T), axis=1) / q[:, 0]  # near 1: close to a zone face
+    picked = np.unique(np.concatenate([rng.choice(len(q), 2000, replace=False), np.argsort(-margin)[:1000]]))
+    compare(rows[picked], cref.near_rows(q, ops, 20, sources=picked), "fp32")
+
+
+def test_headline_trajectory_against_fp64(engine, ops32):
+    """100 steps of the headline workload in both modes from the same float32 start. Energy:
+    the FP32-refined run within 1e-6 of the FP64 run (measured 1.2e-7). Separation: within
+    three times the FP64 method's own sensitivity to a one-ulp change of its start (measured
+    4.6e-3 against 6.3e-3), and equal to 1e-6 to the FP64 C oracle's separation of the FP32
+    run's own relaxed sample."""
+    with engine.haar("O", 100_000, 193) as grid:
+        start = grid.quaternions
+
+    def relaxed(q, mode):
+        with engine.from_quaternions(q, "O", precision=mode) as grid:
+            grid.relax(100, neighbourhood=20)
+            return grid.stats, grid.quaternions.astype(np.float64)
+
+    (s64, _), (s32, q32) = relaxed(start, "fp64"), relaxed(start, "fp32")
+    assert s32["energy"] == pytest.approx(s64["energy"], rel=1e-6)
+    sensitivity = max(abs(relaxed(_nudged(start, k), "fp64")[0]["separation_deg"] - s64["separation_deg"])
+                      for k in range(2))
+    assert abs(s32["separation_deg"] - s64["separation_deg"]) <= 3 * sensitivity + 1e-6 * s64["separation_deg"]
+    own = qvm.separation_deg(cref.near_rows(q32, ops32["O"], 20)["nearest"].min())
+    assert s32["separation_deg"] == pytest.approx(own, rel=1e-6)
