@@ -476,7 +476,7 @@ def covering_section(zo):
             t = time.perf_counter()
             s = g.covering()
             first = time.perf_counter() - t
-            g.relax(1)
+            g.relax(1, neighbourhood=DELTA)  # a near-field step (all pairs at 1M would take minutes)
             t = time.perf_counter()
             s = g.covering()
             again = time.perf_counter() - t
