@@ -59,6 +59,10 @@ const float* zo_operations(void* h);
 
 /* src/exports.zig:41. Full measures below the ratio limit, else Quey energy + separation. */
 int zo_measure(void* h);
+/* Extension (no reference counterpart; src/engine.zig:308-351 gates the ratios off above the
+ * ratio limit): zo_measure with Riesz 1/2/3, Green and log ratios over all pairs at any
+ * count, for samples above the ratio limit that want them (N^2 |K| pair evaluations). */
+int zo_measure_full(void* h);
 /* src/exports.zig:60. Nearest orbit neighbour of every point (near field above 20,000). */
 int zo_spacing(void* h);
 /* src/exports.zig:49. Up to 1,000 Barzilai-Borwein steps of QVM repulsion. */

@@ -351,6 +351,8 @@ class Engine {
   // sample holds exactly `target` orientations (insert.cpp).
   void generate_exact(int gid, uint32_t target, bool add_identity, uint32_t kind);
   void measure();
+  // measure() with every ratio over all pairs at any count (above the ratio limit too).
+  void measure_full();
   void spacing();
   // The covering radius on request (src/engine.zig:377-399): measured again only when the
   // sample (group and float32 orientations) or the iteration has changed since the last one.
@@ -500,7 +502,7 @@ class Engine {
   std::optional<NearTiles> forced_tiles_;
   double forced_walk_ = 0;
   void fetch();
-  Measures full_measure();
+  Measures full_measure(bool fp64 = false);
   Measures relax_state_measure();
   int fixed_arg() const { return fixed_index_ ? (int)*fixed_index_ : -1; }
   std::optional<uint32_t> identity_index() const;

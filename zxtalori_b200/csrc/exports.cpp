@@ -88,6 +88,7 @@ const float* zo_quaternions(void* h) { return static_cast<Engine*>(h)->quaternio
 const float* zo_operations(void* h) { return zo::host_ops32(static_cast<Engine*>(h)->group()); }
 
 int zo_measure(void* h) { return guarded(h, "Measure failed", [](Engine& e) { e.measure(); }); }
+int zo_measure_full(void* h) { return guarded(h, "Measure failed", [](Engine& e) { e.measure_full(); }); }
 int zo_spacing(void* h) { return guarded(h, "Spacing failed", [](Engine& e) { e.spacing(); }); }
 int zo_relax(void* h, uint32_t steps) { return guarded(h, "Relaxation failed", [&](Engine& e) { e.relax(steps); }); }
 
