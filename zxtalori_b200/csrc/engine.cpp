@@ -1363,7 +1363,10 @@ void Engine::bench(uint32_t steps, uint32_t warmup, double flush_bytes, double* 
 size_t Engine::device_bytes() const {
   return q32_.bytes() + q64_.bytes() + relax_state_.bytes() + spacing_state_.bytes() + full_rows_.bytes() +
          full_partial_.bytes() + full_extra_.bytes() + full_pextra_.bytes() + full_degen_.bytes() +
-         full_pdegen_.bytes();
+         full_pdegen_.bytes() + cover_alpha_.bytes() + cover_centre_.bytes() + cover_faces_.bytes() +
+         cover_facets_.bytes() + cover_status_.bytes() + cover_need_.bytes() + cover_list_.bytes() +
+         cover_probes_.bytes() + cover_mesh_.bytes() + cover_mesh_offset_.bytes() + cover_mesh_normal_.bytes() +
+         (cover_near_ ? cover_near_->bytes() : 0);
 }
 
 void Engine::spacing_exact(uint32_t* listed, uint32_t* ties) {
