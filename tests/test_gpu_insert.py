@@ -64,3 +64,31 @@ def test_exact_count_errors(engine):
         engine.generate("O", count=20, exact=True)
     with pytest.raises(RuntimeError, match="Exact-count generation: TransportNotAvailable"):
         engine.generate("O", count=400, exact=True, kind="transport")
+
+
+@pytest.mark.parametrize("group", GROUPS)
+def test_exact_count_identity_and_zone_after_relaxation(engine, group):
+    """The reference's tests/test_workbench.py:7-30, mirrored: 1,000 orientations with a fixed
+    identity; inserted centres do not cluster (every orbit point at least 0.01 in chord from
+    the next); after relaxing, the zone holds, the identity stays and the sample has moved."""
+    with engine.generate(group, count=1000, exact=True, fixed_identity=True) as grid:
+        assert len(grid) == 1000
+        assert grid.stats["base_count"] + grid.stats["inserted_count"] == 1000
+        before = grid.quaternions.copy()
+        ops = grid.operations.astype(np.float64)
+        points, _ = cov.orbit(before.astype(np.float64), ops)
+        assert cKDTree(points).query(before.astype(np.float64), k=2)[0][:, 1].min() > 0.01
+        identity = grid.stats["identity_index"]
+        assert identity is not None
+        grid.relax(12)
+        q = grid.quaternions.astype(np.float64)
+        assert np.max(np.abs(q @ ops.T) - q[:, :1]) < 1e-6
+        np.testing.assert_array_equal(q[identity], [1, 0, 0, 0])
+        assert np.max(np.abs(q - before)) > 1e-5
+        assert grid.stats["separation_deg"] > 0
+
+
+@pytest.mark.parametrize("group,count", [("C6", 84), ("D3", 62), ("D3", 84), ("D4", 84)])
+def test_exact_count_thin_shell(engine, group, count):
+    with engine.generate(group, count=count, exact=True, identity=True) as grid:
+        assert len(grid) == count
