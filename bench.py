@@ -437,8 +437,7 @@ def spacing_section(zo, peak, count=10_000_000, seed=7, measure_count=None):
                            "peak_source": peak[1], "unit": "GB/s", "frac": achieved / peak[0],
                            "limiter": "not HBM: each source reads every site of its first ball's cell rows (tens "
                                       "per source) from L1/L2; ncu on the 1M launch shows the ALU pipe at 71 % "
-                                      "and 13 of 32 lanes active (each thread walks its own rows) "
-                                      "(profiles/spacing_pass_i10m.md)"}}
+                                      "and 13 of 32 lanes active (each thread walks its own rows)"}}
     # The same float32 sample through the FP64 method: indices must agree except exact ties.
     g64 = zo.from_quaternions(q, "I", precision="fp64")
     g64.spacing()
