@@ -192,3 +192,15 @@ def test_mesh_is_the_hull_around_the_zone(engine, group, count):
     hull = ConvexHull(points)
     around = {tuple(sorted(s)) for s in hull.simplices if (s < count).any()}
     assert exported == around
+
+
+@pytest.mark.parametrize("group,count", [("C2", 4), ("C2", 7), ("D2", 5), ("C4", 12), ("T", 4), ("I", 4)])
+def test_covering_of_tiny_samples(engine, group, count):
+    """A handful of orientations: caps of tens of degrees, reaches up to a hemisphere."""
+    q = np.random.default_rng(count).normal(size=(count, 4))
+    with engine.from_quaternions(q, group) as grid:
+        stats = grid.covering()
+        hull = hull_of(grid)
+        assert stats["covering_unresolved_caps"] == 0
+        assert abs(stats["covering_radius_deg"] - hull["radius_deg"]) < 2e-4
+        assert np.allclose(grid.point_values("covering"), hull["point_covering"], atol=2e-3)
