@@ -134,7 +134,7 @@ void Engine::measure_covering() {
   std::vector<uint32_t> status(n);
   std::vector<double> need(n);
   std::vector<double> used(n, reach2);  // the reach each source's star was built in
-  std::vector<uint32_t> again, grid_list, dense_list;
+  std::vector<uint32_t> listed, grid_list, dense_list;
   for (int round = 1;; ++round) {
     ZO_CUDA(cudaMemcpyAsync(status.data(), A.status, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
     ZO_CUDA(cudaMemcpyAsync(need.data(), A.need2, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -152,10 +152,11 @@ void Engine::measure_covering() {
     // need2 holds each listed source's next reach: the kernel reads it before it writes.
     A.reach2_of = A.need2;
     const size_t g = grid_list.size();
-    std::vector<uint32_t>& all = again;
-    all.assign(grid_list.begin(), grid_list.end());
-    all.insert(all.end(), dense_list.begin(), dense_list.end());
-    ZO_CUDA(cudaMemcpyAsync(cover_list_.as<uint32_t>(), all.data(), all.size() * 4, cudaMemcpyHostToDevice, stream_));
+    // The grid's sources first, then those that need every image.
+    listed.assign(grid_list.begin(), grid_list.end());
+    listed.insert(listed.end(), dense_list.begin(), dense_list.end());
+    ZO_CUDA(cudaMemcpyAsync(cover_list_.as<uint32_t>(), listed.data(), listed.size() * 4, cudaMemcpyHostToDevice,
+                            stream_));
     if (g > 0) {
       A.grid = grid;
       A.list = cover_list_.as<uint32_t>();
