@@ -96,6 +96,14 @@ class Dist:
         self.pg.all_reduce(t, op={"max": self.pg.ReduceOp.MAX, "sum": self.pg.ReduceOp.SUM}[op])
         return float(t.item())
 
+    def gather(self, obj):
+        """Every rank's `obj`, in rank order, on every rank."""
+        if not self.pg:
+            return [obj]
+        out = [None] * self.world
+        self.pg.all_gather_object(out, obj)
+        return out
+
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
@@ -302,6 +310,27 @@ def batched_section(zo, samples=256, steps=50, dist=None):
             "seconds": dt, "setup_seconds": setup, "tile_shapes_from_table": shapes, "gpus": world,
             "split": "samples over ranks, largest first to the least-loaded rank; no collective",
             "timing": "wall clock of zo_batch_relax (all steps and closing passes), samples created beforehand"}
+
+
+def served_split_section(zo, device_rate, dist, factor=1.4, per_rate=120):
+    """Config 5 over several GPUs: one request stream at `factor` times the whole job's
+    capacity, request k served by rank k mod N (its own Server, no collective); the ranks'
+    results are gathered for the whole-job throughput (all pair evaluations over the longest
+    rank's span) and latency percentiles."""
+    from zxtalori_b200 import serve
+
+    probe = serve.poisson_requests(1.0, 20_000.0, seed=11)
+    mean_evals = float(np.mean([(r.steps + 1) * r.count * serve.neighbours(r.count, serve.ORDER[r.group],
+                                                                           r.neighbourhood) for r in probe]))
+    rate = factor * dist.world * device_rate / mean_evals
+    reqs = serve.poisson_requests(rate, 1.5 * per_rate / rate, seed=5)[:per_rate]
+    mine = serve.shard_requests(reqs, dist.rank, dist.world)
+    dist.barrier()
+    served = serve.Server().run(mine)
+    everything = [r for part in dist.gather(served) for r in part]
+    return {"rate_per_s": rate, "rate_over_capacity": factor, "gpus": dist.world,
+            "split": "request k to rank k mod N, one Server per GPU, no collective",
+            **serve.summary(everything)}
 
 
 def served_section(zo, device_rate, factors=(0.7, 1.4), per_rate=120, plain_requests=12):
@@ -670,6 +699,7 @@ def run_ours(args, dist):
     extras = {}
     if args.gpus > 1 and not args.no_extras:
         extras["batched"] = batched_section(zo, dist=dist)  # config 4 split over the ranks
+        extras["served"] = served_split_section(zo, value / args.gpus, dist)  # config 5 split over the ranks
     if dist.rank != 0:
         return 0
     # All pairs, spacing, batched and served workloads (configs 1, 3, 4, 5) on one GPU.

@@ -62,3 +62,35 @@ def test_reference_arm_under_torchrun_prints_one_line():
     assert line["ms_per_step"] == line["step_ms"]["p50"]  # measured, one step
     assert line["e2e"] == {"value": line["value"], "unit": "pair-evals/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def _served_split_rank(rank, world, port, out):
+    os.environ.update(RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE=str(world), MASTER_ADDR="127.0.0.1",
+                      MASTER_PORT=str(port))
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from zxtalori_b200 import serve
+
+    dist = bench.Dist()
+    try:
+        reqs = serve.poisson_requests(2.0, 40.0, seed=5)
+        mine = serve.shard_requests(reqs, dist.rank, dist.world)
+        gathered = dist.gather([r.id for r in mine])
+    finally:
+        dist.close()
+    with open(out / f"served{rank}.json", "w") as f:
+        json.dump({"total": len(reqs), "parts": gathered}, f)
+
+
+def test_served_stream_split_over_two_ranks(tmp_path):
+    """bench.py --gpus N splits config 5's request stream over the ranks (request k to rank
+    k mod N) and gathers every rank's results: each request is served by exactly one rank,
+    and every rank sees the same gathered list."""
+    port = free_port()
+    mp.start_processes(_served_split_rank, args=(2, port, tmp_path), nprocs=2, join=True, start_method="spawn")
+    seen = [json.loads((tmp_path / f"served{rank}.json").read_text()) for rank in range(2)]
+    assert seen[0] == seen[1]
+    parts = seen[0]["parts"]
+    ids = sorted(i for part in parts for i in part)
+    assert ids == list(range(seen[0]["total"]))
+    assert all(i % 2 == rank for rank, part in enumerate(parts) for i in part)

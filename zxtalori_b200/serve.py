@@ -176,6 +176,15 @@ class Server:
         return self.results
 
 
+def shard_requests(requests, rank, world):
+    """This rank's share of a request stream when `world` GPUs serve it together (one process
+    and one Server per GPU, no collective): request k goes to rank k mod world, so each rank
+    sees a thinned Poisson stream at 1/world of the rate."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    return [r for r in requests if r.id % world == rank]
+
+
 def serve_one_at_a_time(requests, precision="fp64", clock=time.perf_counter, keep_quaternions=False, measure=True):
     """The plain path: requests in arrival order, one at a time, each relaxed with zo_relax
     (no graphs, no overlap) and then measured; FP64 by default."""
