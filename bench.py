@@ -312,7 +312,7 @@ def batched_section(zo, samples=256, steps=50, dist=None):
             "timing": "wall clock of zo_batch_relax (all steps and closing passes), samples created beforehand"}
 
 
-def served_split_section(zo, device_rate, dist, factor=1.4, per_rate=120):
+def served_split_section(zo, device_rate, dist, factor=1.4, per_rate=200):
     """Config 5 over several GPUs: one request stream at `factor` times the whole job's
     capacity, request k served by rank k mod N (its own Server, no collective); the ranks'
     results are gathered for the whole-job throughput (all pair evaluations over the longest
@@ -333,7 +333,7 @@ def served_split_section(zo, device_rate, dist, factor=1.4, per_rate=120):
             **serve.summary(everything)}
 
 
-def served_section(zo, device_rate, factors=(0.7, 1.4), per_rate=120, plain_requests=12):
+def served_section(zo, device_rate, factors=(0.7, 1.4), per_rate=200, plain_requests=20):
     """Config 5: Poisson arrivals of relax+measure requests (group uniform, N log-uniform in
     [500, 1e6], steps uniform in [10, 200], all pairs below 5,000 orientations else
     neighbourhood 20), served by the continuous-batching loop in FP32-refined mode, at
