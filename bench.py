@@ -326,7 +326,7 @@ def served_split_section(zo, device_rate, dist, factor=1.4, per_rate=200):
     reqs = serve.poisson_requests(rate, 1.5 * per_rate / rate, seed=5)[:per_rate]
     mine = serve.shard_requests(reqs, dist.rank, dist.world)
     dist.barrier()
-    served = serve.Server().run(mine)
+    served = serve.NativeServer().run(mine)
     everything = [r for part in dist.gather(served) for r in part]
     return {"rate_per_s": rate, "rate_over_capacity": factor, "gpus": dist.world,
             "split": "request k to rank k mod N, one Server per GPU, no collective",
@@ -336,7 +336,8 @@ def served_split_section(zo, device_rate, dist, factor=1.4, per_rate=200):
 def served_section(zo, device_rate, factors=(0.7, 1.4), per_rate=200, plain_requests=20):
     """Config 5: Poisson arrivals of relax+measure requests (group uniform, N log-uniform in
     [500, 1e6], steps uniform in [10, 200], all pairs below 5,000 orientations else
-    neighbourhood 20), served by the continuous-batching loop in FP32-refined mode, at
+    neighbourhood 20), served by the library's continuous-batching loop (zo_serve) in
+    FP32-refined mode, at
     rates below and above the GPU's capacity: capacity = the headline's device
     pair-evals/s over the mean pair evaluations of a request. `per_rate` requests per rate
     (p50 and p99 from that many latencies). The plain FP64 path serves a fixed subsample
@@ -355,7 +356,7 @@ def served_section(zo, device_rate, factors=(0.7, 1.4), per_rate=200, plain_requ
         reqs = serve.poisson_requests(rate, 1.5 * per_rate / rate, seed=5)[:per_rate]
         streams[f] = reqs
         t = time.perf_counter()
-        served = serve.Server().run(reqs)
+        served = serve.NativeServer().run(reqs)
         wall = time.perf_counter() - t
         sweep.append({"rate_per_s": rate, "rate_over_capacity": f, "wall_s": wall,
                       "arrival_window_s": reqs[-1].arrival, **serve.summary(served)})
@@ -368,7 +369,7 @@ def served_section(zo, device_rate, factors=(0.7, 1.4), per_rate=200, plain_requ
     plain = serve.summary(serve.serve_one_at_a_time(plain_in))
     plain["wall_s"] = time.perf_counter() - t
     # The same subsample served by the batching loop, for a like-for-like throughput ratio.
-    same = serve.summary(serve.Server().run([serve.Request(r.id, r.group, r.count, r.steps, r.seed,
+    same = serve.summary(serve.NativeServer().run([serve.Request(r.id, r.group, r.count, r.steps, r.seed,
                                                            r.neighbourhood, 0.0) for r in chosen]))
     return {**{k: middle[k] for k in ("requests", "pair_evals_per_s", "latency_p50_s", "latency_p99_s")},
             "capacity_requests_per_s": capacity, "mean_pair_evals_per_request": mean_evals,

@@ -247,6 +247,32 @@ int zo_zone_planes(uint32_t group, uint8_t* order, float* reach);
 int zo_pair_rows_noalloc(uint32_t group, const float* q_device, uint32_t n, double* rows_device, void* stream,
                          char* error, size_t error_len);
 
+/* Extension (no reference counterpart): the continuous-batching relax + measure service on
+ * one GPU, run to completion. Each request is a Haar sample (group, count, seed) relaxed for
+ * `steps` BB steps (neighbourhood 0: all pairs) and then measured; `arrival` is its arrival
+ * time in seconds from the call. Requests are admitted in arrival order while their device
+ * memory fits the budget, every resident sample steps on its own stream in chunks so that
+ * the samples' kernels overlap, and the closing pass and measure() run on worker threads.
+ * settings (n_settings of them, the rest default): [0] memory budget in bytes (0: 80 % of
+ * the free device memory), [1] most resident samples (64), [2] seconds of device work per
+ * chunk (0.02), [3] measure (1), [4] precision (0 FP32-refined, 1 FP64), [5] worker
+ * threads (4), [6] pair evaluations per second for chunk sizing (2.5e11). results: n entries
+ * in completion order (status 0, or -1 with the request's error). Returns 0, or -1 with the
+ * message in `error` when the service itself failed. */
+typedef struct {
+  uint32_t id, group, count, steps, seed;
+  float neighbourhood;
+  double arrival;
+} zo_serve_request;
+typedef struct {
+  uint32_t id, iteration, count, order;
+  double arrival, admitted, finished, neighbourhood, energy, separation_deg;
+  int32_t status;
+  char error[108];
+} zo_serve_result;
+int zo_serve(const zo_serve_request* requests, uint32_t n, const double* settings, uint32_t n_settings,
+             zo_serve_result* results, char* error, size_t error_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -120,3 +120,36 @@ def test_plain_one_at_a_time(engine):
     res = serve.serve_one_at_a_time(reqs)
     assert [r.id for r in res] == [0, 1]
     assert all(r.stats["arithmetic"] == "fp64" for r in res)
+
+
+def test_native_server_same_alone_in_mix_and_as_the_python_loop(engine):
+    """zo_serve (the loop inside the library): every request completes once with exactly its
+    steps; each result's energy and separation are the same served alone, in the mix, and by
+    the Python loop (results do not depend on what else runs)."""
+    from zxtalori_b200 import serve
+
+    requests = [serve.Request(k, g, n, 8 + 3 * k, 100 + k, d, arrival=0.01 * k) for k, (g, n, _, d) in enumerate(SAMPLES)]
+    mixed = serve.NativeServer(chunk_seconds=0.001).run(requests)
+    assert sorted(r.id for r in mixed) == list(range(len(requests)))
+    by_id = {r.id: r for r in mixed}
+    python = {r.id: r for r in serve.Server(chunk_seconds=0.001).run(requests)}
+    for req in requests:
+        alone = serve.NativeServer().run([serve.Request(req.id, req.group, req.count, req.steps, req.seed,
+                                                        req.neighbourhood, 0.0)])[0]
+        got = by_id[req.id]
+        assert got.stats["iteration"] == req.steps
+        assert alone.stats["quey_energy"] == got.stats["quey_energy"] == python[req.id].stats["quey_energy"]
+        assert alone.stats["separation_deg"] == got.stats["separation_deg"] == python[req.id].stats["separation_deg"]
+        assert got.finished >= got.admitted >= got.arrival - 1e-9
+    info = serve.summary(mixed)
+    assert info["requests"] == len(requests) and info["pair_evals_per_s"] > 0
+
+
+def test_native_server_tight_budget_runs_one_at_a_time(engine):
+    from zxtalori_b200 import serve
+
+    requests = [serve.Request(k, "O", 2000, 5, k, 0.0) for k in range(4)]
+    results = serve.NativeServer(memory_budget=1).run(requests)
+    assert sorted(r.id for r in results) == [0, 1, 2, 3]
+    spans = sorted((r.admitted, r.finished) for r in results)
+    assert all(spans[k + 1][0] >= spans[k][1] - 1e-3 for k in range(3))  # admitted after the last finished

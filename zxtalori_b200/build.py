@@ -21,7 +21,7 @@ SRC = HERE / "csrc"
 OUT = HERE / "_lib"
 LIB = OUT / "libzxtalori.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["kernels.cu", "engine.cpp", "groups.cpp", "hopf.cpp", "exports.cpp", "memory.cpp", "no_alloc.cu", "batch.cpp", "cover.cpp", "insert.cpp", "optimize.cpp"]
+SOURCES = ["kernels.cu", "engine.cpp", "groups.cpp", "hopf.cpp", "exports.cpp", "memory.cpp", "no_alloc.cu", "batch.cpp", "cover.cpp", "insert.cpp", "optimize.cpp", "serve.cpp"]
 
 
 def nvcc():

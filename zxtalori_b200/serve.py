@@ -14,6 +14,7 @@ kernels read only its own buffers and sum in a fixed order.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 import time
 from concurrent.futures import ThreadPoolExecutor
@@ -21,7 +22,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .api import GROUPS, haar
+from .api import GROUPS, _library, haar
 from .batch import neighbours
 
 ORDER = {"C2": 2, "C3": 3, "C4": 4, "C6": 6, "D2": 4, "D3": 6, "D4": 8, "D6": 12, "T": 12, "O": 24, "I": 60}
@@ -174,6 +175,60 @@ class Server:
                     else:
                         time.sleep(0.0005)
         return self.results
+
+
+class _NativeRequest(C.Structure):
+    _fields_ = [("id", C.c_uint32), ("group", C.c_uint32), ("count", C.c_uint32), ("steps", C.c_uint32),
+                ("seed", C.c_uint32), ("neighbourhood", C.c_float), ("arrival", C.c_double)]
+
+
+class _NativeResult(C.Structure):
+    _fields_ = [("id", C.c_uint32), ("iteration", C.c_uint32), ("count", C.c_uint32), ("order", C.c_uint32),
+                ("arrival", C.c_double), ("admitted", C.c_double), ("finished", C.c_double),
+                ("neighbourhood", C.c_double), ("energy", C.c_double), ("separation_deg", C.c_double),
+                ("status", C.c_int32), ("error", C.c_char * 108)]
+
+
+@dataclass
+class NativeServer:
+    """The same continuous-batching loop run inside the library (zo_serve): admission,
+    chunked stepping and the finishing workers in C++ threads, one blocking call for the
+    whole request stream (arrival times from the call). Results carry the numbers the
+    summary needs (count, order, iteration, neighbourhood, Quey energy, separation)."""
+    precision: str = "fp32"
+    memory_budget: int | None = None
+    max_active: int = 64
+    chunk_seconds: float = 0.02
+    measure: bool = True
+    workers: int = 4
+    pair_rate: float = 2.5e11
+
+    def run(self, requests):
+        lib = _library()
+        if not hasattr(lib, "_serve_bound"):
+            lib.zo_serve.argtypes = [C.POINTER(_NativeRequest), C.c_uint32, C.POINTER(C.c_double), C.c_uint32,
+                                     C.POINTER(_NativeResult), C.c_char_p, C.c_size_t]
+            lib.zo_serve.restype = C.c_int
+            lib._serve_bound = True
+        reqs = (_NativeRequest * len(requests))()
+        for k, r in enumerate(requests):
+            reqs[k] = _NativeRequest(r.id, GROUPS.index(r.group), r.count, r.steps, r.seed, r.neighbourhood, r.arrival)
+        settings = (C.c_double * 7)(float(self.memory_budget or 0), float(self.max_active), float(self.chunk_seconds),
+                                    1.0 if self.measure else 0.0, 1.0 if self.precision == "fp64" else 0.0,
+                                    float(self.workers), float(self.pair_rate))
+        out = (_NativeResult * len(requests))()
+        error = C.create_string_buffer(512)
+        if lib.zo_serve(reqs, len(requests), settings, 7, out, error, len(error)) != 0:
+            raise RuntimeError(error.value.decode(errors="replace"))
+        results = []
+        for r in out:
+            if r.status != 0:
+                raise RuntimeError(f"request {r.id}: {r.error.decode(errors='replace')}")
+            stats = {"count": r.count, "order": r.order, "iteration": r.iteration,
+                     "relax_neighbourhood": r.neighbourhood or None, "quey_energy": r.energy,
+                     "separation_deg": r.separation_deg}
+            results.append(Result(r.id, r.arrival, r.admitted, r.finished, stats))
+        return results
 
 
 def shard_requests(requests, rank, world):
