@@ -68,8 +68,6 @@ class BatchRun {
     if (stream_) cudaStreamDestroy(stream_);
   }
 
-  const std::vector<Engine*>& engines() const { return engines_; }
-
   // One BB step of every sample.
   void step() {
     ZO_CUDA(cudaSetDevice(device_));

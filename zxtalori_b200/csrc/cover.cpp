@@ -124,16 +124,17 @@ void Engine::measure_covering() {
   }
   const NearGrid* grid = A.grid;
 
-  // Round 0: every source at the first reach.
+  // Round 0: every source at the first reach, in the narrow star.
   A.reach2 = reach2;
   A.reach2_of = nullptr;
   A.list = nullptr;
   A.count = n;
-  ZO_CUDA(launch_cover(A, sms_, stream_));
+  ZO_CUDA(launch_cover(A, sms_, stream_, true));
   r.rounds = 1;
   std::vector<uint32_t> status(n);
   std::vector<double> need(n);
   std::vector<double> used(n, reach2);  // the reach each source's star was built in
+  std::vector<uint8_t> narrow(n, 1);    // built by the narrow star (round 0)
   std::vector<uint32_t> listed, grid_list, dense_list;
   for (int round = 1;; ++round) {
     ZO_CUDA(cudaMemcpyAsync(status.data(), A.status, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
@@ -147,6 +148,7 @@ void Engine::measure_covering() {
       const bool fits = grid && need[i] <= grid_reach2;
       (fits ? grid_list : dense_list).push_back((uint32_t)i);
       used[i] = need[i];
+      narrow[i] = 0;
     }
     if ((grid_list.empty() && dense_list.empty()) || round == kCoverRounds) break;
     // need2 holds each listed source's next reach: the kernel reads it before it writes.
@@ -161,13 +163,13 @@ void Engine::measure_covering() {
       A.grid = grid;
       A.list = cover_list_.as<uint32_t>();
       A.count = (int)g;
-      ZO_CUDA(launch_cover(A, sms_, stream_));
+      ZO_CUDA(launch_cover(A, sms_, stream_, false));
     }
     if (!dense_list.empty()) {
       A.grid = nullptr;
       A.list = cover_list_.as<uint32_t>() + g;
       A.count = (int)dense_list.size();
-      ZO_CUDA(launch_cover(A, sms_, stream_));
+      ZO_CUDA(launch_cover(A, sms_, stream_, false));
     }
     ++r.rounds;
   }
@@ -209,17 +211,20 @@ void Engine::measure_covering() {
   cover_iteration_ = iteration_;
   point_covering_iteration_ = iteration_;
   cover_reach_ = std::move(used);
+  cover_narrow_ = std::move(narrow);
   cover_facet_counts_ = std::move(facets);
   cover_grid_reach2_ = grid ? grid_reach2 : 0.0;
 }
 
-// Every source's star again, in the reach that proved it, written out as tetrahedra of point
+// Every source's star again, in the reach and the star width that proved it (so that the
+// same points are collected and the same facets found), written out as tetrahedra of point
 // keys ((source << 8) | image; the source first) with each facet's unit normal (its cap's
 // centre). The covering is brought up to date first.
 void Engine::export_stars(std::vector<uint4>& tets, std::vector<double4>& normals) {
   cover();
   const int n = (int)n_;
-  if (cover_reach_.size() != (size_t)n || cover_facet_counts_.size() != (size_t)n) throw Failure("CoveringNotMeasured");
+  if (cover_reach_.size() != (size_t)n || cover_facet_counts_.size() != (size_t)n || cover_narrow_.size() != (size_t)n)
+    throw Failure("CoveringNotMeasured");
   std::vector<uint32_t> offset(n + 1, 0);
   uint64_t total = 0;
   for (int i = 0; i < n; ++i) {
@@ -253,29 +258,34 @@ void Engine::export_stars(std::vector<uint4>& tets, std::vector<double4>& normal
   A.mesh_offset = cover_mesh_offset_.as<uint32_t>();
   A.mesh_normal = cover_mesh_normal_.as<double4>();
   // Each source from the chart grid when its reach is within the grid's (the grid of the
-  // covering pass, built for these positions), else from every image.
-  std::vector<uint32_t> grid_list, dense_list;
-  for (int i = 0; i < n; ++i)
-    (cover_grid_reach2_ > 0 && cover_reach_[i] <= cover_grid_reach2_ ? grid_list : dense_list).push_back((uint32_t)i);
-  std::vector<uint32_t> all(grid_list);
-  all.insert(all.end(), dense_list.begin(), dense_list.end());
+  // covering pass, built for these positions), else from every image; in the narrow star when
+  // the first pass proved it there.
+  std::vector<uint32_t> part[4];  // grid narrow, grid wide, dense narrow, dense wide
+  for (int i = 0; i < n; ++i) {
+    const bool in_grid = cover_grid_reach2_ > 0 && cover_reach_[i] <= cover_grid_reach2_;
+    part[(in_grid ? 0 : 2) + (cover_narrow_[i] ? 0 : 1)].push_back((uint32_t)i);
+  }
+  std::vector<uint32_t> all;
+  for (const auto& p : part) all.insert(all.end(), p.begin(), p.end());
   cover_list_.ensure((size_t)n * 4);
   ZO_CUDA(cudaMemcpyAsync(cover_list_.as<uint32_t>(), all.data(), all.size() * 4, cudaMemcpyHostToDevice, stream_));
-  if (!grid_list.empty()) {
-    A.scode = cover_near_->sorted_codes();
-    A.simg = cover_near_->sorted_images();
-    A.cell_off = cover_near_->cell_offsets();
-    A.grid = cover_near_->grid_device();
-    A.grid_reach2 = cover_grid_reach2_;
-    A.list = cover_list_.as<uint32_t>();
-    A.count = (int)grid_list.size();
-    ZO_CUDA(launch_cover(A, sms_, stream_));
-  }
-  if (!dense_list.empty()) {
-    A.grid = nullptr;
-    A.list = cover_list_.as<uint32_t>() + grid_list.size();
-    A.count = (int)dense_list.size();
-    ZO_CUDA(launch_cover(A, sms_, stream_));
+  size_t first = 0;
+  for (int k = 0; k < 4; ++k) {
+    if (!part[k].empty()) {
+      if (k < 2) {
+        A.scode = cover_near_->sorted_codes();
+        A.simg = cover_near_->sorted_images();
+        A.cell_off = cover_near_->cell_offsets();
+        A.grid = cover_near_->grid_device();
+        A.grid_reach2 = cover_grid_reach2_;
+      } else {
+        A.grid = nullptr;
+      }
+      A.list = cover_list_.as<uint32_t>() + first;
+      A.count = (int)part[k].size();
+      ZO_CUDA(launch_cover(A, sms_, stream_, (k & 1) == 0));
+    }
+    first += part[k].size();
   }
   tets.resize(total);
   normals.resize(total);

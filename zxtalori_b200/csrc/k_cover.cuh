@@ -43,18 +43,27 @@
 namespace zo {
 
 constexpr int kCoverWarps = 4;
-constexpr int kCoverMax = 256;      // neighbours per source
-constexpr int kCoverFacets = 256;   // facets per star
+constexpr int kCoverMax = 256;      // neighbours per source (the wide star)
+constexpr int kCoverFacets = 256;   // facets per star (the wide star)
+// The first pass over every source uses a narrow star: 64 neighbours (the reach is sized to
+// hold 48 on average) and 128 facets (a star of V neighbours closes with 2V - 4 facets), so a
+// warp's shared memory is 8 KB instead of 19 KB and three times as many warps stay resident;
+// a source that overflows it is sent to the wide star at the same reach.
+constexpr int kCoverMaxNarrow = 64;
+constexpr int kCoverFacetsNarrow = 128;
 
-struct CoverWarp {
-  double4 d[kCoverMax];            // y_m - x in canonical order
-  uint32_t key[kCoverMax];         // (source << 8) | image of each collected point
-  uint32_t facet[kCoverFacets];    // a | b << 8 | c << 16, a < b < c
-  double4 normal[kCoverFacets];    // each facet's unit normal, oriented to its cap
-  uint32_t used[kCoverMax / 32];   // neighbours touched by some facet
+template <int NB, int NF>
+struct CoverStar {
+  static constexpr int kPoints = NB, kFacets = NF;
+  double4 d[NB];                   // y_m - x in canonical order
+  uint32_t key[NB];                // (source << 8) | image of each collected point
+  uint32_t facet[NF];              // a | b << 8 | c << 16, a < b < c
+  double4 normal[NF];              // each facet's unit normal, oriented to its cap
+  uint32_t used[NB / 32];          // neighbours touched by some facet
   float4 image_dot[kMaxGroupOrder];  // dense collection: x g_k^-1 / |g_k| (float32)
-  int total;                        // points within the reach (may exceed kCoverMax)
+  int total;                       // points within the reach (may exceed NB)
 };
+static_assert(kCoverMax <= 256 && kCoverMaxNarrow <= 256, "facet keys hold 8-bit neighbour indices");
 
 // A vector orthogonal to a, b and c (the 4-D generalised cross product).
 __device__ __forceinline__ double4 cross4(double4 a, double4 b, double4 c) {
@@ -87,7 +96,8 @@ __device__ __forceinline__ double4 cover_point(const float4* __restrict__ q, con
 // the lower index. A point on the hyperplane already (-n . d within rounding of 0: co-spherical
 // points) is met at once (r = inf) when it lies on v's side of the face by more than rounding,
 // never otherwise: a point on the face's own line would make a flat facet. Warp-uniform.
-__device__ __forceinline__ int cover_pivot(const CoverWarp& W, int count, double4 n, double4 v, int e0, int e1,
+template <class Star>
+__device__ __forceinline__ int cover_pivot(const Star& W, int count, double4 n, double4 v, int e0, int e1,
                                            int e2, double& r_out) {
   const unsigned full = 0xffffffffu;
   double best = -INFINITY;
@@ -134,7 +144,8 @@ __device__ __forceinline__ uint32_t facet_key(int a, int b, int c) {
 
 // Collection of the points within reach2 of x into W.key (unsorted; W.total counts them all).
 // Grid: the chart ball of the reach over the sorted shell sites (as k_nearest_exact walks it).
-__device__ __forceinline__ void cover_collect_grid(const CoverArgs& A, const double4* ops, CoverWarp& W, uint32_t i,
+template <class Star>
+__device__ __forceinline__ void cover_collect_grid(const CoverArgs& A, const double4* ops, Star& W, uint32_t i,
                                                    double4 x, double reach2) {
   const NearGrid g = *A.grid;
   const int lane = threadIdx.x & 31;
@@ -159,7 +170,7 @@ __device__ __forceinline__ void cover_collect_grid(const CoverArgs& A, const dou
       const double c2 = dot4(d, d);
       if (c2 <= reach2 && c2 > 1e-24) {
         const int slot = atomicAdd(&W.total, 1);
-        if (slot < kCoverMax) W.key[slot] = key;
+        if (slot < Star::kPoints) W.key[slot] = key;
       }
     }
   }
@@ -167,7 +178,8 @@ __device__ __forceinline__ void cover_collect_grid(const CoverArgs& A, const dou
 
 // Dense: every image of every source, screened in float32 (dot of q_j with x g_k^-1, within
 // 4e-6 of the reach's cosine; the float32 error is below 1e-6), then tested in FP64.
-__device__ __forceinline__ void cover_collect_dense(const CoverArgs& A, const double4* ops, int order, CoverWarp& W,
+template <class Star>
+__device__ __forceinline__ void cover_collect_dense(const CoverArgs& A, const double4* ops, int order, Star& W,
                                                     uint32_t i, double4 x, double reach2) {
   const int lane = threadIdx.x & 31;
   const float lim = (float)(1.0 - 0.5 * reach2) - 4e-6f;
@@ -185,20 +197,26 @@ __device__ __forceinline__ void cover_collect_dense(const CoverArgs& A, const do
         const double c2 = dot4(d, d);
         if (c2 <= reach2 && c2 > 1e-24) {
           const int slot = atomicAdd(&W.total, 1);
-          if (slot < kCoverMax) W.key[slot] = key;
+          if (slot < Star::kPoints) W.key[slot] = key;
         }
       }
     }
   }
 }
 
+// NB, NF: the star's capacity (neighbours, facets). A narrow star (NB < kCoverMax) that
+// cannot hold a source's points or facets reports it short at the reach it was asked for, so
+// the wide star runs it again at that reach.
+template <int NB, int NF>
 __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs A) {
+  using Star = CoverStar<NB, NF>;
+  constexpr bool kNarrow = NB < kCoverMax;
   extern __shared__ __align__(16) unsigned char cover_smem[];
   __shared__ double4 ops[kMaxGroupOrder];
   const int off = c_group_offset[A.gid], order = c_group_order[A.gid];
   for (int k = threadIdx.x; k < order; k += blockDim.x) ops[k] = c_ops32[off + k];
   __syncthreads();
-  CoverWarp& W = reinterpret_cast<CoverWarp*>(cover_smem)[threadIdx.x >> 5];
+  Star& W = reinterpret_cast<Star*>(cover_smem)[threadIdx.x >> 5];
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   const int count_src = A.list ? A.count : A.n;
@@ -210,6 +228,7 @@ __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs
     double reach2 = A.reach2_of ? A.reach2_of[i] : A.reach2;
     if (A.grid) reach2 = fmin(reach2, A.grid_reach2);
     reach2 = fmin(reach2, 4.0);
+    const double asked2 = reach2;
     if (!A.grid) {
       // x g_k^-1 / |g_k|: (q_j g_k) . x = q_j . (x conj(g_k)) for the float32 operator g_k.
       for (int k = lane; k < order; k += 32) {
@@ -228,38 +247,38 @@ __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs
       else cover_collect_dense(A, ops, order, W, i, x, reach2);
       __syncwarp();
       const int total = W.total;
-      if (total <= kCoverMax) {
+      if (total <= NB) {
         count = total;
         break;
       }
-      reach2 *= pow(0.8 * kCoverMax / (double)total, 2.0 / 3.0);
+      reach2 *= pow(0.8 * NB / (double)total, 2.0 / 3.0);
       __syncwarp();
     }
     uint32_t status = kCoverOk;
     double alpha = 0.0;
     double4 centre = x;
     int faces = 0, nfacets = 0;
-    if (count < 4) status = count == 0 && W.total > kCoverMax ? kCoverCrowded : kCoverSparse;
+    if (count < 4) status = count == 0 && W.total > NB ? kCoverCrowded : kCoverSparse;
     if (status == kCoverOk) {
       // Canonical order: each key's rank among the collected keys (keys are distinct).
-      uint32_t mine[kCoverMax / 32];
-      int rank[kCoverMax / 32];
-      for (int u = 0; u < kCoverMax / 32; ++u) {
+      uint32_t mine[NB / 32];
+      int rank[NB / 32];
+      for (int u = 0; u < NB / 32; ++u) {
         const int e = lane + 32 * u;
         mine[u] = e < count ? W.key[e] : 0xffffffffu;
         rank[u] = 0;
       }
       for (int e2 = 0; e2 < count; ++e2) {
         const uint32_t k2 = W.key[e2];
-        for (int u = 0; u < kCoverMax / 32; ++u) rank[u] += k2 < mine[u];
+        for (int u = 0; u < NB / 32; ++u) rank[u] += k2 < mine[u];
       }
       __syncwarp();
-      for (int u = 0; u < kCoverMax / 32; ++u)
+      for (int u = 0; u < NB / 32; ++u)
         if (lane + 32 * u < count) {
           W.d[rank[u]] = sub4d(cover_point(A.q, ops, mine[u]), x);
           if (A.mesh) W.key[rank[u]] = mine[u];  // every lane has read the keys (the sync above)
         }
-      if (lane < kCoverMax / 32) W.used[lane] = 0u;
+      if (lane < NB / 32) W.used[lane] = 0u;
       __syncwarp();
       // 2. A first facet: from the tangent hyperplane (n = x) pivot towards the nearest
       // point, then about it, then about both.
@@ -355,7 +374,7 @@ __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs
           for (int t = lane; t < tail; t += 32) seen |= W.facet[t] == key;
           seen = __any_sync(full, seen);
           if (!seen) {
-            if (tail == kCoverFacets) {
+            if (tail == NF) {
               status = kCoverStarFull;
               break;
             }
@@ -380,8 +399,8 @@ __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs
           if (A.mesh_normal) A.mesh_normal[first + t] = W.normal[t];
         }
       }
-      if (lane < kCoverMax / 32) faces = __popc(W.used[lane]);
-      for (int o = 4; o; o >>= 1) faces += __shfl_xor_sync(full, faces, o);
+      if (lane < NB / 32) faces = __popc(W.used[lane]);
+      for (int o = 16; o; o >>= 1) faces += __shfl_xor_sync(full, faces, o);
       faces = __shfl_sync(full, faces, 0);
     }
     // Certificate: every cap of the star lies within 2 alpha of x.
@@ -395,6 +414,11 @@ __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs
       }
     } else if (status == kCoverSparse) {
       need2 = fmin(4.0, 4.0 * reach2);  // too few points or no closed star: twice the reach
+    }
+    if (kNarrow && status != kCoverOk &&
+        (status == kCoverCrowded || status == kCoverStarFull || reach2 < asked2)) {
+      status = kCoverShort;  // to the wide star, at least at the reach this one was asked for
+      need2 = fmax(need2, asked2);
     }
     if (lane == 0) {
       A.alpha[i] = alpha;

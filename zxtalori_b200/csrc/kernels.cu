@@ -65,18 +65,27 @@ cudaError_t launch_refine_nearest(const float4* q32, int n, int gid, Rows rows, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s) {
+template <int NB, int NF>
+static cudaError_t launch_cover_star(const CoverArgs& A, int count, int sms, cudaStream_t s) {
+  const size_t smem = kCoverWarps * sizeof(CoverStar<NB, NF>);
+  cudaError_t e = cudaFuncSetAttribute(k_cover_star<NB, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // Warps loop over the sources: as many blocks as stay resident.
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cover_star<NB, NF>, kCoverWarps * 32, smem);
+  if (e != cudaSuccess) return e;
+  const int blocks = std::max(1, std::min((count + kCoverWarps - 1) / kCoverWarps, std::max(1, per_sm) * sms));
+  k_cover_star<NB, NF><<<blocks, kCoverWarps * 32, smem, s>>>(A);
+  probe_count();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s, bool narrow) {
   const int count = A.list ? A.count : A.n;
   if (count <= 0) return cudaSuccess;
   if (A.n >= (1 << 24)) return cudaErrorInvalidValue;  // point keys hold the source in 24 bits
-  const size_t smem = kCoverWarps * sizeof(CoverWarp);
-  cudaError_t e = cudaFuncSetAttribute(k_cover_star, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  // Warps loop over the sources: a few resident blocks per SM.
-  const int blocks = std::max(1, std::min((count + kCoverWarps - 1) / kCoverWarps, 4 * sms));
-  k_cover_star<<<blocks, kCoverWarps * 32, smem, s>>>(A);
-  probe_count();
-  return cudaGetLastError();
+  return narrow ? launch_cover_star<kCoverMaxNarrow, kCoverFacetsNarrow>(A, count, sms, s)
+                : launch_cover_star<kCoverMax, kCoverFacets>(A, count, sms, s);
 }
 
 // FP32 FMA throughput probe: 8 independent FMA chains per thread (latency hidden by ILP and

@@ -193,7 +193,9 @@ struct CoverArgs {
   const uint32_t* mesh_offset;
   double4* mesh_normal;  // with mesh (may be null): each facet's unit normal, its cap's centre
 };
-cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s);
+// narrow: the first pass's star of 64 neighbours and 128 facets (more warps resident); a
+// source it cannot hold comes back short at its reach for the wide star (256 and 256).
+cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s, bool narrow);
 
 // Relaxation step pieces.
 cudaError_t launch_relax_stats(Rows rows, const double4* prev_f, const double4* prev_d, int n, int fixed,
