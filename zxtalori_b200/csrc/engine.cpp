@@ -1551,11 +1551,16 @@ const char* Engine::stats() {
     j.integer("covering_certificate_probes", (long long)cover_->probes);
     j.null("covering_exact_predicates");
     j.integer("covering_rounds", cover_->rounds);
+    j.integer("covering_first_pass_short", cover_->first_short);
+    j.integer("covering_first_pass_sparse", cover_->first_sparse);
+    j.integer("covering_rerun_grid", cover_->rerun_grid);
+    j.integer("covering_rerun_dense", cover_->rerun_dense);
   } else {
     for (const char* k : {"covering_unresolved_caps", "covering_iteration", "covering_witness",
                           "covering_domain_bound_deg", "covering_shell_points", "covering_fence_points",
                           "covering_tetrahedra", "covering_certificate_probes", "covering_exact_predicates",
-                          "covering_rounds"})
+                          "covering_rounds", "covering_first_pass_short", "covering_first_pass_sparse",
+                          "covering_rerun_grid", "covering_rerun_dense"})
       j.null(k);
   }
   j.boolean("measured", m.has_value());

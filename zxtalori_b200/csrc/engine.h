@@ -115,6 +115,9 @@ struct CoverResult {
   uint64_t probes = 0;             // pivots evaluated
   uint32_t rounds = 0;             // collection rounds (sources with a short reach run again)
   uint32_t shell_points = 0;       // shell sites of the chart grid the stars were collected from (0: every image)
+  // After the first pass: sources short of reach, sources without a closed star; sources
+  // built again from the chart grid and from every image (over all later rounds).
+  uint32_t first_short = 0, first_sparse = 0, rerun_grid = 0, rerun_dense = 0;
 };
 
 // Plateau kicks of the covering optimiser (src/engine.zig:407-413 setKicks).
