@@ -148,11 +148,14 @@ def test_chart_grid_against_hull(engine):
 def test_covering_at_the_headline_size(engine):
     """O, N = 100,000 (seed 193): every star proven and the same as every image's; a cell has
     about 15.5 Voronoi faces on average (the mean vertex degree of a random 3-D Delaunay
-    triangulation)."""
+    triangulation). Every source the first (narrow) pass left short ran again, all of them
+    from the chart grid: a reach past the grid's is tried at the grid's full reach first."""
     with engine.haar("O", 100_000, 193) as grid:
         near, near_cov, near_faces = _per_point(grid, 0)
         dense, dense_cov, dense_faces = _per_point(grid, 1)
     assert near["covering_unresolved_caps"] == 0 and near["covering_shell_points"] > 0
+    first = near["covering_first_pass_short"] + near["covering_first_pass_sparse"]
+    assert 0 < first <= near["covering_rerun_grid"] and near["covering_rerun_dense"] == 0
     assert np.array_equal(near_cov, dense_cov) and np.array_equal(near_faces, dense_faces)
     assert 13 < near_faces.mean() < 17
     assert near["covering_domain_bound_deg"] >= near["covering_radius_deg"] > near["simplex_bound_deg"]
