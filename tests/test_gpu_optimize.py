@@ -82,3 +82,29 @@ def test_invalid_settings_through_the_abi(engine):
         assert grid._lib.zo_error(grid._handle).decode() == "Covering kicks: InvalidKickPatience"
         assert grid._lib.zo_cover_optimize(grid._handle, 1, 2, 1, 0.0) == -1
         assert grid._lib.zo_error(grid._handle).decode() == "Covering optimization: InvalidCoveringMode"
+
+
+def test_undone_steps_bring_back_the_covering_they_set_aside(engine):
+    """A step that does not lower the radius is undone, and the covering measured before it
+    comes back instead of being measured again: after a batch that ends without the
+    finishing pass, the engine's covering (radius, per-point caps and faces, and the mesh
+    built from its stars and chart grid) equals a fresh measurement of the same sample."""
+    with engine.haar("O", 4000, 4) as grid:
+        grid._check(grid._lib.zo_debug_cover_mode(grid._handle, 2))  # the chart grid's path
+        grid.relax(20)
+        grid.covering()
+        grid._check(grid._lib.zo_cover_optimize(grid._handle, 40, 1, 0, 0.0))
+        stats = grid.stats
+        assert stats["covering_optimizer_skipped"] > 0 and stats["covering_optimizer_improved"] > 0
+        assert stats["covering_current"]
+        kept = (stats["covering_radius_deg"], grid.point_values("covering").copy(),
+                grid.point_values("faces").copy())
+        kept_mesh = grid.triangulation()
+        grid._check(grid._lib.zo_debug_cover_mode(grid._handle, 2))  # drops the covering
+        fresh_mesh = grid.triangulation()
+        fresh = grid.stats
+        assert fresh["covering_radius_deg"] == kept[0]
+        assert np.array_equal(grid.point_values("covering"), kept[1])
+        assert np.array_equal(grid.point_values("faces"), kept[2])
+        assert np.array_equal(fresh_mesh["tetrahedra"], kept_mesh["tetrahedra"])
+        assert np.array_equal(fresh_mesh["stereographic"], kept_mesh["stereographic"])

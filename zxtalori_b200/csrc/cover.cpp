@@ -236,6 +236,42 @@ void Engine::measure_covering() {
   cover_grid_reach2_ = grid ? grid_reach2 : 0.0;
 }
 
+void Engine::swap_covering() {
+  CoverSaved& o = cover_saved_;
+  std::swap(cover_, o.result);
+  std::swap(cover_iteration_, o.iteration);
+  std::swap(cover_key_, o.key);
+  std::swap(point_covering_iteration_, o.point_iteration);
+  point_covering_.swap(o.point_covering);
+  point_faces_.swap(o.point_faces);
+  cover_alpha_.swap(o.alpha);
+  cover_centre_.swap(o.centre);
+  cover_faces_.swap(o.faces);
+  cover_facets_.swap(o.facets);
+  cover_status_.swap(o.status);
+  std::swap(cover_near_, o.near);
+  std::swap(cover_reach_, o.reach);
+  std::swap(cover_narrow_, o.narrow);
+  std::swap(cover_facet_counts_, o.facet_counts);
+  std::swap(cover_grid_reach2_, o.grid_reach2);
+}
+
+void Engine::set_covering_aside() {
+  const bool current = cover_ && cover_key_ == sample_key() && cover_iteration_ == iteration_ &&
+                       point_covering_iteration_ && *point_covering_iteration_ == iteration_;
+  swap_covering();
+  cover_saved_.valid = current;
+  cover_.reset();  // what came back is older: the next cover() measures afresh
+  cover_cached_ = false;
+}
+
+bool Engine::restore_covering() {
+  if (!cover_saved_.valid || cover_saved_.iteration != iteration_ || cover_saved_.key != sample_key()) return false;
+  swap_covering();
+  cover_saved_.valid = false;
+  return true;
+}
+
 // Every source's star again, in the reach and the star width that proved it (so that the
 // same points are collected and the same facets found), written out as tetrahedra of point
 // keys ((source << 8) | image; the source first) with each facet's unit normal (its cap's

@@ -841,6 +841,7 @@ void Engine::reset_run() {
   point_covering_iteration_.reset();
   cover_.reset();
   cover_cached_ = false;
+  cover_saved_.valid = false;
   relax_state_.reset();
   iteration_ = 0;
   step_deg_ = 0;
@@ -1366,7 +1367,9 @@ size_t Engine::device_bytes() const {
          full_pdegen_.bytes() + cover_alpha_.bytes() + cover_centre_.bytes() + cover_faces_.bytes() +
          cover_facets_.bytes() + cover_status_.bytes() + cover_need_.bytes() + cover_list_.bytes() +
          cover_probes_.bytes() + cover_mesh_.bytes() + cover_mesh_offset_.bytes() + cover_mesh_normal_.bytes() +
-         (cover_near_ ? cover_near_->bytes() : 0);
+         (cover_near_ ? cover_near_->bytes() : 0) + cover_saved_.alpha.bytes() + cover_saved_.centre.bytes() +
+         cover_saved_.faces.bytes() + cover_saved_.facets.bytes() + cover_saved_.status.bytes() +
+         (cover_saved_.near ? cover_saved_.near->bytes() : 0);
 }
 
 void Engine::spacing_exact(uint32_t* listed, uint32_t* ties) {

@@ -73,6 +73,11 @@ class PinnedArray {
   T* data() { return p_; }
   const T* data() const { return p_; }
   size_t size() const { return n_; }
+  void swap(PinnedArray& o) noexcept {
+    std::swap(p_, o.p_);
+    std::swap(n_, o.n_);
+    std::swap(cap_, o.cap_);
+  }
 
  private:
   T* p_ = nullptr;
@@ -92,6 +97,11 @@ class DeviceBuffer {
   template <class T>
   T* as() const { return static_cast<T*>(ptr_); }
   size_t bytes() const { return bytes_; }
+  void swap(DeviceBuffer& o) noexcept {
+    std::swap(ptr_, o.ptr_);
+    std::swap(bytes_, o.bytes_);
+    std::swap(stream_, o.stream_);
+  }
 
  private:
   void* ptr_ = nullptr;
@@ -575,6 +585,25 @@ class Engine {
   std::vector<uint32_t> cover_facet_counts_;
   double cover_grid_reach2_ = 0;
   DeviceBuffer cover_mesh_, cover_mesh_offset_, cover_mesh_normal_;
+  // A covering set aside (the optimiser's current sample while a candidate step is
+  // measured): everything a covering pass leaves for later calls, swapped in and out whole.
+  struct CoverSaved {
+    bool valid = false;
+    std::optional<CoverResult> result;
+    uint32_t iteration = 0;
+    uint64_t key = 0;
+    std::optional<uint32_t> point_iteration;
+    PinnedArray<float> point_covering, point_faces;
+    DeviceBuffer alpha, centre, faces, facets, status;
+    std::unique_ptr<NearField> near;
+    std::vector<double> reach;
+    std::vector<uint8_t> narrow;
+    std::vector<uint32_t> facet_counts;
+    double grid_reach2 = 0;
+  } cover_saved_;
+  void swap_covering();       // exchanges the covering state with cover_saved_
+  void set_covering_aside();  // the current covering to cover_saved_; none current after it
+  bool restore_covering();    // back from cover_saved_ when it is of the current sample
   void export_stars(std::vector<uint4>& tets, std::vector<double4>& normals);
   std::vector<float> insertion_centres(uint32_t wanted);
   uint32_t distinct_rows(std::vector<float>& values, uint32_t unique) const;

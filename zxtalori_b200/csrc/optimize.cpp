@@ -115,6 +115,7 @@ void Engine::optimize_covering(uint32_t steps, uint32_t mode, bool finish, doubl
     ++o.full_steps;
     bool accepted = false;
     if (jobs > 0) {
+      set_covering_aside();  // the current sample's covering, back unchanged if the step is undone
       move_to(candidate);
       cover();
       const double radius = cover_->radius_deg;
@@ -140,7 +141,10 @@ void Engine::optimize_covering(uint32_t steps, uint32_t mode, bool finish, doubl
     if (!accepted) {
       ++o.skipped;
       o.trust *= 0.5;
-      if (jobs > 0) move_to(o.current);
+      if (jobs > 0) {
+        move_to(o.current);
+        restore_covering();
+      }
     }
     // Plateau: restore the best sample and kick every orientation.
     if (o.current_radius < o.gain_ref * (1.0 - kicks_.progress)) {
