@@ -97,3 +97,27 @@ def test_python_api_surface():
     for method in ("relax", "measure", "spacing", "point_values", "quaternions", "stats", "operations", "set",
                    "identity", "save", "close", "covering", "triangulation", "optimize_covering"):
         assert hasattr(zo.Grid, method), method
+
+
+def test_serve_structs_match_the_header(tmp_path):
+    """The ctypes request and result records of serve.NativeServer have the C layout that
+    include/zxtalori.h declares for zo_serve (sizes and every field's offset, from gcc)."""
+    from zxtalori_b200.serve import _NativeRequest, _NativeResult
+
+    records = {"zo_serve_request": _NativeRequest, "zo_serve_result": _NativeResult}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for c_name, record in records.items():
+        lines.append(f'  printf("{c_name} size %zu\\n", sizeof({c_name}));')
+        for field, _ in record._fields_:
+            lines.append(f'  printf("{c_name} {field} %zu\\n", offsetof({c_name}, {field}));')
+    lines += ["  return 0;", "}"]
+    source = tmp_path / "layout.c"
+    source.write_text("\n".join(lines) + "\n")
+    binary = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-o", str(binary), str(source)], check=True)
+    printed = dict(line.rsplit(" ", 1) for line in subprocess.run([str(binary)], check=True, capture_output=True,
+                                                                   text=True).stdout.splitlines())
+    for c_name, record in records.items():
+        assert int(printed[f"{c_name} size"]) == ctypes.sizeof(record)
+        for field, _ in record._fields_:
+            assert int(printed[f"{c_name} {field}"]) == getattr(record, field).offset, (c_name, field)
