@@ -314,7 +314,7 @@ def batched_section(zo, samples=256, steps=50, dist=None):
 
 def served_split_section(zo, device_rate, dist, factor=1.4, per_rate=200):
     """Config 5 over several GPUs: one request stream at `factor` times the whole job's
-    capacity, request k served by rank k mod N (its own Server, no collective); the ranks'
+    capacity, request k served by rank k mod N (its own zo_serve loop, no collective); the ranks'
     results are gathered for the whole-job throughput (all pair evaluations over the longest
     rank's span) and latency percentiles."""
     from zxtalori_b200 import serve
@@ -329,7 +329,7 @@ def served_split_section(zo, device_rate, dist, factor=1.4, per_rate=200):
     served = serve.NativeServer().run(mine)
     everything = [r for part in dist.gather(served) for r in part]
     return {"rate_per_s": rate, "rate_over_capacity": factor, "gpus": dist.world,
-            "split": "request k to rank k mod N, one Server per GPU, no collective",
+            "split": "request k to rank k mod N, one zo_serve loop per GPU, no collective",
             **serve.summary(everything)}
 
 
