@@ -143,20 +143,19 @@ void Engine::measure_covering() {
   A.reach2_of = nullptr;
   A.list = nullptr;
   A.count = n;
-  ZO_CUDA(launch_cover(A, sms_, stream_, true));
+  ZO_CUDA(launch_cover(A, sms_, stream_, 0));
   r.rounds = 1;
   std::vector<uint32_t> status(n);
   std::vector<double> need(n);
   std::vector<double> used(n, reach2);  // the reach each source's star was built in
-  std::vector<uint8_t> narrow(n, 1);    // built by the narrow star (round 0)
-  std::vector<uint32_t> listed, grid_list, dense_list;
+  std::vector<uint8_t> width(n, 0);     // the star width it was built in (0 narrow .. 2 wide)
+  std::vector<uint32_t> listed, part[6];  // reruns: (grid, every image) x width
   for (int round = 1;; ++round) {
     ZO_CUDA(cudaMemcpyAsync(status.data(), A.status, (size_t)n * 4, cudaMemcpyDeviceToHost, stream_));
     ZO_CUDA(cudaMemcpyAsync(need.data(), A.need2, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, stream_));
     ZO_CUDA(cudaStreamSynchronize(stream_));
     if (cancelled_.load()) throw Failure("Cancelled");
-    grid_list.clear();
-    dense_list.clear();
+    for (auto& p : part) p.clear();
     for (int i = 0; i < n; ++i) {
       if (status[i] != kCoverShort && status[i] != kCoverSparse) continue;
       if (round == 1) ++(status[i] == kCoverShort ? r.first_short : r.first_sparse);
@@ -164,32 +163,30 @@ void Engine::measure_covering() {
       // (the kernel clamps to it): a star left open by points missing beyond a short reach
       // can show a cap much wider than its true one.
       const bool fits = grid && (need[i] <= grid_reach2 || used[i] < grid_reach2);
-      (fits ? grid_list : dense_list).push_back((uint32_t)i);
       used[i] = fits ? std::min(need[i], grid_reach2) : need[i];
-      narrow[i] = 0;
+      width[i] = (uint8_t)std::min(2, width[i] + 1);
+      part[(fits ? 0 : 3) + width[i]].push_back((uint32_t)i);
     }
-    if ((grid_list.empty() && dense_list.empty()) || round == kCoverRounds) break;
-    r.rerun_grid += (uint32_t)grid_list.size();
-    r.rerun_dense += (uint32_t)dense_list.size();
+    size_t total = 0;
+    for (const auto& p : part) total += p.size();
+    if (total == 0 || round == kCoverRounds) break;
+    r.rerun_grid += (uint32_t)(part[1].size() + part[2].size());
+    r.rerun_dense += (uint32_t)(part[4].size() + part[5].size());
     // need2 holds each listed source's next reach: the kernel reads it before it writes.
     A.reach2_of = A.need2;
-    const size_t g = grid_list.size();
-    // The grid's sources first, then those that need every image.
-    listed.assign(grid_list.begin(), grid_list.end());
-    listed.insert(listed.end(), dense_list.begin(), dense_list.end());
+    listed.clear();
+    for (const auto& p : part) listed.insert(listed.end(), p.begin(), p.end());
     ZO_CUDA(cudaMemcpyAsync(cover_list_.as<uint32_t>(), listed.data(), listed.size() * 4, cudaMemcpyHostToDevice,
                             stream_));
-    if (g > 0) {
-      A.grid = grid;
-      A.list = cover_list_.as<uint32_t>();
-      A.count = (int)g;
-      ZO_CUDA(launch_cover(A, sms_, stream_, false));
-    }
-    if (!dense_list.empty()) {
-      A.grid = nullptr;
-      A.list = cover_list_.as<uint32_t>() + g;
-      A.count = (int)dense_list.size();
-      ZO_CUDA(launch_cover(A, sms_, stream_, false));
+    size_t first = 0;
+    for (int k = 0; k < 6; ++k) {
+      if (!part[k].empty()) {
+        A.grid = k < 3 ? grid : nullptr;
+        A.list = cover_list_.as<uint32_t>() + first;
+        A.count = (int)part[k].size();
+        ZO_CUDA(launch_cover(A, sms_, stream_, k % 3));
+      }
+      first += part[k].size();
     }
     ++r.rounds;
   }
@@ -231,7 +228,7 @@ void Engine::measure_covering() {
   cover_iteration_ = iteration_;
   point_covering_iteration_ = iteration_;
   cover_reach_ = std::move(used);
-  cover_narrow_ = std::move(narrow);
+  cover_width_ = std::move(width);
   cover_facet_counts_ = std::move(facets);
   cover_grid_reach2_ = grid ? grid_reach2 : 0.0;
 }
@@ -251,7 +248,7 @@ void Engine::swap_covering() {
   cover_status_.swap(o.status);
   std::swap(cover_near_, o.near);
   std::swap(cover_reach_, o.reach);
-  std::swap(cover_narrow_, o.narrow);
+  std::swap(cover_width_, o.width);
   std::swap(cover_facet_counts_, o.facet_counts);
   std::swap(cover_grid_reach2_, o.grid_reach2);
 }
@@ -279,7 +276,7 @@ bool Engine::restore_covering() {
 void Engine::export_stars(std::vector<uint4>& tets, std::vector<double4>& normals) {
   cover();
   const int n = (int)n_;
-  if (cover_reach_.size() != (size_t)n || cover_facet_counts_.size() != (size_t)n || cover_narrow_.size() != (size_t)n)
+  if (cover_reach_.size() != (size_t)n || cover_facet_counts_.size() != (size_t)n || cover_width_.size() != (size_t)n)
     throw Failure("CoveringNotMeasured");
   std::vector<uint32_t> offset(n + 1, 0);
   uint64_t total = 0;
@@ -314,21 +311,21 @@ void Engine::export_stars(std::vector<uint4>& tets, std::vector<double4>& normal
   A.mesh_offset = cover_mesh_offset_.as<uint32_t>();
   A.mesh_normal = cover_mesh_normal_.as<double4>();
   // Each source from the chart grid when its reach is within the grid's (the grid of the
-  // covering pass, built for these positions), else from every image; in the narrow star when
-  // the first pass proved it there.
-  std::vector<uint32_t> part[4];  // grid narrow, grid wide, dense narrow, dense wide
+  // covering pass, built for these positions), else from every image; in the star width
+  // that proved it.
+  std::vector<uint32_t> part[6];  // (grid, every image) x width
   for (int i = 0; i < n; ++i) {
     const bool in_grid = cover_grid_reach2_ > 0 && cover_reach_[i] <= cover_grid_reach2_;
-    part[(in_grid ? 0 : 2) + (cover_narrow_[i] ? 0 : 1)].push_back((uint32_t)i);
+    part[(in_grid ? 0 : 3) + cover_width_[i]].push_back((uint32_t)i);
   }
   std::vector<uint32_t> all;
   for (const auto& p : part) all.insert(all.end(), p.begin(), p.end());
   cover_list_.ensure((size_t)n * 4);
   ZO_CUDA(cudaMemcpyAsync(cover_list_.as<uint32_t>(), all.data(), all.size() * 4, cudaMemcpyHostToDevice, stream_));
   size_t first = 0;
-  for (int k = 0; k < 4; ++k) {
+  for (int k = 0; k < 6; ++k) {
     if (!part[k].empty()) {
-      if (k < 2) {
+      if (k < 3) {
         A.scode = cover_near_->sorted_codes();
         A.simg = cover_near_->sorted_images();
         A.cell_off = cover_near_->cell_offsets();
@@ -339,7 +336,7 @@ void Engine::export_stars(std::vector<uint4>& tets, std::vector<double4>& normal
       }
       A.list = cover_list_.as<uint32_t>() + first;
       A.count = (int)part[k].size();
-      ZO_CUDA(launch_cover(A, sms_, stream_, (k & 1) == 0));
+      ZO_CUDA(launch_cover(A, sms_, stream_, k % 3));
     }
     first += part[k].size();
   }

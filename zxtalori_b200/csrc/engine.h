@@ -578,10 +578,11 @@ class Engine {
   DeviceBuffer cover_alpha_, cover_centre_, cover_faces_, cover_facets_, cover_status_, cover_need_, cover_list_,
       cover_probes_;
   std::unique_ptr<NearField> cover_near_;
-  // Of the last covering pass: the reach each source's star was proven in, whether the
-  // narrow star proved it, its facet count, and the reach its chart grid holds (0: no grid).
+  // Of the last covering pass: the reach each source's star was proven in, the star width
+  // that proved it (0 narrow, 1 middle, 2 wide), its facet count, and the reach its chart
+  // grid holds (0: no grid).
   std::vector<double> cover_reach_;
-  std::vector<uint8_t> cover_narrow_;
+  std::vector<uint8_t> cover_width_;
   std::vector<uint32_t> cover_facet_counts_;
   double cover_grid_reach2_ = 0;
   DeviceBuffer cover_mesh_, cover_mesh_offset_, cover_mesh_normal_;
@@ -597,7 +598,7 @@ class Engine {
     DeviceBuffer alpha, centre, faces, facets, status;
     std::unique_ptr<NearField> near;
     std::vector<double> reach;
-    std::vector<uint8_t> narrow;
+    std::vector<uint8_t> width;
     std::vector<uint32_t> facet_counts;
     double grid_reach2 = 0;
   } cover_saved_;

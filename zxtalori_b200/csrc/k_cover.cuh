@@ -51,6 +51,10 @@ constexpr int kCoverFacets = 256;   // facets per star (the wide star)
 // a source that overflows it is sent to the wide star at the same reach.
 constexpr int kCoverMaxNarrow = 64;
 constexpr int kCoverFacetsNarrow = 128;
+// Reruns (a reach wider than the first) start in a middle star of 128 neighbours and 256
+// facets (15 KB per warp), then go to the wide one.
+constexpr int kCoverMaxMiddle = 128;
+constexpr int kCoverFacetsMiddle = 256;
 
 template <int NB, int NF>
 struct CoverStar {
@@ -63,7 +67,8 @@ struct CoverStar {
   float4 image_dot[kMaxGroupOrder];  // dense collection: x g_k^-1 / |g_k| (float32)
   int total;                       // points within the reach (may exceed NB)
 };
-static_assert(kCoverMax <= 256 && kCoverMaxNarrow <= 256, "facet keys hold 8-bit neighbour indices");
+static_assert(kCoverMax <= 256 && kCoverMaxNarrow <= kCoverMaxMiddle && kCoverMaxMiddle <= kCoverMax,
+              "facet keys hold 8-bit neighbour indices");
 
 // A vector orthogonal to a, b and c (the 4-D generalised cross product).
 __device__ __forceinline__ double4 cross4(double4 a, double4 b, double4 c) {
@@ -204,9 +209,9 @@ __device__ __forceinline__ void cover_collect_dense(const CoverArgs& A, const do
   }
 }
 
-// NB, NF: the star's capacity (neighbours, facets). A narrow star (NB < kCoverMax) that
-// cannot hold a source's points or facets reports it short at the reach it was asked for, so
-// the wide star runs it again at that reach.
+// NB, NF: the star's capacity (neighbours, facets). A star narrower than the wide one
+// (NB < kCoverMax) that cannot hold a source's points or facets reports it short at the
+// reach it was asked for, so the next width runs it again at that reach.
 template <int NB, int NF>
 __global__ void __launch_bounds__(kCoverWarps * 32) k_cover_star(const CoverArgs A) {
   using Star = CoverStar<NB, NF>;

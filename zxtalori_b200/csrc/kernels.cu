@@ -80,12 +80,15 @@ static cudaError_t launch_cover_star(const CoverArgs& A, int count, int sms, cud
   return cudaGetLastError();
 }
 
-cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s, bool narrow) {
+cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s, int width) {
   const int count = A.list ? A.count : A.n;
   if (count <= 0) return cudaSuccess;
   if (A.n >= (1 << 24)) return cudaErrorInvalidValue;  // point keys hold the source in 24 bits
-  return narrow ? launch_cover_star<kCoverMaxNarrow, kCoverFacetsNarrow>(A, count, sms, s)
-                : launch_cover_star<kCoverMax, kCoverFacets>(A, count, sms, s);
+  switch (width) {
+    case 0: return launch_cover_star<kCoverMaxNarrow, kCoverFacetsNarrow>(A, count, sms, s);
+    case 1: return launch_cover_star<kCoverMaxMiddle, kCoverFacetsMiddle>(A, count, sms, s);
+    default: return launch_cover_star<kCoverMax, kCoverFacets>(A, count, sms, s);
+  }
 }
 
 // FP32 FMA throughput probe: 8 independent FMA chains per thread (latency hidden by ILP and

@@ -193,9 +193,10 @@ struct CoverArgs {
   const uint32_t* mesh_offset;
   double4* mesh_normal;  // with mesh (may be null): each facet's unit normal, its cap's centre
 };
-// narrow: the first pass's star of 64 neighbours and 128 facets (more warps resident); a
-// source it cannot hold comes back short at its reach for the wide star (256 and 256).
-cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s, bool narrow);
+// width: the star's capacity. 0 narrow (64 neighbours, 128 facets: the first pass), 1
+// middle (128, 256: the first rerun), 2 wide (256, 256). A narrower star keeps more warps
+// resident; a source it cannot hold comes back short at its reach for the next width.
+cudaError_t launch_cover(const CoverArgs& A, int sms, cudaStream_t s, int width);
 
 // Relaxation step pieces.
 cudaError_t launch_relax_stats(Rows rows, const double4* prev_f, const double4* prev_d, int n, int fixed,
