@@ -78,8 +78,10 @@ zo_serve_result finish(Active a, bool measure, double t0_seconds) {
   r.neighbourhood = a.request.neighbourhood;
   r.count = a.request.count;
   r.order = kOrders[a.request.group];
+  // This thread works on the engine's device from here on, the engine's release included.
+  const cudaError_t device = cudaSetDevice(a.engine->device());
   try {
-    ZO_CUDA(cudaSetDevice(a.engine->device()));
+    ZO_CUDA(device);
     AllocScope scope(a.engine->stream());
     a.engine->relax_finish();
     if (measure) a.engine->measure();
