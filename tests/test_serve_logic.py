@@ -204,3 +204,49 @@ def test_batch_shards_cover_every_sample_once_and_balance():
         assert shares == [batch.shard(specs, r, world) for r in range(world)]  # the same split on every rank
     with pytest.raises(ValueError):
         batch.shard(specs, 2, 2)
+
+
+class FakeServeLib:
+    """Stands in for the library's zo_serve: checks what NativeServer passes and answers
+    with one result per request, in reverse order (completion order is not arrival order)."""
+
+    _serve_bound = True  # the argument types are the real library's business
+
+    def __init__(self, fail_id=None):
+        self.fail_id = fail_id
+        self.seen = None
+
+    def zo_serve(self, requests, n, settings, n_settings, results, error, error_len):
+        self.seen = ([(requests[k].id, requests[k].group, requests[k].count, requests[k].steps, requests[k].seed,
+                       requests[k].neighbourhood, requests[k].arrival) for k in range(n)],
+                     [settings[k] for k in range(n_settings)])
+        for slot, k in enumerate(reversed(range(n))):
+            r = results[slot]
+            r.id, r.count, r.order, r.iteration = requests[k].id, requests[k].count, 24, requests[k].steps
+            r.arrival, r.admitted, r.finished = requests[k].arrival, requests[k].arrival + 0.5, requests[k].arrival + 1.0
+            r.neighbourhood, r.energy, r.separation_deg = requests[k].neighbourhood, 1.5, 2.0
+            r.status = -1 if requests[k].id == self.fail_id else 0
+            if r.status:
+                r.error = b"Measure: Cancelled"
+        return 0
+
+
+def test_native_server_marshals_requests_settings_and_results(monkeypatch):
+    """NativeServer (the Python face of zo_serve) passes each request and its settings as the
+    header lays them out and turns the records back into results; a failed request raises."""
+    fake = FakeServeLib()
+    monkeypatch.setattr(serve, "_library", lambda: fake)
+    reqs = [serve.Request(7, "O", 2000, 30, 5, 20.0, 0.25), serve.Request(9, "I", 600, 10, 6, 0.0, 1.5)]
+    out = serve.NativeServer(memory_budget=1 << 30, max_active=8, workers=2).run(reqs)
+    passed, settings = fake.seen
+    assert passed == [(7, serve.GROUPS.index("O"), 2000, 30, 5, 20.0, 0.25), (9, serve.GROUPS.index("I"), 600, 10, 6,
+                                                                             0.0, 1.5)]
+    assert settings == [float(1 << 30), 8.0, 0.02, 1.0, 0.0, 2.0, 2.5e11]
+    assert [r.id for r in out] == [9, 7]
+    assert out[1].stats == {"count": 2000, "order": 24, "iteration": 30, "relax_neighbourhood": 20.0,
+                            "quey_energy": 1.5, "separation_deg": 2.0}
+    assert out[0].stats["relax_neighbourhood"] is None  # all pairs
+    assert (out[1].arrival, out[1].admitted, out[1].finished) == (0.25, 0.75, 1.25)
+    monkeypatch.setattr(serve, "_library", lambda: FakeServeLib(fail_id=9))
+    with pytest.raises(RuntimeError, match="request 9: Measure: Cancelled"):
+        serve.NativeServer().run(reqs)
